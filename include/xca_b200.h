@@ -1,0 +1,114 @@
+/*
+ * xca_b200: C-ABI of the B200-native pseudo-particle strong-coupling hot path.
+ *
+ * The reference (TRIQS/xca) exposes this path as C++ classes bound to Python with c2py.  Each entry
+ * point below replaces one reference interface; the comment names it by file:line within TRIQS/xca
+ * (cppdlr, the third-party DLR library, is cited through TRIQS/xca's binding of it).
+ *
+ * Conventions
+ *  - Every function returns an int status: XCA_OK or one of the error codes; xca_last_error() gives
+ *    the message of the last failing call on the calling thread.  No C++ exception crosses the ABI.
+ *    XCA_ERR_INVALID maps the reference's std::invalid_argument, XCA_ERR_RUNTIME its
+ *    std::runtime_error.
+ *  - Host buffers are owned by the caller.  The context owns its device memory and one CUDA stream.
+ *    One context per thread; a context is not thread safe (as the reference's evaluator).
+ *  - Complex arrays are complex128, interleaved (re, im), row-major.  Block Green's functions are
+ *    packed slabs: the blocks in block order, block b an (r, d_b, d_b) array.  The device path
+ *    computes in real FP64 and rejects inputs with a non-zero imaginary part (XCA_ERR_UNSUPPORTED).
+ *  - Imaginary-time nodes are in cppdlr's relative format (t < 0 stands for 1 + t, t = tau / beta);
+ *    real frequencies are dimensionless (omega * beta).
+ */
+#ifndef XCA_B200_H
+#define XCA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XCA_OK 0
+#define XCA_ERR_INVALID 1
+#define XCA_ERR_RUNTIME 2
+#define XCA_ERR_CUDA 3
+#define XCA_ERR_UNSUPPORTED 4
+
+typedef struct xca_ctx xca_ctx;
+
+/* Message of the last failing call on this thread (empty string if none). */
+const char *xca_last_error(void);
+
+/* ABI version of this library. */
+int xca_abi_version(void);
+
+/* cppdlr::build_dlr_rf(lambda, eps): DLR real frequencies, ascending.
+ * Replaces python/triqs_xca/pycppdlr.wrap.cxx:210-214 (build_dlr_rf).  rf_out has room for max_r. */
+int xca_dlr_build_rf(double lambda, double eps, double *rf_out, int max_r, int *r_out);
+
+/* cppdlr::imtime_ops(lambda, dlr_rf).get_itnodes(): DLR imaginary-time nodes, relative format,
+ * ascending absolute time.  Replaces python/triqs_xca/pycppdlr.wrap.cxx:44-47, 111-112. */
+int xca_dlr_build_it(double lambda, const double *rf, int r, double *it_out);
+
+/* Context on CUDA device `device`.  Replaces the construction of a DiagramEvaluator's owned state
+ * (c++/triqs_xca/block_sparse_backbone.hpp:80-84). */
+int xca_ctx_create(int device, xca_ctx **out);
+int xca_ctx_destroy(xca_ctx *ctx);
+
+/* DiagramEvaluator(beta, Lambda, eps, hyb_poles, hyb_coeffs, Fq): TRIQS-free constructor,
+ * c++/triqs_xca/block_sparse_backbone.hpp:158-162 (and the atom_diag constructor :144-147 once the
+ * caller has built Fq).  Uploads the DLR basis (r, rf, it), the hybridization (p physical poles, the
+ * evaluator multiplies them by beta; coefficients p x n x n complex), the symmetry-set labels of the
+ * n orbitals and the field operators as BlockOpSymSet slabs (c++/triqs_xca/block_sparse.hpp:181-200):
+ * F_index[s * n_blocks + b] is the target block of set s acting on block b (-1: none); F_data packs,
+ * in (s, b) order over present columns, a (q_s, d_target, d_b) complex slab.  The barred operators
+ * of BlockOpSymQuartet (c++/triqs_xca/block_sparse.cpp:496-577) are built on the device.
+ * Validation as check_sym_set_block_diagonal (c++/triqs_xca/block_sparse.cpp:443-492). */
+int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, int r, const double *rf, const double *it,
+                        int p, const double *hyb_poles, const double *hyb_coeffs, int n, const long *sym_set_labels,
+                        int n_blocks, const int *block_dims, const int *F_index, const double *F_data,
+                        const int *Fd_index, const double *Fd_data);
+
+/* DiagramEvaluator::get_num_self_energy_backbones, c++/triqs_xca/block_sparse_backbone.cpp:721-724. */
+int xca_num_self_energy_backbones(xca_ctx *ctx, int m, const int *topology, long *out);
+
+/* DiagramEvaluator::get_num_single_ptcle_gf_backbones, c++/triqs_xca/block_sparse_backbone.cpp:733-736. */
+int xca_num_single_ptcle_gf_backbones(xca_ctx *ctx, int m, const int *topology, long *out);
+
+/* DiagramEvaluator::compute_self_energy(G, topology[, f_ix_vec]),
+ * c++/triqs_xca/block_sparse_backbone.cpp:369-459.  topology is m x 2 int.  f_ix == NULL evaluates
+ * every flat index; otherwise the n_fix listed ones (out of range: XCA_ERR_RUNTIME as :319).
+ * G and Sigma_out are host packed complex slabs; blocks that receive nothing come back as zeros. */
+int xca_compute_self_energy(xca_ctx *ctx, const double *G, int m, const int *topology, const long *f_ix, long n_fix,
+                            double *Sigma_out);
+
+/* Same evaluation on device-resident real FP64 slabs (G_dev, Sigma_dev are device pointers of the
+ * packed real layout), accumulating into Sigma_dev with weight `scale` (Sigma_dev += scale * Sigma).
+ * This is the call the solve loop and the benchmark use with data resident in HBM. */
+int xca_compute_self_energy_device(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
+                                   double *Sigma_dev);
+
+/* Number of valid (flat index, block, symmetry set) items of find_path_self_energy
+ * (c++/triqs_xca/block_sparse_backbone.cpp:229-314) for this G and topology, and optionally the rows
+ * (f_ix, b_ix, p_kap, ind_path[0..2m-2]) of the first max_rows of them in flat-index order. */
+int xca_self_energy_items(xca_ctx *ctx, const double *G, int m, const int *topology, long *rows, long max_rows,
+                          long *n_items);
+
+/* Size in bytes of the packed real slab of the evaluator's blocks, and its rank r. */
+int xca_slab_info(xca_ctx *ctx, long *n_doubles, int *r);
+
+/* Device pointer to `bytes` of context-owned device memory (reused across calls; grown as needed). */
+int xca_device_buffer(xca_ctx *ctx, int slot, long bytes, double **dev_ptr);
+
+/* Copies between host and device slabs on the context's stream (synchronous). */
+int xca_copy_to_device(xca_ctx *ctx, double *dev, const double *host, long n_doubles);
+int xca_copy_to_host(xca_ctx *ctx, double *host, const double *dev, long n_doubles);
+
+/* Wait for the context's stream. */
+int xca_synchronize(xca_ctx *ctx);
+
+/* Number of kernels this library launched on the context since creation. */
+int xca_kernel_launches(xca_ctx *ctx, long *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* XCA_B200_H */

@@ -1,0 +1,220 @@
+"""Python face of the device evaluator, with the reference's names
+(``python/triqs_xca/block_sparse.wrap.cxx``: ``DiagramEvaluator`` and its methods,
+``c++/triqs_xca/block_sparse_backbone.hpp:23-165``).
+
+A block Green's function is passed as a list of ``(r, d_b, d_b)`` arrays, as objects with a ``.data``
+attribute, or as an iterable of ``(name, g)`` pairs (the shape of a TRIQS ``BlockGf``); results come
+back as a list of ``(r, d_b, d_b)`` complex arrays.  All evaluation runs in ``libxca_b200.so`` on the
+GPU.
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .atom_diag import AtomDiag, get_operators
+
+
+class BlockOpSymQuartet:
+    """Field operators grouped in symmetry sets (``c++/triqs_xca/block_sparse.hpp:270-291``): the
+    F and F^dag slabs per set and block column; the barred operators are formed by the library."""
+
+    def __init__(self, sym_set_labels, F_index, F_blocks, Fd_index, Fd_blocks, dims):
+        self.sym_set_labels = np.ascontiguousarray(sym_set_labels, dtype=np.int64)
+        self.F_index = np.ascontiguousarray(F_index, dtype=np.int32)
+        self.F_blocks = F_blocks
+        self.Fd_index = np.ascontiguousarray(Fd_index, dtype=np.int32)
+        self.Fd_blocks = Fd_blocks
+        self.dims = np.ascontiguousarray(dims, dtype=np.int32)
+
+    @classmethod
+    def from_atom_diag(cls, ad):
+        labels, Fi, Fb, Fdi, Fdb = get_operators(ad)
+        return cls(labels, Fi, Fb, Fdi, Fdb, ad.get_subspace_dims())
+
+    def packed(self):
+        def pack(index, blocks):
+            parts = []
+            for s in range(index.shape[0]):
+                for b in range(index.shape[1]):
+                    if index[s, b] >= 0:
+                        parts.append(np.ascontiguousarray(blocks[s][b], dtype=np.complex128).ravel())
+            data = np.concatenate(parts) if parts else np.zeros(1, np.complex128)
+            return np.ascontiguousarray(data).view(np.float64)
+
+        return pack(self.F_index, self.F_blocks), pack(self.Fd_index, self.Fd_blocks)
+
+
+def _blocks_of(G):
+    out = []
+    for g in G:
+        if isinstance(g, tuple) and len(g) == 2:
+            g = g[1]
+        if hasattr(g, "data"):
+            g = g.data
+        out.append(np.asarray(g))
+    return out
+
+
+class DiagramEvaluator:
+    """Evaluator of the pseudo-particle self-energy backbones on one GPU.
+
+    ``DiagramEvaluator(hyb_poles, hyb_coeffs, tau_mesh, atom_diag)`` (bsb.hpp:144-147) or
+    ``DiagramEvaluator(beta, Lambda, eps, hyb_poles, hyb_coeffs, Fq)`` (bsb.hpp:158-162).
+    ``device`` selects the CUDA device.
+    """
+
+    def __init__(self, *args, device=0):
+        if len(args) == 4:
+            hyb_poles, hyb_coeffs, mesh, ad = args
+            if not isinstance(ad, AtomDiag):
+                raise TypeError("atom_diag must be an xca_b200.atom_diag.AtomDiag")
+            beta, lam, eps = mesh.beta, mesh.lam, mesh.eps
+            rf, it = mesh.dlr_rf, mesh.dlr_it.it
+            Fq = BlockOpSymQuartet.from_atom_diag(ad)
+        elif len(args) == 6:
+            beta, lam, eps, hyb_poles, hyb_coeffs, Fq = args
+            from .pycppdlr import ImTimeOps, build_dlr_rf
+            rf = build_dlr_rf(lam, eps)
+            it = ImTimeOps(lam, rf).it
+        else:
+            raise TypeError("DiagramEvaluator(hyb_poles, hyb_coeffs, tau_mesh, atom_diag) or "
+                            "DiagramEvaluator(beta, Lambda, eps, hyb_poles, hyb_coeffs, Fq)")
+        self._setup(float(beta), float(lam), float(eps), np.asarray(rf, float), np.asarray(it, float),
+                    hyb_poles, hyb_coeffs, Fq, device)
+
+    @classmethod
+    def from_arrays(cls, beta, lam, eps, rf, it, hyb_poles, hyb_coeffs, Fq, device=0):
+        self = cls.__new__(cls)
+        self._setup(float(beta), float(lam), float(eps), np.asarray(rf, float), np.asarray(it, float),
+                    hyb_poles, hyb_coeffs, Fq, device)
+        return self
+
+    def _setup(self, beta, lam, eps, rf, it, hyb_poles, hyb_coeffs, Fq, device):
+        L = _lib.lib()
+        self._ctx = ctypes.c_void_p()
+        _lib.check(L.xca_ctx_create(int(device), ctypes.byref(self._ctx)))
+        self.beta = beta
+        self.r = len(rf)
+        self.rf = np.ascontiguousarray(rf, dtype=float)
+        self.it = np.ascontiguousarray(it, dtype=float)
+        poles = np.ascontiguousarray(hyb_poles, dtype=float)
+        coeffs = np.ascontiguousarray(hyb_coeffs, dtype=np.complex128)
+        n = len(Fq.sym_set_labels)
+        if coeffs.shape != (len(poles), n, n):
+            raise ValueError(f"DiagramEvaluator: hyb_coeffs must have shape (p, n, n) with p = {len(poles)} and n = {n}, "
+                             f"got {coeffs.shape}")
+        self.n = n
+        self.q = int(Fq.sym_set_labels.max()) + 1
+        self.dims = np.ascontiguousarray(Fq.dims, dtype=np.int32)
+        self.Nmax = int(self.dims.max())
+        self.p = len(poles)
+        self.Fq = Fq
+        fdata, fddata = Fq.packed()
+        self._keep = (poles, coeffs, fdata, fddata)
+        _lib.check(L.xca_evaluator_setup(self._ctx, beta, lam, eps, self.r, _lib.as_dp(self.rf), _lib.as_dp(self.it),
+                                         self.p, _lib.as_dp(poles), _lib.as_dp(coeffs.view(np.float64)), n,
+                                         _lib.as_lp(Fq.sym_set_labels), len(self.dims), _lib.as_ip(self.dims),
+                                         _lib.as_ip(Fq.F_index), _lib.as_dp(fdata), _lib.as_ip(Fq.Fd_index), _lib.as_dp(fddata)))
+        nd = ctypes.c_long()
+        rr = ctypes.c_int()
+        _lib.check(L.xca_slab_info(self._ctx, ctypes.byref(nd), ctypes.byref(rr)))
+        self.slab = nd.value
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx and _lib._lib is not None:
+            _lib._lib.xca_ctx_destroy(ctx)
+            self._ctx = None
+
+    # ---------------------------------------------------------------- packing
+    def pack(self, G):
+        blocks = _blocks_of(G)
+        if len(blocks) != len(self.dims):
+            raise ValueError(f"expected {len(self.dims)} blocks, got {len(blocks)}")
+        for g, d in zip(blocks, self.dims):
+            if g.shape != (self.r, d, d):
+                raise ValueError(f"block of shape {g.shape}, expected {(self.r, d, d)}")
+        return np.ascontiguousarray(np.concatenate([np.asarray(g, np.complex128).ravel() for g in blocks]))
+
+    def unpack(self, flat):
+        out, off = [], 0
+        for d in self.dims:
+            sz = self.r * d * d
+            out.append(flat[off:off + sz].reshape(self.r, d, d).copy())
+            off += sz
+        return out
+
+    @staticmethod
+    def _topo(topology):
+        t = np.ascontiguousarray(np.asarray(topology, dtype=np.int32).reshape(-1, 2))
+        return t, t.shape[0]
+
+    # ---------------------------------------------------------------- reference API
+    def get_num_self_energy_backbones(self, topology):
+        t, m = self._topo(topology)
+        out = ctypes.c_long()
+        _lib.check(_lib.lib().xca_num_self_energy_backbones(self._ctx, m, _lib.as_ip(t), ctypes.byref(out)))
+        return out.value
+
+    def get_num_single_ptcle_gf_backbones(self, topology):
+        t, m = self._topo(topology)
+        out = ctypes.c_long()
+        _lib.check(_lib.lib().xca_num_single_ptcle_gf_backbones(self._ctx, m, _lib.as_ip(t), ctypes.byref(out)))
+        return out.value
+
+    def compute_self_energy(self, G_ppsc, topology, f_ix=None):
+        """Sigma contribution of one topology (all flat indices, one, or a list), bsb.cpp:369-459."""
+        t, m = self._topo(topology)
+        g = self.pack(G_ppsc)
+        out = np.zeros_like(g)
+        if f_ix is None:
+            fp, nf = None, 0
+        else:
+            fix = np.ascontiguousarray(np.atleast_1d(f_ix), dtype=np.int64)
+            fp, nf = _lib.as_lp(fix), len(fix)
+        _lib.check(_lib.lib().xca_compute_self_energy(self._ctx, _lib.as_dp(g.view(np.float64)), m, _lib.as_ip(t), fp, nf,
+                                                      _lib.as_dp(out.view(np.float64))))
+        return self.unpack(out)
+
+    def self_energy_items(self, G_ppsc, topology, max_rows=None):
+        """Valid (f_ix, b_ix, p_kap, ind_path...) items of find_path_self_energy in flat-index order."""
+        t, m = self._topo(topology)
+        g = self.pack(G_ppsc)
+        n = ctypes.c_long()
+        L = _lib.lib()
+        _lib.check(L.xca_self_energy_items(self._ctx, _lib.as_dp(g.view(np.float64)), m, _lib.as_ip(t), None, 0, ctypes.byref(n)))
+        rows_n = n.value if max_rows is None else min(n.value, max_rows)
+        rows = np.zeros((max(rows_n, 1), 3 + 2 * m - 1), np.int64)
+        _lib.check(L.xca_self_energy_items(self._ctx, _lib.as_dp(g.view(np.float64)), m, _lib.as_ip(t), _lib.as_lp(rows),
+                                           rows_n, ctypes.byref(n)))
+        return rows[:rows_n]
+
+    # ---------------------------------------------------------------- device-resident use
+    def device_buffer(self, slot, n_doubles):
+        ptr = ctypes.POINTER(ctypes.c_double)()
+        _lib.check(_lib.lib().xca_device_buffer(self._ctx, int(slot), int(n_doubles) * 8, ctypes.byref(ptr)))
+        return ctypes.cast(ptr, ctypes.c_void_p).value
+
+    def to_device(self, dev_ptr, host_real):
+        a = np.ascontiguousarray(host_real, dtype=np.float64)
+        _lib.check(_lib.lib().xca_copy_to_device(self._ctx, ctypes.c_void_p(dev_ptr), _lib.as_dp(a), a.size))
+
+    def to_host(self, dev_ptr, n_doubles):
+        a = np.zeros(n_doubles)
+        _lib.check(_lib.lib().xca_copy_to_host(self._ctx, _lib.as_dp(a), ctypes.c_void_p(dev_ptr), a.size))
+        return a
+
+    def compute_self_energy_device(self, G_dev, topology, scale, Sigma_dev):
+        t, m = self._topo(topology)
+        _lib.check(_lib.lib().xca_compute_self_energy_device(self._ctx, ctypes.c_void_p(G_dev), m, _lib.as_ip(t), float(scale),
+                                                             ctypes.c_void_p(Sigma_dev)))
+
+    def synchronize(self):
+        _lib.check(_lib.lib().xca_synchronize(self._ctx))
+
+    def kernel_launches(self):
+        out = ctypes.c_long()
+        _lib.check(_lib.lib().xca_kernel_launches(self._ctx, ctypes.byref(out)))
+        return out.value
