@@ -1,0 +1,280 @@
+"""Benchmark: TCA pseudo-particle self-energy evaluations per second on the two-orbital
+Hubbard-Kanamori model (4 spin-orbitals, 9 (N_up, N_dn) blocks of size <= 4, U = 4, J = 0.5,
+U' = 3, half filling mu = 4.75, beta = 20, DLR Lambda = 200, eps = 1e-12, diagonal Bethe
+hybridization t = 1 fitted on the DLR poles, fixed seeded G_pp from numpy default_rng(0)).
+
+One step = one full Sigma evaluation: orders 1..3, every connected topology, every flat index,
+every block, accumulated with the reference's signs (python/triqs_xca/block_sparse_solver.py:597-640).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl xca|reference]
+
+Under torchrun (N > 1) every rank evaluates an interleaved shard of the work units of each topology
+and the partial Sigma slabs are summed with one NCCL all-reduce per step (strong scaling).
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "TCA Sigma(tau) evals/s (FP64 plain)"
+UNIT = "evals/s"
+CONFIG_NAME = "kanamori_2orb_beta20_L200_eps1e-12_TCA"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="xca", choices=["xca", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def topologies(max_order=3):
+    from xca_b200.diag import all_connected_pairings
+    out = []
+    for order in range(1, max_order + 1):
+        for sign, topo in all_connected_pairings(order):
+            # Sigma_order += (-1)^order * parity * (-1)^(order+1) * compute_self_energy
+            out.append((order, np.array(topo, np.int32), float((-1) ** order * sign * (-1) ** (order + 1))))
+    return out
+
+
+def build_model():
+    from xca_b200 import models
+    from xca_b200.pycppdlr import ImTimeOps, build_dlr_rf
+    rf = build_dlr_rf(200.0, 1e-12)
+    it = ImTimeOps(200.0, rf).get_itnodes()
+    m = models.kanamori_2orb(rf, it)
+    G = models.seeded_G(m, 0)
+    return m, G
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_sigma_rate(m, G, seconds, nthreads=0):
+    """Oracle (CPU restatement) timed on a bounded random sample of flat indices of every topology;
+    returns (evals/s extrapolated to the full evaluation, threads used, sample description)."""
+    from oracle import oracle as O
+    d = O.Dlr(m.lam, m.eps, rf=m.rf, it=m.it)
+    ev = O.Evaluator(d, m.beta, m.hyb_poles, m.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
+    topos = topologies()
+    rng = np.random.default_rng(7)
+    nmax = [ev.num_self_energy_backbones(t) for _, t, _ in topos]
+    per_topo = seconds / len(topos)
+    total_time = 0.0
+    sampled = 0
+    for (_, t, _), nm in zip(topos, nmax):
+        k = min(nm, 64)
+        while True:
+            fix = np.sort(rng.choice(nm, size=k, replace=False))
+            t0 = time.perf_counter()
+            ev.compute_self_energy(G, t, f_ix=fix, nthreads=nthreads)
+            dt = time.perf_counter() - t0
+            if dt > 0.2 * per_topo or k == nm:
+                break
+            k = min(nm, max(k * 2, int(k * 0.5 * per_topo / max(dt, 1e-6))))
+        total_time += dt * nm / k
+        sampled += k
+    threads = nthreads or int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    return 1.0 / total_time, threads, f"{sampled} random flat indices over {len(topos)} topologies, extrapolated to {sum(nmax)}"
+
+
+def run_reference(args, rank):
+    """--impl reference: the CPU restatement of the reference's path on the host cores."""
+    if rank != 0:
+        return
+    m, G = build_model()
+    vals = []
+    for _ in range(args.warmup):
+        cpu_sigma_rate(m, G, min(args.cpu_seconds, 5.0) / 2)
+    for _ in range(args.steps):
+        v, cores, sample = cpu_sigma_rate(m, G, args.cpu_seconds / max(args.steps, 1))
+        vals.append(v)
+    v = float(np.median(vals))
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "c128",
+           "data": "synthetic", "impl": "reference",
+           "config": {"workload": CONFIG_NAME, "l2": "inputs < L2; CPU run"},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from xca_b200.block_sparse import BlockOpSymQuartet, DiagramEvaluator
+    m, G = build_model()
+    Fq = BlockOpSymQuartet(m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks, m.dims)
+    ev = DiagramEvaluator.from_arrays(m.beta, m.lam, m.eps, m.rf, m.it, m.hyb_poles, m.hyb_coeffs, Fq, device=local)
+    topos = topologies()
+    dev = torch.device("cuda", local)
+    greal = np.concatenate([g.real.ravel() for g in G])
+    G_t = torch.tensor(greal, dtype=torch.float64, device=dev)
+    S_t = torch.zeros(ev.slab, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    def step():
+        ev.zero_device(S_t.data_ptr(), ev.slab)
+        for _, t, fac in topos:
+            ev.compute_self_energy_device_shard(G_t.data_ptr(), t, fac, S_t.data_ptr(), rank, world)
+        if world > 1:
+            ev.synchronize()
+            dist.all_reduce(S_t)
+            torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    ev.synchronize()
+    # algorithmic work of one step
+    alg_flops, items = 0.0, 0
+    for _, t, _ in topos:
+        f, n = ev.self_energy_flops(G, t)
+        alg_flops += f
+        items += n
+    launches0 = ev.kernel_launches()
+    clocks = ClockSampler(local)
+    ev.profile(True)
+    ev.profile(True)  # reset counters
+    step_ms = []
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        ev.flush_l2(256 << 20)  # 256 MiB write: evicts the 126 MB L2 between timed steps
+        ev.event_record(0)
+        step()
+        ev.event_record(1)
+        step_ms.append(ev.event_elapsed(0, 1))
+    ev.synchronize()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sigma_ms, sigma_launches = ev.profile(False)
+    clk = clocks.stop()
+    launches = ev.kernel_launches() - launches0 - args.steps  # minus the L2 flushes
+    t_step = float(np.sum(step_ms)) / args.steps
+    if dist is not None:
+        tt = torch.tensor([t_step], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step = float(tt.item())
+    value = 1000.0 / t_step
+
+    # end to end through the public host API: host G in, host Sigma out, every step (rank 0 only)
+    e2e = None
+    if rank == 0:
+        def host_eval():
+            acc = [np.zeros_like(g) for g in G]
+            for _, t, fac in topos:
+                part = ev.compute_self_energy(G, t)
+                for b in range(len(acc)):
+                    acc[b] += fac * part[b]
+            return acc
+        host_eval()
+        t0 = time.perf_counter()
+        ne = max(1, min(args.steps, 3))
+        for _ in range(ne):
+            host_eval()
+        te = (time.perf_counter() - t0) / ne
+        e2e = {"value": 1.0 / te, "unit": UNIT, "h2d_bytes_per_step": int(len(topos) * ev.slab * 8),
+               "d2h_bytes_per_step": int(len(topos) * ev.slab * 8)}
+
+    peak = ev.fp64_fma_peak()
+    kernel_s = sigma_ms * 1e-3 / max(args.steps, 1)
+    achieved = alg_flops / world / kernel_s / 1e12 if kernel_s > 0 else None
+    traffic = None
+    prof_path = os.path.join(ROOT, "profiles", "sigma_items_kernel_kanamori_2orb.json")
+    if os.path.exists(prof_path):
+        try:
+            traffic = json.load(open(prof_path)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_sigma_rate(m, G, args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": t_step, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic",
+               "config": {"workload": CONFIG_NAME, "r": int(ev.r), "poles": int(ev.p), "items_per_step": int(items),
+                          "alg_gflop_per_step": alg_flops / 1e9, "l2": "flushed (256 MiB write) before every timed step"},
+               "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                            "kernel": "sigma_items_kernel",
+                            "peak_source": "FP64 FMA throughput measured by xca_fp64_fma_probe on this GPU",
+                            "kernel_ms_per_step": sigma_ms / max(args.steps, 1), "launches_per_step": sigma_launches / max(args.steps, 1)},
+               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

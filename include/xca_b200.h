@@ -58,8 +58,8 @@ int xca_ctx_destroy(xca_ctx *ctx);
  * evaluator multiplies them by beta; coefficients p x n x n complex), the symmetry-set labels of the
  * n orbitals and the field operators as BlockOpSymSet slabs (c++/triqs_xca/block_sparse.hpp:181-200):
  * F_index[s * n_blocks + b] is the target block of set s acting on block b (-1: none); F_data packs,
- * in (s, b) order over present columns, a (q_s, d_target, d_b) complex slab.  The barred operators
- * of BlockOpSymQuartet (c++/triqs_xca/block_sparse.cpp:496-577) are built on the device.
+ * in (s, b) order over present columns, a (q_s, d_target, d_b) complex slab.  The library forms the
+ * barred operators of BlockOpSymQuartet (c++/triqs_xca/block_sparse.cpp:496-577) and uploads them.
  * Validation as check_sym_set_block_diagonal (c++/triqs_xca/block_sparse.cpp:443-492). */
 int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, int r, const double *rf, const double *it,
                         int p, const double *hyb_poles, const double *hyb_coeffs, int n, const long *sym_set_labels,
@@ -85,11 +85,42 @@ int xca_compute_self_energy(xca_ctx *ctx, const double *G, int m, const int *top
 int xca_compute_self_energy_device(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
                                    double *Sigma_dev);
 
+/* One shard of compute_self_energy_device: the work units u of the topology with u % n_shards == shard
+ * (units are runs of pole tuples of one path class).  Summing the shards of every rank (an all-reduce)
+ * gives the full result; replaces the flat-index scatter of python/triqs_xca/block_sparse_solver.py:29-33
+ * and 629-640 whose partial results are then all-reduced (:638). */
+int xca_compute_self_energy_device_shard(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
+                                         double *Sigma_dev, int shard, int n_shards);
+
+/* Zero n_doubles of device memory on the context's stream. */
+int xca_zero_device(xca_ctx *ctx, double *dev, long n_doubles);
+
 /* Number of valid (flat index, block, symmetry set) items of find_path_self_energy
  * (c++/triqs_xca/block_sparse_backbone.cpp:229-314) for this G and topology, and optionally the rows
  * (f_ix, b_ix, p_kap, ind_path[0..2m-2]) of the first max_rows of them in flat-index order. */
 int xca_self_energy_items(xca_ctx *ctx, const double *G, int m, const int *topology, long *rows, long max_rows,
                           long *n_items);
+
+/* Algorithmic real-FP64 flop count and number of items of compute_self_energy(G, topology) over every
+ * flat index, from the fixed per-item cost model (vertex 2 r d' d c [+ r d' c with a K factor]; edge
+ * r d^2 #K + 2 r^2 (d^2 + d c) + 2 [r^2 (d^2 + 2 d c) + 3 r d^2 c]; zero vertex
+ * |S| 2 r d_v d_1 d_0 + |S|^2 2 r d_v d_0 + |S| 2 r d_v+1 d_v d_0; accumulation r d_out d_0).
+ * No counterpart in the reference (measurement support). */
+int xca_self_energy_flops(xca_ctx *ctx, const double *G, int m, const int *topology, double *alg_flops, long *n_items);
+
+/* Measurement support (no counterpart in the reference): enable/disable CUDA-event timing of every
+ * Sigma kernel launch; returns (and resets) the summed device time and launch count recorded so far. */
+int xca_profile(xca_ctx *ctx, int enable, double *sigma_ms, long *sigma_launches);
+
+/* Measurement support: record CUDA event `slot` (0..7) on the context's stream; elapsed ms between two. */
+int xca_event_record(xca_ctx *ctx, int slot);
+int xca_event_elapsed(xca_ctx *ctx, int slot_a, int slot_b, double *ms);
+
+/* Measurement support: overwrite `bytes` of scratch device memory on the context's stream (L2 flush). */
+int xca_flush_l2(xca_ctx *ctx, long bytes);
+
+/* Measurement support: FP64 fused-multiply-add throughput of this device in TFLOP/s (2 flops per FMA). */
+int xca_fp64_fma_probe(xca_ctx *ctx, double *tflops);
 
 /* Size in bytes of the packed real slab of the evaluator's blocks, and its rank r. */
 int xca_slab_info(xca_ctx *ctx, long *n_doubles, int *r);

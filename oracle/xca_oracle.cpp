@@ -67,26 +67,27 @@ void lu_factor(std::vector<T> &a, int n, std::vector<int> &piv) {
     }
   }
 }
-// Solve A X = B in place, B is n x nrhs row-major.
+// Solve A X = B in place, B is n x nrhs row-major, with the LU factors of lu_factor.  The
+// substitutions run in the column order of the reference BLAS dtrsm that LAPACK getrs calls: forward,
+// for k ascending, b_i -= L_ik b_k (i > k); backward, for k descending, b_k /= U_kk then
+// b_i -= U_ik b_k (i < k).
 template <class T, class U>
 void lu_solve(const std::vector<T> &lu, int n, const std::vector<int> &piv, U *b, long nrhs) {
   for (int k = 0; k < n; ++k)
     if (piv[k] != k)
       for (long j = 0; j < nrhs; ++j) std::swap(b[(size_t)k * nrhs + j], b[(size_t)piv[k] * nrhs + j]);
-  for (int i = 1; i < n; ++i)
-    for (int k = 0; k < i; ++k) {
+  for (int k = 0; k < n; ++k)
+    for (int i = k + 1; i < n; ++i) {
       T f = lu[(size_t)i * n + k];
-      if (f == T(0)) continue;
       for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] -= f * b[(size_t)k * nrhs + j];
     }
-  for (int i = n - 1; i >= 0; --i) {
-    for (int k = i + 1; k < n; ++k) {
+  for (int k = n - 1; k >= 0; --k) {
+    T d = lu[(size_t)k * n + k];
+    for (long j = 0; j < nrhs; ++j) b[(size_t)k * nrhs + j] /= d;
+    for (int i = 0; i < k; ++i) {
       T f = lu[(size_t)i * n + k];
-      if (f == T(0)) continue;
       for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] -= f * b[(size_t)k * nrhs + j];
     }
-    T d = lu[(size_t)i * n + i];
-    for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] /= d;
   }
 }
 
@@ -145,7 +146,7 @@ struct Dlr {
   // cppdlr imtime_ops::convolve(beta, fc, gc, time_order) for matrix-valued expansions:
   // fc (r, a, b), gc (r, b, c) -> values h (r, a, c) of int f(tau - tau') g(tau') dtau'.
   void convolve(double beta, int a, int b, int c, const cd *fc, const cd *gc, bool time_order, cd *h) const {
-    std::vector<cd> ft((size_t)r * a * b, 0.0), gt((size_t)r * b * c, 0.0), q((size_t)r * a * c, 0.0);
+    std::vector<cd> ft((size_t)r * a * b, 0.0), gt((size_t)r * b * c, 0.0);
     for (int l = 0; l < r; ++l)
       for (int k = 0; k < r; ++k) {
         if (k == l) continue;
@@ -155,10 +156,10 @@ struct Dlr {
       }
     for (int i = 0; i < r; ++i)
       for (int x = 0; x < a * c; ++x) h[(size_t)i * a * c + x] = 0;
+    std::vector<cd> Q((size_t)r * a * c, 0.0), P((size_t)r * a * c, 0.0);
     for (int l = 0; l < r; ++l) {
       const cd *f = fc + (size_t)l * a * b, *g = gc + (size_t)l * b * c;
       const cd *fh = ft.data() + (size_t)l * a * b, *gh = gt.data() + (size_t)l * b * c;
-      std::vector<cd> Q((size_t)a * c, 0.0), P((size_t)a * c, 0.0);
       for (int x = 0; x < a; ++x)
         for (int z = 0; z < c; ++z) {
           cd sq = 0, sp = 0;
@@ -166,18 +167,32 @@ struct Dlr {
             sq += fh[x * b + y] * g[y * c + z] + f[x * b + y] * gh[y * c + z];
             sp += f[x * b + y] * g[y * c + z];
           }
-          Q[x * c + z] = sq;
-          P[x * c + z] = sp;
+          Q[(size_t)l * a * c + x * c + z] = sq;
+          P[(size_t)l * a * c + x * c + z] = sp;
         }
-      // With the signed kernel K: time-ordered h = beta sum_l K_l(t)[Q_l + t K_l(0) P_l];
-      // full h = -beta sum_l K_l(t)[Q_l + (t + K_l(1)) P_l] (Q built with weights 1 / (om_k - om_l)).
-      for (int i = 0; i < r; ++i) {
-        double kil = cf2it[(size_t)i * r + l];
-        double wd = time_order ? tabs[i] * k0[l] : tabs[i] + k1[l];
-        double sg = time_order ? beta : -beta;
-        cd *hi = h + (size_t)i * a * c;
-        for (int x = 0; x < a * c; ++x) hi[x] += sg * kil * (Q[x] + wd * P[x]);
-      }
+    }
+    if (time_order) {
+      // h(t_i) = h1_i + t_i h2_i with h1_i = sum_l (beta K_il) Q_l and h2_i = sum_l (beta K_il) (K_l(0) P_l),
+      // each sum from zero in ascending l: beta sum_l K_l(t_i) [Q_l + t_i K_l(0) P_l] for the signed kernel.
+      for (int i = 0; i < r; ++i)
+        for (int x = 0; x < a * c; ++x) {
+          cd h1 = 0, h2 = 0;
+          for (int l = 0; l < r; ++l) {
+            double bk = beta * cf2it[(size_t)i * r + l];
+            h1 += bk * Q[(size_t)l * a * c + x];
+            h2 += bk * (k0[l] * P[(size_t)l * a * c + x]);
+          }
+          h[(size_t)i * a * c + x] = h1 + tabs[i] * h2;
+        }
+    } else {
+      // full (fermionic) convolution: h = -beta sum_l K_l(t)[Q_l + (t + K_l(1)) P_l] (weights 1 / (om_k - om_l))
+      for (int l = 0; l < r; ++l)
+        for (int i = 0; i < r; ++i) {
+          double kil = cf2it[(size_t)i * r + l];
+          double wd = tabs[i] + k1[l];
+          cd *hi = h + (size_t)i * a * c;
+          for (int x = 0; x < a * c; ++x) hi[x] += -beta * kil * (Q[(size_t)l * a * c + x] + wd * P[(size_t)l * a * c + x]);
+        }
     }
   }
   // cppdlr imtime_ops::convmat_inplace(M, beta, Fermion, fc, time_order) (dlr_dyson_ppsc.hpp:149):

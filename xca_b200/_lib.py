@@ -40,7 +40,15 @@ SIGNATURES = {
     "xca_num_single_ptcle_gf_backbones": [P, I, ip, lp],
     "xca_compute_self_energy": [P, dp, I, ip, lp, L, dp],
     "xca_compute_self_energy_device": [P, P, I, ip, D, P],
+    "xca_compute_self_energy_device_shard": [P, P, I, ip, D, P, I, I],
+    "xca_zero_device": [P, P, L],
     "xca_self_energy_items": [P, dp, I, ip, lp, L, lp],
+    "xca_self_energy_flops": [P, dp, I, ip, dp, lp],
+    "xca_profile": [P, I, dp, lp],
+    "xca_event_record": [P, I],
+    "xca_event_elapsed": [P, I, I, dp],
+    "xca_flush_l2": [P, L],
+    "xca_fp64_fma_probe": [P, dp],
     "xca_slab_info": [P, lp, ip],
     "xca_device_buffer": [P, I, L, dpp],
     "xca_copy_to_device": [P, P, dp, L],

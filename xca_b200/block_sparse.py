@@ -211,6 +211,49 @@ class DiagramEvaluator:
         _lib.check(_lib.lib().xca_compute_self_energy_device(self._ctx, ctypes.c_void_p(G_dev), m, _lib.as_ip(t), float(scale),
                                                              ctypes.c_void_p(Sigma_dev)))
 
+    def compute_self_energy_device_shard(self, G_dev, topology, scale, Sigma_dev, shard, n_shards):
+        t, m = self._topo(topology)
+        _lib.check(_lib.lib().xca_compute_self_energy_device_shard(self._ctx, ctypes.c_void_p(G_dev), m, _lib.as_ip(t),
+                                                                   float(scale), ctypes.c_void_p(Sigma_dev), int(shard),
+                                                                   int(n_shards)))
+
+    def zero_device(self, dev_ptr, n_doubles):
+        _lib.check(_lib.lib().xca_zero_device(self._ctx, ctypes.c_void_p(dev_ptr), int(n_doubles)))
+
+    def self_energy_flops(self, G_ppsc, topology):
+        """(algorithmic real flops, number of items) of one full compute_self_energy(G, topology)."""
+        t, m = self._topo(topology)
+        g = self.pack(G_ppsc)
+        fl = ctypes.c_double()
+        n = ctypes.c_long()
+        _lib.check(_lib.lib().xca_self_energy_flops(self._ctx, _lib.as_dp(g.view(np.float64)), m, _lib.as_ip(t),
+                                                    ctypes.byref(fl), ctypes.byref(n)))
+        return fl.value, n.value
+
+    def profile(self, enable):
+        """Enable/disable per-launch CUDA-event timing; returns (Sigma kernel ms, launches) recorded so far."""
+        ms = ctypes.c_double()
+        n = ctypes.c_long()
+        _lib.check(_lib.lib().xca_profile(self._ctx, int(bool(enable)), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def event_record(self, slot):
+        _lib.check(_lib.lib().xca_event_record(self._ctx, int(slot)))
+
+    def event_elapsed(self, a, b):
+        ms = ctypes.c_double()
+        _lib.check(_lib.lib().xca_event_elapsed(self._ctx, int(a), int(b), ctypes.byref(ms)))
+        return ms.value
+
+    def fp64_fma_peak(self):
+        """Measured FP64 FMA throughput of the device in TFLOP/s."""
+        out = ctypes.c_double()
+        _lib.check(_lib.lib().xca_fp64_fma_probe(self._ctx, ctypes.byref(out)))
+        return out.value
+
+    def flush_l2(self, nbytes=256 << 20):
+        _lib.check(_lib.lib().xca_flush_l2(self._ctx, int(nbytes)))
+
     def synchronize(self):
         _lib.check(_lib.lib().xca_synchronize(self._ctx))
 

@@ -59,35 +59,109 @@ struct DevBuf {
   }
 };
 
-// -------------------------------------------------------------------------------- Sigma kernel
-// Dynamic shared memory: [LU | W | Kit] (3 r^2 doubles) | piv (r ints, padded) | per-warp NBUF slabs of
-// r * nmax^2 doubles.
-__global__ void __launch_bounds__(256) sigma_items_kernel(DevBasis B, const ClassRec *__restrict__ classes,
-                                                          const WorkUnit *__restrict__ units, int n_units,
-                                                          int *__restrict__ unit_counter, const double *__restrict__ G,
-                                                          double *__restrict__ Sigma, double scale) {
+// -------------------------------------------------------------------------------- Sigma kernels
+// Per-warp item state kept in shared memory for one batch.
+struct ItemState {
+  double scale;          // prefactor * prefactor sign * order / direction sign
+  int lpole[MAXM];       // pole index of line i (i >= 1)
+  int caseA[MAXM];       // line i in case 4(a): K on its end vertices; else 4(b): K on the edges it spans
+  long opoff;            // per-step scratch: operator slab offset of this item
+  long taboff;           // per-step scratch: edge-table offset of this item
+  int kcol;              // per-step scratch: K-table column of the vertex (-1: none), sign in kneg
+  int kneg;
+  int keep;              // 1e-16 guard outcome
+};
+
+// Edge tables: for block b and K signature sig, fc = K^-1 (G_b * prod K) and Ft = W fc.
+// sig 0: no factor; 1 + s p + l: one factor (s = 0: K(t, +beta w_l), 1: K(t, -beta w_l));
+// 1 + 2p + (s1 p + l1) 2p + s2 p + l2: two factors, the lower line's first.
+template <int RP>
+__global__ void __launch_bounds__(128) edge_table_kernel(DevBasis B, const double *__restrict__ G, long n_pairs) {
+  extern __shared__ double smem[];
+  double *sLU = smem;
+  double *sW = sLU + RP * RP;
+  int *sPerm = reinterpret_cast<int *>(sW + RP * RP);
+  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
+    sLU[i] = B.LUp[i];
+    sW[i] = B.Wp[i];
+  }
+  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
+  __syncthreads();
+  const int r = B.r, p = B.p;
+  const int lane = threadIdx.x & 31;
+  const long warp_global = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+  for (long pair = warp_global; pair < n_pairs; pair += nwarps) {
+    const int b = (int)(pair / B.nsig);
+    const int sig = (int)(pair - (long)b * B.nsig);
+    const int d = B.dims[b];
+    const int dd = d * d;
+    int nf = 0, s1 = 0, l1 = 0, s2 = 0, l2 = 0;
+    if (sig >= 1 && sig < 1 + 2 * p) {
+      nf = 1;
+      s1 = (sig - 1) / p;
+      l1 = (sig - 1) - s1 * p;
+    } else if (sig >= 1 + 2 * p) {
+      nf = 2;
+      int q = sig - 1 - 2 * p;
+      int a = q / (2 * p), c = q - a * (2 * p);
+      s1 = a / p; l1 = a - s1 * p;
+      s2 = c / p; l2 = c - s2 * p;
+    }
+    const double *g = G + B.goff[b];
+    double *out = const_cast<double *>(B.tab) + B.tab_off[b] + (long)sig * 2 * r * dd;
+    for (int col = lane; col < dd; col += 32) {
+      double x[RP];
+#pragma unroll
+      for (int i = 0; i < RP; ++i) {
+        int src = sPerm[i];
+        double v = 0.0;
+        if (src >= 0) {
+          v = g[src * dd + col];
+          if (nf >= 1) v = mul(v, (s1 ? B.kitm : B.kitp)[(size_t)src * p + l1]);
+          if (nf >= 2) v = mul(v, (s2 ? B.kitm : B.kitp)[(size_t)src * p + l2]);
+        }
+        x[i] = v;
+      }
+      lu_solve_reg<RP>(sLU, x);
+#pragma unroll
+      for (int i = 0; i < RP; ++i)
+        if (i < r) out[i * dd + col] = x[i];
+      matvec_reg<RP>(sW, x, r, out + (long)r * dd + col, dd);
+    }
+  }
+}
+
+// Dynamic shared memory: LU | W | BK (3 RP^2 doubles) | perm (RP ints) | per warp: 32 item states,
+// NSLAB slab regions of B.region doubles, r * nmax^2 doubles of accumulator.
+template <int RP>
+__global__ void __launch_bounds__(32 * WARPS_MAX) sigma_items_kernel(DevBasis B, const ClassRec *__restrict__ classes,
+                                                                      const WorkUnit *__restrict__ units, int n_units,
+                                                                      int *__restrict__ unit_counter, const double *__restrict__ G,
+                                                                      double *__restrict__ Sigma, double scale, int nmax) {
   extern __shared__ double smem[];
   const int r = B.r, p = B.p, n = B.n;
-  const int r2 = r * r;
   double *sLU = smem;
-  double *sW = sLU + r2;
-  double *sK = sW + r2;
-  int *sPiv = reinterpret_cast<int *>(sK + r2);
-  const int pivpad = (r + 1) / 2;  // doubles occupied by r ints
-  double *warp_base = sK + r2 + pivpad;
-  for (int i = threadIdx.x; i < r2; i += blockDim.x) {
-    sLU[i] = B.LU[i];
-    sW[i] = B.W[i];
-    sK[i] = B.Kit[i];
+  double *sW = sLU + RP * RP;
+  double *sBK = sW + RP * RP;
+  int *sPerm = reinterpret_cast<int *>(sBK + RP * RP);
+  double *warp_area = sBK + RP * RP + (RP + 1) / 2;
+  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
+    sLU[i] = B.LUp[i];
+    sW[i] = B.Wp[i];
+    sBK[i] = B.BKp[i];
   }
-  for (int i = threadIdx.x; i < r; i += blockDim.x) sPiv[i] = B.piv[i];
+  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
   __syncthreads();
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int slab = r * B.nmax * B.nmax;
-  double *bufA = warp_base + (size_t)warp * NBUF * slab;
-  double *bufB = bufA + slab, *bufC = bufB + slab, *bufD = bufC + slab, *bufE = bufD + slab, *acc = bufE + slab;
+  const size_t items_bytes = ((sizeof(ItemState) * 32 + 15) / 16) * 16;
+  const size_t warp_doubles = items_bytes / 8 + (size_t)NSLAB * B.region + (size_t)r * nmax * nmax;
+  double *wbase = warp_area + (size_t)warp * warp_doubles;
+  ItemState *ist = reinterpret_cast<ItemState *>(wbase);
+  double *slabs = wbase + items_bytes / 8;
+  double *acc = slabs + (size_t)NSLAB * B.region;
 
   while (true) {
     int u = 0;
@@ -95,159 +169,207 @@ __global__ void __launch_bounds__(256) sigma_items_kernel(DevBasis B, const Clas
     u = __shfl_sync(0xffffffffu, u, 0);
     if (u >= n_units) break;
     const WorkUnit wu = units[u];
-    const ClassRec &C = classes[wu.cls];
+    const ClassRec C = classes[wu.cls];
     const int m = C.m, vct0 = C.vct0;
     const int d0 = C.bdims[0], d1 = C.bdims[1];
     const int dout = C.bdims[2 * m];
+    const int cap = C.batch;  // items per lockstep batch; cap * (largest d * c of the chain) <= 32
+    const int slab = r * C.dcmax;  // item j's T / X / Y slabs are j-strided within each of the three regions
+    double *regT = slabs, *regX = slabs + B.region, *regY = slabs + 2 * (size_t)B.region;
     for (int i = lane; i < r * dout * d0; i += 32) acc[i] = 0.0;
     bool any = false;
 
-    for (int it = 0; it < wu.count; ++it) {
-      int p_ix = wu.first + it;
-      // ---- decode the pole tuple (Backbone::set_pole_inds, backbone.cpp:86-150)
-      int lpole[MAXM] = {0, 0, 0};
-      int caseA[MAXM] = {0, 0, 0};
-      {
-        int q = p_ix;
+    for (int first = 0; first < wu.count; first += cap) {
+      const int nb_items = min(cap, wu.count - first);
+      // ---- decode the pole tuples (Backbone::set_pole_inds, backbone.cpp:86-150)
+      if (lane < nb_items) {
+        ItemState &S = ist[lane];
+        int q = wu.first + first + lane;
+        S.lpole[0] = 0;
+        S.caseA[0] = 0;
+        for (int i = 1; i < MAXM; ++i) { S.lpole[i] = 0; S.caseA[i] = 0; }
         for (int i = 1; i < m; ++i) {
-          lpole[i] = q % p;
+          S.lpole[i] = q % p;
           q /= p;
         }
+        double pf = 1.0;
+        int psign = 1;
+        for (int i = 1; i < m; ++i) {
+          int fwd = (C.fbmask >> i) & 1;
+          double w = B.polesb[S.lpole[i]];
+          S.caseA[i] = fwd ? (w <= 0.0) : (w >= 0.0);
+          if (!fwd) psign = -psign;
+          int row = S.caseA[i] ? (fwd ? 1 : 0) : (fwd ? 0 : 1);
+          int ex = S.caseA[i] ? 1 : C.lb[i] - C.la[i] - 1;
+          if (ex != 0) pf = mul(pf, B.kpow[((size_t)row * p + S.lpole[i]) * (MAXE + 1) + ex]);
+        }
+        int dsign = (m % 2 == 0) ? -1 : 1;
+        if (!(C.fbmask & 1)) dsign = -dsign;
+        S.scale = mul(pf, (double)(psign * dsign));
       }
-      double pf = 1.0;
-      int psign = 1;
-      for (int i = 1; i < m; ++i) {
-        int fwd = (C.fbmask >> i) & 1;
-        double w = B.polesb[lpole[i]];
-        caseA[i] = fwd ? (w <= 0.0) : (w >= 0.0);
-        if (!fwd) psign = -psign;
-        // prefactor *= pow(K^{+-}_l(0), -exp) in line order (Hybridization::multiply_kernels_prefactor)
-        int row = caseA[i] ? (fwd ? 1 : 0) : (fwd ? 0 : 1);
-        int ex = caseA[i] ? 1 : C.lb[i] - C.la[i] - 1;
-        if (ex != 0) pf = mul(pf, B.kpow[((size_t)row * p + lpole[i]) * (MAXE + 1) + ex]);
-      }
-      int dsign = (m % 2 == 0) ? -1 : 1;
-      if (!(C.fbmask & 1)) dsign = -dsign;
-      const double total_scale = mul(pf, (double)(psign * dsign));
-
-      // ---- T := G[ind_path[0]]  (d1 x d1)
-      double *T = bufA, *S = bufB;
+      // T := G[ind_path[0]] (d1 x d1) for every item
       {
         const double *g = G + B.goff[C.ind_path[0]];
-        for (int i = lane; i < r * d1 * d1; i += 32) T[i] = g[i];
+        const int sz = r * d1 * d1;
+        for (int idx = lane; idx < nb_items * sz; idx += 32) {
+          int j = idx / sz;
+          regT[(size_t)j * slab + (idx - j * sz)] = g[idx - j * sz];
+        }
       }
       __syncwarp();
+      double *T = regT, *X = regX, *Y = regY;
 
-      // vertex multiply: T(t) <- k(t) * F * T(t) (multiply_left_vertex)
+      // ---- vertex v: T(t) <- k(t) F T(t)  (multiply_left_vertex)
       auto vertex = [&](int v, int ncol) {
         const int line = C.vline[v];
-        const int l = lpole[line];
         const int b = C.ind_path[v - 1];
         const int dv = C.bdims[v], dvp = C.bdims[v + 1];
         const int s = C.vset[v], qo = C.vqo[v];
-        const double *F;
-        switch (C.vkind[v]) {
-          case 0: F = B.ops + B.F_off[s * B.nb + b] + (size_t)qo * dvp * dv; break;
-          case 1: F = B.ops + B.Fd_off[s * B.nb + b] + (size_t)qo * dvp * dv; break;
-          case 2: F = B.ops + B.Fb_off[s * B.nb + b] + ((size_t)qo * p + l) * dvp * dv; break;
-          default: F = B.ops + B.Fdb_off[s * B.nb + b] + ((size_t)qo * p + l) * dvp * dv; break;
-        }
-        // K factor on this vertex: lines in case A carry K on both endpoints
-        const double *kcol = nullptr;
-        if (line > 0 && caseA[line]) {
-          int fwd = (C.fbmask >> line) & 1;
-          int ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
-          kcol = (ks > 0 ? B.kitp : B.kitm) + l;
-        }
-        const int tot = r * dvp * ncol;
-        for (int idx = lane; idx < tot; idx += 32) {
-          int t = idx / (dvp * ncol);
-          int rem = idx - t * dvp * ncol;
-          int x = rem / ncol, z = rem - x * ncol;
-          const double *Tt = T + t * dv * ncol;
-          double sacc = 0.0;
-          for (int y = 0; y < dv; ++y) sacc = add(sacc, mul(F[x * dv + y], Tt[y * ncol + z]));
-          if (kcol) sacc = mul(sacc, kcol[(size_t)t * p]);
-          S[idx] = sacc;
+        if (lane < nb_items) {
+          ItemState &S = ist[lane];
+          const int l = S.lpole[line];
+          long off;
+          switch (C.vkind[v]) {
+            case 0: off = B.F_off[s * B.nb + b] + (long)qo * dvp * dv; break;
+            case 1: off = B.Fd_off[s * B.nb + b] + (long)qo * dvp * dv; break;
+            case 2: off = B.Fb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
+            default: off = B.Fdb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
+          }
+          S.opoff = off;
+          S.kcol = -1;
+          if (line > 0 && S.caseA[line]) {
+            int fwd = (C.fbmask >> line) & 1;
+            int ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
+            S.kcol = l;
+            S.kneg = ks < 0;
+          }
         }
         __syncwarp();
-        double *tmp = T; T = S; S = tmp;
+        const int per = r * dvp * ncol;
+        for (int idx = lane; idx < nb_items * per; idx += 32) {
+          int j = idx / per;
+          int rem = idx - j * per;
+          int t = rem / (dvp * ncol);
+          int r2 = rem - t * dvp * ncol;
+          int x = r2 / ncol, z = r2 - x * ncol;
+          const ItemState &S = ist[j];
+          const double *F = B.ops + S.opoff;
+          const double *Tt = T + (size_t)j * slab + t * dv * ncol;
+          double a = 0.0;
+          for (int y = 0; y < dv; ++y) a = add(a, mul(F[x * dv + y], Tt[y * ncol + z]));
+          if (S.kcol >= 0) a = mul(a, (S.kneg ? B.kitm : B.kitp)[(size_t)t * p + S.kcol]);
+          X[(size_t)j * slab + rem] = a;
+        }
+        __syncwarp();
+        double *tmp = T; T = X; X = tmp;
       };
 
-      // edge e: T <- conv(G_b * prod K, T)  (integrate_left_edge + cppdlr time-ordered convolution)
+      // ---- edge e: T <- conv(G_b * prod K, T)  (integrate_left_edge, time-ordered DLR convolution)
       auto edge = [&](int e, int ncol) {
         const int b = C.ind_path[e];
         const int d = C.bdims[e + 1];
-        const double *g = G + B.goff[b];
-        // GK into S with the edge's K factors (lines in case B cover edges la..lb-1)
-        const int dd = d * d;
-        for (int idx = lane; idx < r * dd; idx += 32) {
-          int t = idx / dd;
-          double v = g[idx];
-          for (int i = 1; i < m; ++i) {
-            if (!caseA[i] && e >= C.la[i] && e < C.lb[i]) {
-              int fwd = (C.fbmask >> i) & 1;
-              v = mul(v, (fwd ? B.kitp : B.kitm)[(size_t)t * p + lpole[i]]);
+        const int dd = d * d, dc = d * ncol;
+        if (lane < nb_items) {
+          ItemState &S = ist[lane];
+          int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
+          for (int i = 1; i < m; ++i)
+            if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
+              sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
+              lp[nf] = S.lpole[i];
+              nf++;
+            }
+          long sig = 0;
+          if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
+          if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
+          S.taboff = B.tab_off[b] + sig * 2 * r * dd;
+        }
+        __syncwarp();
+        // (a) gc = K^-1 T (in place, column per lane) and Gt = W gc (into X)
+        for (int cl = lane; cl < nb_items * dc; cl += 32) {
+          const int j = cl / dc, col = cl - j * dc;
+          double *Tj = T + (size_t)j * slab;
+          double x[RP];
+#pragma unroll
+          for (int i = 0; i < RP; ++i) {
+            int src = sPerm[i];
+            x[i] = src >= 0 ? Tj[src * dc + col] : 0.0;
+          }
+          lu_solve_reg<RP>(sLU, x);
+#pragma unroll
+          for (int i = 0; i < RP; ++i)
+            if (i < r) Tj[i * dc + col] = x[i];
+          matvec_reg<RP>(sW, x, r, X + (size_t)j * slab + col, dc);
+        }
+        __syncwarp();
+        // (b) Q_l = Ft_l gc_l + fc_l Gt_l  (into Y)
+        const int per = r * dc;
+        for (int idx = lane; idx < nb_items * per; idx += 32) {
+          int j = idx / per;
+          int rem = idx - j * per;
+          int l = rem / dc;
+          int r2 = rem - l * dc;
+          int x = r2 / ncol, z = r2 - x * ncol;
+          const double *tb = B.tab + ist[j].taboff;
+          const double *fl = tb + l * dd, *ftl = tb + (long)r * dd + l * dd;
+          const double *gl = T + (size_t)j * slab + l * dc, *gtl = X + (size_t)j * slab + l * dc;
+          double a = 0.0;
+          for (int y = 0; y < d; ++y) a = add(a, add(mul(ftl[x * d + y], gl[y * ncol + z]), mul(fl[x * d + y], gtl[y * ncol + z])));
+          Y[(size_t)j * slab + rem] = a;
+        }
+        __syncwarp();
+        // (c) h1 = (beta K) Q  (into X, Gt no longer needed)
+        for (int cl = lane; cl < nb_items * dc; cl += 32) {
+          const int j = cl / dc, col = cl - j * dc;
+          const double *Yj = Y + (size_t)j * slab;
+          double q[RP];
+#pragma unroll
+          for (int i = 0; i < RP; ++i) q[i] = i < r ? Yj[i * dc + col] : 0.0;
+          matvec_reg<RP>(sBK, q, r, X + (size_t)j * slab + col, dc);
+        }
+        __syncwarp();
+        // (d) P'_l = K(0, om_l) (fc_l gc_l)  (into Y)
+        for (int idx = lane; idx < nb_items * per; idx += 32) {
+          int j = idx / per;
+          int rem = idx - j * per;
+          int l = rem / dc;
+          int r2 = rem - l * dc;
+          int x = r2 / ncol, z = r2 - x * ncol;
+          const double *fl = B.tab + ist[j].taboff + l * dd;
+          const double *gl = T + (size_t)j * slab + l * dc;
+          double a = 0.0;
+          for (int y = 0; y < d; ++y) a = add(a, mul(fl[x * d + y], gl[y * ncol + z]));
+          Y[(size_t)j * slab + rem] = mul(B.k0[l], a);
+        }
+        __syncwarp();
+        // (e) h = h1 + t_i (beta K) P'  (into T)
+        for (int cl = lane; cl < nb_items * dc; cl += 32) {
+          const int j = cl / dc, col = cl - j * dc;
+          const double *Yj = Y + (size_t)j * slab;
+          double q[RP];
+#pragma unroll
+          for (int i = 0; i < RP; ++i) q[i] = i < r ? Yj[i * dc + col] : 0.0;
+          double *Tj = T + (size_t)j * slab;
+          const double *h1 = X + (size_t)j * slab;
+          constexpr int CH = 8;
+#pragma unroll 1
+          for (int l0 = 0; l0 < RP; l0 += CH) {
+            if (l0 >= r) break;
+            double a[CH];
+#pragma unroll
+            for (int jj = 0; jj < CH; ++jj) a[jj] = 0.0;
+#pragma unroll
+            for (int k = 0; k < RP; ++k) {
+#pragma unroll
+              for (int jj = 0; jj < CH; ++jj) a[jj] = add(a[jj], mul(sBK[(l0 + jj) * RP + k], q[k]));
+            }
+#pragma unroll
+            for (int jj = 0; jj < CH; ++jj) {
+              int i = l0 + jj;
+              if (i < r) Tj[i * dc + col] = add(h1[i * dc + col], mul(B.tabs[i], a[jj]));
             }
           }
-          S[idx] = v;
         }
         __syncwarp();
-        // coefficients: fc = K^{-1} GK (in S), gc = K^{-1} T (in T)
-        lu_solve_cols(sLU, sPiv, r, S, dd, lane);
-        lu_solve_cols(sLU, sPiv, r, T, d * ncol, lane);
-        __syncwarp();
-        // Hilbert sums: Ft = W fc (bufC/bufD as free scratch), Gt = W gc
-        double *Ft = (S == bufA || T == bufA) ? ((S == bufB || T == bufB) ? bufC : bufB) : bufA;
-        // pick three free slabs among A..E not equal to S or T
-        double *freeb[5] = {bufA, bufB, bufC, bufD, bufE};
-        double *fr[3];
-        int nf = 0;
-        for (int k = 0; k < 5 && nf < 3; ++k)
-          if (freeb[k] != S && freeb[k] != T) fr[nf++] = freeb[k];
-        Ft = fr[0];
-        double *Gt = fr[1], *Q = fr[2];
-        matvec_cols(sW, r, S, Ft, dd, lane);
-        matvec_cols(sW, r, T, Gt, d * ncol, lane);
-        __syncwarp();
-        // Q_l = Ft_l gc_l + fc_l Gt_l
-        const int dc = d * ncol;
-        for (int idx = lane; idx < r * dc; idx += 32) {
-          int l = idx / dc;
-          int rem = idx - l * dc;
-          int x = rem / ncol, z = rem - x * ncol;
-          const double *fl = S + l * dd, *ftl = Ft + l * dd, *gl = T + l * dc, *gtl = Gt + l * dc;
-          double s = 0.0;
-          for (int y = 0; y < d; ++y) s = add(s, add(mul(ftl[x * d + y], gl[y * ncol + z]), mul(fl[x * d + y], gtl[y * ncol + z])));
-          Q[idx] = s;
-        }
-        __syncwarp();
-        // P_l = fc_l gc_l  (into Ft, no longer needed)
-        for (int idx = lane; idx < r * dc; idx += 32) {
-          int l = idx / dc;
-          int rem = idx - l * dc;
-          int x = rem / ncol, z = rem - x * ncol;
-          const double *fl = S + l * dd, *gl = T + l * dc;
-          double s = 0.0;
-          for (int y = 0; y < d; ++y) s = add(s, mul(fl[x * d + y], gl[y * ncol + z]));
-          Ft[idx] = s;
-        }
-        __syncwarp();
-        // h(t_i) = sum_l (beta K(t_i, om_l)) (Q_l + (t_i K(0, om_l)) P_l)  -> written into Gt, becomes T
-        for (int idx = lane; idx < r * dc; idx += 32) {
-          int i = idx / dc;
-          int c = idx - i * dc;
-          const double *kr = sK + i * r;
-          double ti = B.tabs[i];
-          double s = 0.0;
-          for (int l = 0; l < r; ++l)
-            s = add(s, mul(mul(B.beta, kr[l]), add(Q[l * dc + c], mul(mul(ti, B.k0[l]), Ft[l * dc + c]))));
-          Gt[idx] = s;
-        }
-        __syncwarp();
-        T = Gt;
-        // S: any slab that is not T
-        S = (T == bufA) ? bufB : bufA;
       };
 
       for (int v = 1; v < vct0; ++v) {
@@ -264,23 +386,25 @@ __global__ void __launch_bounds__(256) sigma_items_kernel(DevBasis B, const Clas
         const long ok_off = fwd ? B.F_off[pk * B.nb + C.b_out] : B.Fd_off[pk * B.nb + C.b_out];
         const long om_off = fwd ? B.Fd_off[pk * B.nb + b_mu] : B.F_off[pk * B.nb + b_mu];
         const double hs = fwd ? 1.0 : -1.0;
-        // set size: count orbitals of set pk
         int qs = 0;
         for (int i = 0; i < n; ++i)
           if (B.set_to_orb[pk * n + i] >= 0) qs = i + 1;
-        double *X = (S == bufC || T == bufC) ? bufD : bufC;
-        if (X == S || X == T) X = bufE;
-        for (int i = lane; i < r * dvp * d0; i += 32) S[i] = 0.0;
+        const int pout = r * dvp * d0, pmid = r * dv * d0;
+        for (int idx = lane; idx < nb_items * pout; idx += 32) {
+          int j = idx / pout;
+          X[(size_t)j * slab + (idx - j * pout)] = 0.0;
+        }
         __syncwarp();
         for (int mu = 0; mu < qs; ++mu) {
           const int om = B.set_to_orb[pk * n + mu];
-          // X(t) = sum_kap hs Delta_{mu kap}(t) T(t) F_kap
-          for (int idx = lane; idx < r * dv * d0; idx += 32) {
-            int t = idx / (dv * d0);
-            int rem = idx - t * dv * d0;
-            int x = rem / d0, z = rem - x * d0;
-            const double *Tt = T + t * dv * d1;
-            double s = 0.0;
+          for (int idx = lane; idx < nb_items * pmid; idx += 32) {
+            int j = idx / pmid;
+            int rem = idx - j * pmid;
+            int t = rem / (dv * d0);
+            int r2 = rem - t * dv * d0;
+            int x = r2 / d0, z = r2 - x * d0;
+            const double *Tt = T + (size_t)j * slab + t * dv * d1;
+            double a = 0.0;
             for (int kap = 0; kap < qs; ++kap) {
               const int ok = B.set_to_orb[pk * n + kap];
               double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
@@ -288,40 +412,49 @@ __global__ void __launch_bounds__(256) sigma_items_kernel(DevBasis B, const Clas
               const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0;
               double tf = 0.0;
               for (int y = 0; y < d1; ++y) tf = add(tf, mul(Tt[x * d1 + y], Fk[y * d0 + z]));
-              s = add(s, mul(mul(hs, h), tf));
+              a = add(a, mul(mul(hs, h), tf));
             }
-            X[idx] = s;
+            Y[(size_t)j * slab + rem] = a;
           }
           __syncwarp();
           const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
-          for (int idx = lane; idx < r * dvp * d0; idx += 32) {
-            int t = idx / (dvp * d0);
-            int rem = idx - t * dvp * d0;
-            int x = rem / d0, z = rem - x * d0;
-            double s = 0.0;
-            for (int y = 0; y < dv; ++y) s = add(s, mul(Fm[x * dv + y], X[t * dv * d0 + y * d0 + z]));
-            S[idx] = add(S[idx], s);
+          for (int idx = lane; idx < nb_items * pout; idx += 32) {
+            int j = idx / pout;
+            int rem = idx - j * pout;
+            int t = rem / (dvp * d0);
+            int r2 = rem - t * dvp * d0;
+            int x = r2 / d0, z = r2 - x * d0;
+            const double *Yt = Y + (size_t)j * slab + t * dv * d0;
+            double a = 0.0;
+            for (int y = 0; y < dv; ++y) a = add(a, mul(Fm[x * dv + y], Yt[y * d0 + z]));
+            X[(size_t)j * slab + rem] = add(X[(size_t)j * slab + rem], a);
           }
           __syncwarp();
         }
-        double *tmp = T; T = S; S = tmp;
+        double *tmp = T; T = X; X = tmp;
       }
       for (int v = vct0 + 1; v < 2 * m; ++v) {
         edge(v - 1, d0);
         vertex(v, d0);
       }
-      // ---- prefactor, sign and the |T| > 1e-16 guard, then accumulate
-      {
-        const int tot = r * dout * d0;
+      // ---- prefactor and signs, the |T| > 1e-16 guard, accumulation in item order
+      const int tot = r * dout * d0;
+      for (int j = 0; j < nb_items; ++j) {
+        const double sc = ist[j].scale;
         double mx = 0.0;
-        for (int i = lane; i < tot; i += 32) mx = fmax(mx, fabs(mul(T[i], total_scale)));
+        for (int i = lane; i < tot; i += 32) mx = fmax(mx, fabs(mul(T[(size_t)j * slab + i], sc)));
         mx = warp_max(mx);
-        if (mx > 1e-16) {
-          for (int i = lane; i < tot; i += 32) acc[i] = add(acc[i], mul(T[i], total_scale));
-          any = true;
-        }
-        __syncwarp();
+        if (lane == 0) ist[j].keep = mx > 1e-16;
       }
+      __syncwarp();
+      for (int i = lane; i < tot; i += 32) {
+        double a = acc[i];
+        for (int j = 0; j < nb_items; ++j)
+          if (ist[j].keep) a = add(a, mul(T[(size_t)j * slab + i], ist[j].scale));
+        acc[i] = a;
+      }
+      for (int j = 0; j < nb_items; ++j) any = any || ist[j].keep;
+      __syncwarp();
     }
     if (any) {
       double *dst = Sigma + B.goff[C.b_out];
@@ -347,6 +480,17 @@ __global__ void block_maxabs_kernel(const double *G, const long *goff, const int
   if (threadIdx.x == 0) out[b] = red[0];
 }
 
+// FP64 fused multiply-add throughput probe (measurement support): 8 independent chains per thread.
+__global__ void fp64_fma_probe_kernel(double *out, int iters, double x, double y) {
+  double a0 = threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
+  for (int i = 0; i < iters; ++i) {
+    a0 = fma(a0, x, y); a1 = fma(a1, x, y); a2 = fma(a2, x, y); a3 = fma(a3, x, y);
+    a4 = fma(a4, x, y); a5 = fma(a5, x, y); a6 = fma(a6, x, y); a7 = fma(a7, x, y);
+  }
+  double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 1.2345678e300) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 __global__ void zero_kernel(double *x, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) x[i] = 0.0;
 }
@@ -365,6 +509,7 @@ struct ClassSet {
   // item order for the reference's flat-index walk: per (fb_ix, o_ix) the classes in (b, pk) order
   std::vector<std::vector<int>> by_fbo;
   long long n_items = 0;
+  std::map<std::pair<int, int>, std::unique_ptr<ClassSet>> shards;
 };
 
 struct Ctx {
@@ -387,21 +532,35 @@ struct Ctx {
   std::vector<double> hval, hrefl, kitp, kitm, k0p, k0m, kpow;
   std::vector<double> LU, W, Kit;
   std::vector<int> piv;
+  int RP = 0;                                   // padded rank of the register-resident columns
+  std::vector<double> LUp, Wp, BKp;             // RP x RP padded matrices
+  std::vector<int> perm;                        // RP
+  std::vector<long> tab_off;                    // per block offset into the edge tables
+  long nsig_alloc = 0;
+  int region = 0;
   // device copies
-  DevBuf<double> d_LU, d_W, d_Kit, d_tabs, d_k0, d_kitp, d_kitm, d_k0p, d_k0m, d_kpow, d_polesb, d_hval, d_hrefl, d_ops;
-  DevBuf<int> d_piv, d_dims, d_set_to_orb;
+  DevBuf<double> d_tabs, d_k0, d_kitp, d_kitm, d_kpow, d_polesb, d_hval, d_hrefl, d_ops;
+  DevBuf<int> d_dims, d_set_to_orb, d_perm;
+  DevBuf<double> d_LUp, d_Wp, d_BKp, d_tab;
+  DevBuf<long> d_tab_off;
   DevBuf<long> d_goff, d_F_off, d_Fd_off, d_Fb_off, d_Fdb_off;
   DevBuf<int> d_counter;
   DevBuf<double> d_G, d_Sig, d_maxabs;
   std::vector<std::unique_ptr<DevBuf<double>>> user_bufs;
   std::map<std::string, std::unique_ptr<ClassSet>> class_cache;
-  int unit_size = 16;
+  int unit_batches = 4;  // lockstep batches per work unit
+  // profiling: CUDA events around every Sigma launch (enabled on request), user events, L2 flush buffer
+  bool profile = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  cudaEvent_t user_events[8] = {nullptr};
+  DevBuf<double> d_flush;
 
-  DevBasis basis() const {
+  DevBasis basis(int nsig) const {
     DevBasis B;
-    B.r = r; B.p = p; B.n = n; B.nb = nb; B.nq = nq; B.nmax = nmax; B.beta = beta;
-    B.LU = d_LU.ptr; B.piv = d_piv.ptr; B.W = d_W.ptr; B.Kit = d_Kit.ptr; B.tabs = d_tabs.ptr; B.k0 = d_k0.ptr;
-    B.kitp = d_kitp.ptr; B.kitm = d_kitm.ptr; B.k0p = d_k0p.ptr; B.k0m = d_k0m.ptr; B.kpow = d_kpow.ptr; B.polesb = d_polesb.ptr;
+    B.r = r; B.p = p; B.n = n; B.nb = nb; B.nq = nq; B.region = region; B.beta = beta;
+    B.LUp = d_LUp.ptr; B.perm = d_perm.ptr; B.Wp = d_Wp.ptr; B.BKp = d_BKp.ptr; B.tabs = d_tabs.ptr; B.k0 = d_k0.ptr;
+    B.tab = d_tab.ptr; B.tab_off = d_tab_off.ptr; B.nsig = nsig;
+    B.kitp = d_kitp.ptr; B.kitm = d_kitm.ptr; B.kpow = d_kpow.ptr; B.polesb = d_polesb.ptr;
     B.hval = d_hval.ptr; B.hrefl = d_hrefl.ptr; B.goff = d_goff.ptr; B.dims = d_dims.ptr; B.ops = d_ops.ptr;
     B.F_off = d_F_off.ptr; B.Fd_off = d_Fd_off.ptr; B.Fb_off = d_Fb_off.ptr; B.Fdb_off = d_Fdb_off.ptr;
     B.set_to_orb = d_set_to_orb.ptr;
@@ -511,6 +670,12 @@ static ClassSet *get_classes(Ctx *c, const Topology &T, const std::vector<int> &
           for (int i = 0; i < m; ++i) { R.la[i] = T.t[i][0]; R.lb[i] = T.t[i][1]; }
           for (int i = 0; i < nv - 1; ++i) R.ind_path[i] = path[i];
           for (int i = 0; i <= nv; ++i) R.bdims[i] = bd[i];
+          {
+            int mxb = 0;
+            for (int i = 1; i <= nv; ++i) mxb = std::max(mxb, bd[i]);
+            R.dcmax = mxb * std::max(bd[0], bd[1]);
+            R.batch = std::max(1, 32 / R.dcmax);
+          }
           for (int v = 0; v < nv; ++v) {
             R.vline[v] = vline[v];
             if (v == 0 || v == vct0) { R.vkind[v] = 0; R.vset[v] = pk; R.vqo[v] = 0; continue; }
@@ -523,11 +688,12 @@ static ClassSet *get_classes(Ctx *c, const Topology &T, const std::vector<int> &
         }
     }
   for (size_t k = 0; k < cs->classes.size(); ++k) {
-    for (long s = 0; s < npt; s += c->unit_size) {
+    const long usz = (long)cs->classes[k].batch * c->unit_batches;
+    for (long s = 0; s < npt; s += usz) {
       WorkUnit u;
       u.cls = (int)k;
       u.first = (int)s;
-      u.count = (int)std::min<long>(c->unit_size, npt - s);
+      u.count = (int)std::min<long>(usz, npt - s);
       cs->units.push_back(u);
     }
   }
@@ -539,21 +705,65 @@ static ClassSet *get_classes(Ctx *c, const Topology &T, const std::vector<int> &
   return ret;
 }
 
+static size_t sigma_warp_doubles(const Ctx *c) {
+  size_t items_bytes = ((sizeof(ItemState) * 32 + 15) / 16) * 16;
+  return items_bytes / 8 + (size_t)NSLAB * c->region + (size_t)c->r * c->nmax * c->nmax;
+}
+
 static size_t sigma_smem_bytes(const Ctx *c, int warps) {
-  size_t base = (size_t)3 * c->r * c->r + (c->r + 1) / 2;
-  size_t per = (size_t)NBUF * c->r * c->nmax * c->nmax;
-  return (base + per * warps) * sizeof(double);
+  size_t base = (size_t)3 * c->RP * c->RP + (c->RP + 1) / 2;
+  return (base + sigma_warp_doubles(c) * warps) * sizeof(double);
 }
 
 static int sigma_warps(const Ctx *c) {
-  int dev = c->device;
   int maxsm = 0;
-  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  int w = 8;
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+  int w = WARPS_MAX;
   while (w > 1 && sigma_smem_bytes(c, w) > (size_t)maxsm) --w;
   if (sigma_smem_bytes(c, w) > (size_t)maxsm)
     throw Error(XCA_ERR_UNSUPPORTED, "block dimension too large for the shared-memory Sigma kernel (nmax = " + std::to_string(c->nmax) + ")");
   return w;
+}
+
+template <int RP>
+static void launch_tables_rp(Ctx *c, const double *G_dev, int nsig) {
+  long pairs = (long)c->nb * nsig;
+  size_t smem = (2 * (size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
+  CUDA_CHECK(cudaFuncSetAttribute(edge_table_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  long blocks = std::min<long>((pairs + 3) / 4, (long)nsm * 16);
+  edge_table_kernel<RP><<<(int)std::max<long>(1, blocks), 128, smem, c->stream>>>(c->basis(nsig), G_dev, pairs);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+}
+
+// Edge tables of the current G for every signature an order-m topology can use.
+static int prepare_tables(Ctx *c, const double *G_dev, int m) {
+  int nsig = (m >= 3) ? (int)c->nsig_alloc : 1 + 2 * c->p;
+  switch (c->RP) {
+    case 32: launch_tables_rp<32>(c, G_dev, nsig); break;
+    case 48: launch_tables_rp<48>(c, G_dev, nsig); break;
+    default: launch_tables_rp<64>(c, G_dev, nsig); break;
+  }
+  return nsig;
+}
+
+template <int RP>
+static void launch_sigma_rp(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_dev, double scale, int nsig) {
+  int warps = sigma_warps(c);
+  size_t smem = sigma_smem_bytes(c, warps);
+  CUDA_CHECK(cudaFuncSetAttribute(sigma_items_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  c->d_counter.resize(1);
+  CUDA_CHECK(cudaMemsetAsync(c->d_counter.ptr, 0, sizeof(int), c->stream));
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  int grid = std::max(1, std::min<int>(nsm, (int)((cs->units.size() + warps - 1) / warps)));
+  sigma_items_kernel<RP><<<grid, 32 * warps, smem, c->stream>>>(c->basis(nsig), cs->d_classes.ptr, cs->d_units.ptr,
+                                                                (int)cs->units.size(), c->d_counter.ptr, G_dev, Sig_dev, scale,
+                                                                c->nmax);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
 }
 
 static std::vector<int> zero_flags_device(Ctx *c, const double *G_dev) {
@@ -569,20 +779,52 @@ static std::vector<int> zero_flags_device(Ctx *c, const double *G_dev) {
   return z;
 }
 
-static void launch_sigma(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_dev, double scale) {
+static void launch_sigma(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_dev, double scale, int nsig) {
   if (cs->units.empty()) return;
-  int warps = sigma_warps(c);
-  size_t smem = sigma_smem_bytes(c, warps);
-  CUDA_CHECK(cudaFuncSetAttribute(sigma_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  c->d_counter.resize(1);
-  CUDA_CHECK(cudaMemsetAsync(c->d_counter.ptr, 0, sizeof(int), c->stream));
-  int nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  int grid = std::max(1, std::min<int>(nsm, (int)((cs->units.size() + warps - 1) / warps)));
-  sigma_items_kernel<<<grid, 32 * warps, smem, c->stream>>>(c->basis(), cs->d_classes.ptr, cs->d_units.ptr, (int)cs->units.size(),
-                                                           c->d_counter.ptr, G_dev, Sig_dev, scale);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (c->profile) {
+    CUDA_CHECK(cudaEventCreate(&e0));
+    CUDA_CHECK(cudaEventCreate(&e1));
+    CUDA_CHECK(cudaEventRecord(e0, c->stream));
+  }
+  switch (c->RP) {
+    case 32: launch_sigma_rp<32>(c, cs, G_dev, Sig_dev, scale, nsig); break;
+    case 48: launch_sigma_rp<48>(c, cs, G_dev, Sig_dev, scale, nsig); break;
+    default: launch_sigma_rp<64>(c, cs, G_dev, Sig_dev, scale, nsig); break;
+  }
+  if (c->profile) {
+    CUDA_CHECK(cudaEventRecord(e1, c->stream));
+    c->prof_events.emplace_back(e0, e1);
+  }
+}
+
+// Algorithmic real-FP64 flop count of one item (vertex / edge / zero-vertex / accumulate terms of the
+// fixed per-item cost model), for one case pattern of its lines.
+static double item_flops(const Ctx *c, const ClassRec &R, const int *caseA) {
+  const double r = c->r;
+  const int m = R.m, vct0 = R.vct0;
+  double f = 0;
+  auto vertex = [&](int v, int ncol) {
+    double dv = R.bdims[v], dvp = R.bdims[v + 1];
+    f += 2 * r * dvp * dv * ncol;
+    int line = R.vline[v];
+    if (line > 0 && caseA[line]) f += r * dvp * ncol;
+  };
+  auto edge = [&](int e, int ncol) {
+    double d = R.bdims[e + 1];
+    int nk = 0;
+    for (int i = 1; i < m; ++i)
+      if (!caseA[i] && e >= R.la[i] && e < R.lb[i]) nk++;
+    f += r * d * d * nk + 2 * r * r * (d * d + d * ncol) + 2 * (r * r * (d * d + 2 * d * ncol) + 3 * r * d * d * ncol);
+  };
+  for (int v = 1; v < vct0; ++v) { vertex(v, R.bdims[1]); edge(v, R.bdims[1]); }
+  {
+    double S = c->ssizes[R.pk], dv = R.bdims[vct0], d1 = R.bdims[1], d0 = R.bdims[0], dvp = R.bdims[vct0 + 1];
+    f += S * 2 * r * dv * d1 * d0 + S * S * 2 * r * dv * d0 + S * 2 * r * dvp * dv * d0;
+  }
+  for (int v = vct0 + 1; v < 2 * m; ++v) { edge(v - 1, R.bdims[0]); vertex(v, R.bdims[0]); }
+  f += r * R.bdims[2 * m] * R.bdims[0];
+  return f;
 }
 
 // real part of a host complex slab, rejecting non-zero imaginary parts
@@ -662,6 +904,9 @@ int xca_ctx_destroy(xca_ctx *ctx) {
   if (!c) return XCA_OK;
   set_device(c);
   cudaStreamSynchronize(c->stream);
+  for (auto &e : c->prof_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  for (auto &e : c->user_events)
+    if (e) cudaEventDestroy(e);
   cudaStream_t s = c->stream;
   delete c;
   if (s) cudaStreamDestroy(s);
@@ -810,21 +1055,7 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
   {
     std::vector<double> cfs = c->hval;
     long nc = (long)n * n;
-    for (int k = 0; k < r; ++k)
-      if (c->piv[k] != k)
-        for (long j = 0; j < nc; ++j) std::swap(cfs[(size_t)k * nc + j], cfs[(size_t)c->piv[k] * nc + j]);
-    for (int i = 1; i < r; ++i)
-      for (int k = 0; k < i; ++k) {
-        double f = c->LU[(size_t)i * r + k];
-        for (long j = 0; j < nc; ++j) cfs[(size_t)i * nc + j] -= f * cfs[(size_t)k * nc + j];
-      }
-    for (int i = r - 1; i >= 0; --i) {
-      for (int k = i + 1; k < r; ++k) {
-        double f = c->LU[(size_t)i * r + k];
-        for (long j = 0; j < nc; ++j) cfs[(size_t)i * nc + j] -= f * cfs[(size_t)k * nc + j];
-      }
-      for (long j = 0; j < nc; ++j) cfs[(size_t)i * nc + j] /= c->LU[(size_t)i * r + i];
-    }
+    lu_solve(c->LU, r, c->piv, cfs.data(), nc);
     c->hrefl.assign((size_t)r * nc, 0.0);
     for (int i = 0; i < r; ++i)
       for (int l = 0; l < r; ++l) {
@@ -832,11 +1063,49 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
         for (long j = 0; j < nc; ++j) c->hrefl[(size_t)i * nc + j] += k * cfs[(size_t)l * nc + j];
       }
   }
+  // padded matrices of the register-resident column kernels
+  if (r > 64) throw Error(XCA_ERR_UNSUPPORTED, "DLR rank " + std::to_string(r) + " above 64 is not supported by the device kernels");
+  c->RP = r <= 32 ? 32 : (r <= 48 ? 48 : 64);
+  const int RP = c->RP;
+  c->LUp.assign((size_t)RP * RP, 0.0); c->Wp.assign((size_t)RP * RP, 0.0); c->BKp.assign((size_t)RP * RP, 0.0);
+  for (int i = 0; i < RP; ++i)
+    for (int k = 0; k < RP; ++k) {
+      if (i < r && k < r) {
+        c->LUp[(size_t)i * RP + k] = c->LU[(size_t)i * r + k];
+        c->Wp[(size_t)i * RP + k] = c->W[(size_t)i * r + k];
+        c->BKp[(size_t)i * RP + k] = beta * c->Kit[(size_t)i * r + k];
+      } else if (i == k) {
+        c->LUp[(size_t)i * RP + k] = 1.0;
+      }
+    }
+  c->perm.assign(RP, -1);
+  {
+    std::vector<int> idx(r);
+    for (int i = 0; i < r; ++i) idx[i] = i;
+    for (int k = 0; k < r; ++k) std::swap(idx[k], idx[c->piv[k]]);
+    for (int i = 0; i < r; ++i) c->perm[i] = idx[i];
+  }
+  // edge tables: per block, 1 + 2p + 4p^2 signatures of [fc | W fc] (r d^2 each)
+  c->nsig_alloc = 1 + 2L * p + 4L * p * p;
+  c->tab_off.assign(n_blocks, 0);
+  long toff = 0;
+  for (int b = 0; b < n_blocks; ++b) {
+    c->tab_off[b] = toff;
+    toff += c->nsig_alloc * 2L * r * block_dims[b] * block_dims[b];
+  }
+  if ((double)toff * 8.0 > 24e9) throw Error(XCA_ERR_UNSUPPORTED, "edge tables would exceed 24 GB");
+  c->d_tab.resize(toff);
+  {
+    int mxb = 0;
+    for (int b = 0; b < n_blocks; ++b) mxb = std::max(mxb, block_dims[b]);
+    c->region = r * std::max(32, mxb * mxb);
+  }
   // upload
   cudaStream_t s = c->stream;
-  c->d_LU.upload(c->LU, s); c->d_piv.upload(c->piv, s); c->d_W.upload(c->W, s); c->d_Kit.upload(c->Kit, s);
+  c->d_LUp.upload(c->LUp, s); c->d_Wp.upload(c->Wp, s); c->d_BKp.upload(c->BKp, s); c->d_perm.upload(c->perm, s);
+  c->d_tab_off.upload(c->tab_off, s);
   c->d_tabs.upload(c->tabs, s); c->d_k0.upload(c->k0, s); c->d_kitp.upload(c->kitp, s); c->d_kitm.upload(c->kitm, s);
-  c->d_k0p.upload(c->k0p, s); c->d_k0m.upload(c->k0m, s); c->d_kpow.upload(c->kpow, s); c->d_polesb.upload(c->polesb, s);
+  c->d_kpow.upload(c->kpow, s); c->d_polesb.upload(c->polesb, s);
   c->d_hval.upload(c->hval, s); c->d_hrefl.upload(c->hrefl, s); c->d_ops.upload(c->ops, s);
   c->d_dims.upload(c->dims, s); c->d_set_to_orb.upload(c->set_to_orb, s); c->d_goff.upload(c->goff, s);
   c->d_F_off.upload(c->F_off, s); c->d_Fd_off.upload(c->Fd_off, s); c->d_Fb_off.upload(c->Fb_off, s); c->d_Fdb_off.upload(c->Fdb_off, s);
@@ -872,7 +1141,47 @@ int xca_compute_self_energy_device(xca_ctx *ctx, const double *G_dev, int m, con
   Topology T = parse_topology(m, topology);
   auto zero = zero_flags_device(c, G_dev);
   ClassSet *cs = get_classes(c, T, zero);
-  launch_sigma(c, cs, G_dev, Sigma_dev, scale);
+  int nsig = prepare_tables(c, G_dev, m);
+  launch_sigma(c, cs, G_dev, Sigma_dev, scale, nsig);
+  API_END
+}
+
+int xca_compute_self_energy_device_shard(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
+                                         double *Sigma_dev, int shard, int n_shards) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c->ready) throw Error(XCA_ERR_INVALID, "evaluator not set up");
+  if (n_shards < 1 || shard < 0 || shard >= n_shards) throw Error(XCA_ERR_INVALID, "shard out of range");
+  set_device(c);
+  Topology T = parse_topology(m, topology);
+  auto zero = zero_flags_device(c, G_dev);
+  ClassSet *cs = get_classes(c, T, zero);
+  int nsig = prepare_tables(c, G_dev, m);
+  if (n_shards == 1) {
+    launch_sigma(c, cs, G_dev, Sigma_dev, scale, nsig);
+  } else {
+    auto key = std::make_pair(shard, n_shards);
+    auto it = cs->shards.find(key);
+    if (it == cs->shards.end()) {
+      auto sub = std::make_unique<ClassSet>();
+      sub->classes = cs->classes;
+      for (size_t u = shard; u < cs->units.size(); u += n_shards) sub->units.push_back(cs->units[u]);
+      sub->d_classes.upload(sub->classes, c->stream);
+      sub->d_units.upload(sub->units, c->stream);
+      it = cs->shards.emplace(key, std::move(sub)).first;
+    }
+    launch_sigma(c, it->second.get(), G_dev, Sigma_dev, scale, nsig);
+  }
+  API_END
+}
+
+int xca_zero_device(xca_ctx *ctx, double *dev, long n) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  set_device(c);
+  zero_kernel<<<std::max<long>(1, std::min<long>(1184, (n + 255) / 256)), 256, 0, c->stream>>>(dev, n);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
   API_END
 }
 
@@ -892,8 +1201,9 @@ int xca_compute_self_energy(xca_ctx *ctx, const double *G, int m, const int *top
   c->launches++;
   auto zero = zero_flags_device(c, c->d_G.ptr);
   ClassSet *cs = get_classes(c, T, zero);
+  int nsig = prepare_tables(c, c->d_G.ptr, m);
   if (f_ix == nullptr) {
-    launch_sigma(c, cs, c->d_G.ptr, c->d_Sig.ptr, 1.0);
+    launch_sigma(c, cs, c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
   } else {
     // subset of flat indices: build a dedicated unit list (one unit per listed f_ix and valid class)
     const long omax = ipow(c->n, m - 1), npt = ipow(c->p, m - 1);
@@ -911,7 +1221,7 @@ int xca_compute_self_energy(xca_ctx *ctx, const double *G, int m, const int *top
       tmp.units = units;
       tmp.d_classes.upload(tmp.classes, c->stream);
       tmp.d_units.upload(tmp.units, c->stream);
-      launch_sigma(c, &tmp, c->d_G.ptr, c->d_Sig.ptr, 1.0);
+      launch_sigma(c, &tmp, c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
       CUDA_CHECK(cudaStreamSynchronize(c->stream));
     }
   }
@@ -972,6 +1282,131 @@ int xca_self_energy_items(xca_ctx *ctx, const double *G, int m, const int *topol
         }
       }
   *n_items = count;
+  API_END
+}
+
+int xca_self_energy_flops(xca_ctx *ctx, const double *G, int m, const int *topology, double *alg_flops, long *n_items) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c->ready) throw Error(XCA_ERR_INVALID, "evaluator not set up");
+  Topology T = parse_topology(m, topology);
+  std::vector<double> g;
+  real_part(G, c->slab, g, "G");
+  std::vector<int> zero(c->nb);
+  for (int b = 0; b < c->nb; ++b) {
+    long o = c->goff[b], sz = (long)c->r * c->dims[b] * c->dims[b];
+    double mx = 0;
+    for (long i = 0; i < sz; ++i) mx = std::max(mx, std::fabs(g[o + i]));
+    zero[b] = mx < 1e-16;
+  }
+  set_device(c);
+  ClassSet *cs = get_classes(c, T, zero);
+  // count pole tuples per case pattern: a line's case depends on its direction and its pole's sign
+  const int p = c->p;
+  long nA[2] = {0, 0};
+  for (int l = 0; l < p; ++l) {
+    if (c->polesb[l] <= 0.0) nA[1]++;  // forward line, case A
+    if (c->polesb[l] >= 0.0) nA[0]++;  // backward line, case A
+  }
+  double tot = 0;
+  for (const ClassRec &R : cs->classes) {
+    int nl = m - 1;
+    for (int mask = 0; mask < (1 << nl); ++mask) {
+      int caseA[MAXM] = {0, 0, 0};
+      double count = 1;
+      for (int i = 1; i < m; ++i) {
+        int fwd = (R.fbmask >> i) & 1;
+        caseA[i] = (mask >> (i - 1)) & 1;
+        long a = nA[fwd];
+        count *= caseA[i] ? a : (p - a);
+      }
+      if (count > 0) tot += count * item_flops(c, R, caseA);
+    }
+  }
+  *alg_flops = tot;
+  *n_items = (long)cs->n_items;
+  API_END
+}
+
+int xca_profile(xca_ctx *ctx, int enable, double *sigma_ms, long *sigma_launches) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  set_device(c);
+  double ms = 0;
+  long n = 0;
+  if (!c->prof_events.empty()) {
+    CUDA_CHECK(cudaStreamSynchronize(c->stream));
+    for (auto &e : c->prof_events) {
+      float x = 0;
+      CUDA_CHECK(cudaEventElapsedTime(&x, e.first, e.second));
+      ms += x;
+      n++;
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    c->prof_events.clear();
+  }
+  c->profile = enable != 0;
+  if (sigma_ms) *sigma_ms = ms;
+  if (sigma_launches) *sigma_launches = n;
+  API_END
+}
+
+int xca_event_record(xca_ctx *ctx, int slot) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  set_device(c);
+  if (slot < 0 || slot >= 8) throw Error(XCA_ERR_INVALID, "event slot out of range");
+  if (!c->user_events[slot]) CUDA_CHECK(cudaEventCreate(&c->user_events[slot]));
+  CUDA_CHECK(cudaEventRecord(c->user_events[slot], c->stream));
+  API_END
+}
+
+int xca_event_elapsed(xca_ctx *ctx, int slot_a, int slot_b, double *ms) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  set_device(c);
+  if (slot_a < 0 || slot_a >= 8 || slot_b < 0 || slot_b >= 8 || !c->user_events[slot_a] || !c->user_events[slot_b])
+    throw Error(XCA_ERR_INVALID, "event slot not recorded");
+  CUDA_CHECK(cudaEventSynchronize(c->user_events[slot_b]));
+  float x = 0;
+  CUDA_CHECK(cudaEventElapsedTime(&x, c->user_events[slot_a], c->user_events[slot_b]));
+  *ms = x;
+  API_END
+}
+
+int xca_flush_l2(xca_ctx *ctx, long bytes) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  set_device(c);
+  long n = (bytes + 7) / 8;
+  c->d_flush.resize(n);
+  zero_kernel<<<1184, 256, 0, c->stream>>>(c->d_flush.ptr, n);
+  CUDA_CHECK(cudaGetLastError());
+  API_END
+}
+
+int xca_fp64_fma_probe(xca_ctx *ctx, double *tflops) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  set_device(c);
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  const int blocks = nsm * 8, threads = 256, iters = 8192;
+  c->d_flush.resize((size_t)blocks * threads);
+  cudaEvent_t e0, e1;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  fp64_fma_probe_kernel<<<blocks, threads, 0, c->stream>>>(c->d_flush.ptr, iters, 0.999999, 1e-7);
+  CUDA_CHECK(cudaEventRecord(e0, c->stream));
+  for (int rep = 0; rep < 5; ++rep) fp64_fma_probe_kernel<<<blocks, threads, 0, c->stream>>>(c->d_flush.ptr, iters, 0.999999, 1e-7);
+  CUDA_CHECK(cudaEventRecord(e1, c->stream));
+  CUDA_CHECK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *tflops = 5.0 * 2.0 * 8.0 * iters * (double)blocks * threads / (ms * 1e-3) / 1e12;
   API_END
 }
 
