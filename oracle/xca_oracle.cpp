@@ -26,6 +26,16 @@ using cd = std::complex<double>;
 
 namespace {
 
+// Fused multiply-adds of the restated arithmetic: every a * b + c below is one correctly rounded
+// operation per real component, the operation model the device path reproduces bit for bit.
+inline cd cfma(const cd &a, const cd &b, const cd &c) {
+  return {std::fma(a.real(), b.real(), std::fma(-a.imag(), b.imag(), c.real())),
+          std::fma(a.real(), b.imag(), std::fma(a.imag(), b.real(), c.imag()))};
+}
+inline cd dfma(double a, const cd &b, const cd &c) { return {std::fma(a, b.real(), c.real()), std::fma(a, b.imag(), c.imag())}; }
+inline double dfma(double a, double b, double c) { return std::fma(a, b, c); }
+inline cd dfma(const cd &a, const cd &b, const cd &c) { return cfma(a, b, c); }
+
 // ---------------------------------------------------------------- kernel and DLR basis
 // cppdlr::k_it (call sites hyb.cpp:98-103).  cppdlr's kernel carries the Green's-function sign,
 // K(t, om) = -exp(-t om) / (1 + exp(-om)) (om >= 0), -exp((1 - t) om) / (1 + exp(om)) (om < 0): the
@@ -70,7 +80,7 @@ void lu_factor(std::vector<T> &a, int n, std::vector<int> &piv) {
 // Solve A X = B in place, B is n x nrhs row-major, with the LU factors of lu_factor.  The
 // substitutions run in the column order of the reference BLAS dtrsm that LAPACK getrs calls: forward,
 // for k ascending, b_i -= L_ik b_k (i > k); backward, for k descending, b_k /= U_kk then
-// b_i -= U_ik b_k (i < k).
+// b_i -= U_ik b_k (i < k), each update one fused multiply-add.
 template <class T, class U>
 void lu_solve(const std::vector<T> &lu, int n, const std::vector<int> &piv, U *b, long nrhs) {
   for (int k = 0; k < n; ++k)
@@ -79,14 +89,14 @@ void lu_solve(const std::vector<T> &lu, int n, const std::vector<int> &piv, U *b
   for (int k = 0; k < n; ++k)
     for (int i = k + 1; i < n; ++i) {
       T f = lu[(size_t)i * n + k];
-      for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] -= f * b[(size_t)k * nrhs + j];
+      for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] = dfma(-f, b[(size_t)k * nrhs + j], b[(size_t)i * nrhs + j]);
     }
   for (int k = n - 1; k >= 0; --k) {
     T d = lu[(size_t)k * n + k];
     for (long j = 0; j < nrhs; ++j) b[(size_t)k * nrhs + j] /= d;
     for (int i = 0; i < k; ++i) {
       T f = lu[(size_t)i * n + k];
-      for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] -= f * b[(size_t)k * nrhs + j];
+      for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] = dfma(-f, b[(size_t)k * nrhs + j], b[(size_t)i * nrhs + j]);
     }
   }
 }
@@ -151,8 +161,8 @@ struct Dlr {
       for (int k = 0; k < r; ++k) {
         if (k == l) continue;
         double w = (time_order ? k0[k] : 1.0) / (rf[k] - rf[l]);
-        for (int x = 0; x < a * b; ++x) ft[(size_t)l * a * b + x] += w * fc[(size_t)k * a * b + x];
-        for (int x = 0; x < b * c; ++x) gt[(size_t)l * b * c + x] += w * gc[(size_t)k * b * c + x];
+        for (int x = 0; x < a * b; ++x) ft[(size_t)l * a * b + x] = dfma(w, fc[(size_t)k * a * b + x], ft[(size_t)l * a * b + x]);
+        for (int x = 0; x < b * c; ++x) gt[(size_t)l * b * c + x] = dfma(w, gc[(size_t)k * b * c + x], gt[(size_t)l * b * c + x]);
       }
     for (int i = 0; i < r; ++i)
       for (int x = 0; x < a * c; ++x) h[(size_t)i * a * c + x] = 0;
@@ -164,8 +174,8 @@ struct Dlr {
         for (int z = 0; z < c; ++z) {
           cd sq = 0, sp = 0;
           for (int y = 0; y < b; ++y) {
-            sq += fh[x * b + y] * g[y * c + z] + f[x * b + y] * gh[y * c + z];
-            sp += f[x * b + y] * g[y * c + z];
+            sq = cfma(fh[x * b + y], g[y * c + z], cfma(f[x * b + y], gh[y * c + z], sq));
+            sp = cfma(f[x * b + y], g[y * c + z], sp);
           }
           Q[(size_t)l * a * c + x * c + z] = sq;
           P[(size_t)l * a * c + x * c + z] = sp;
@@ -179,10 +189,10 @@ struct Dlr {
           cd h1 = 0, h2 = 0;
           for (int l = 0; l < r; ++l) {
             double bk = beta * cf2it[(size_t)i * r + l];
-            h1 += bk * Q[(size_t)l * a * c + x];
-            h2 += bk * (k0[l] * P[(size_t)l * a * c + x]);
+            h1 = dfma(bk, Q[(size_t)l * a * c + x], h1);
+            h2 = dfma(bk, k0[l] * P[(size_t)l * a * c + x], h2);
           }
-          h[(size_t)i * a * c + x] = h1 + tabs[i] * h2;
+          h[(size_t)i * a * c + x] = dfma(tabs[i], h2, h1);
         }
     } else {
       // full (fermionic) convolution: h = -beta sum_l K_l(t)[Q_l + (t + K_l(1)) P_l] (weights 1 / (om_k - om_l))
@@ -407,7 +417,7 @@ void left_mul(int r, const cd *F, int R, int K, const cd *in, int C, cd *out) {
     for (int i = 0; i < R; ++i)
       for (int j = 0; j < C; ++j) {
         cd s = 0;
-        for (int k = 0; k < K; ++k) s += F[i * K + k] * a[k * C + j];
+        for (int k = 0; k < K; ++k) s = cfma(F[i * K + k], a[k * C + j], s);
         o[i * C + j] = s;
       }
   }
@@ -420,7 +430,7 @@ void right_mul(int r, const cd *in, int R, int K, const cd *F, int C, cd *out) {
     for (int i = 0; i < R; ++i)
       for (int j = 0; j < C; ++j) {
         cd s = 0;
-        for (int k = 0; k < K; ++k) s += a[i * K + k] * F[k * C + j];
+        for (int k = 0; k < K; ++k) s = cfma(a[i * K + k], F[k * C + j], s);
         o[i * C + j] = s;
       }
   }
@@ -523,7 +533,7 @@ void zero_vertex(const Evaluator &E, const Backbone &B, Work &w, bool fwd, int b
       for (int t = 0; t < r; ++t) {
         cd h = fwd ? E.values[((size_t)t * E.n + om) * E.n + ok] : E.values_refl[((size_t)t * E.n + ok) * E.n + om];
         cd f = hs * h;
-        for (int x = 0; x < dv * d0; ++x) w.tm[(size_t)t * dv * d0 + x] += f * w.tk[k * sz + (size_t)t * dv * d0 + x];
+        for (int x = 0; x < dv * d0; ++x) w.tm[(size_t)t * dv * d0 + x] = cfma(f, w.tk[k * sz + (size_t)t * dv * d0 + x], w.tm[(size_t)t * dv * d0 + x]);
       }
     }
     const cd *Fm = Sm.blocks[b_mu].data() + (size_t)mu * dvp * dv;

@@ -150,7 +150,8 @@ inline void lu_factor(std::vector<double> &a, int n, std::vector<int> &piv) {
 
 // Solve A X = B in place (B is n x nrhs, row-major) with the factors of lu_factor, in the column order
 // of the reference BLAS dtrsm that LAPACK getrs calls: row interchanges; forward, for k ascending,
-// b_i -= L_ik b_k (i > k); backward, for k descending, b_k /= U_kk then b_i -= U_ik b_k (i < k).
+// b_i -= L_ik b_k (i > k); backward, for k descending, b_k /= U_kk then b_i -= U_ik b_k (i < k); every
+// update is one fused multiply-add.
 inline void lu_solve(const std::vector<double> &lu, int n, const std::vector<int> &piv, double *b, long nrhs) {
   for (int k = 0; k < n; ++k)
     if (piv[k] != k)
@@ -158,14 +159,14 @@ inline void lu_solve(const std::vector<double> &lu, int n, const std::vector<int
   for (int k = 0; k < n; ++k)
     for (int i = k + 1; i < n; ++i) {
       double f = lu[(size_t)i * n + k];
-      for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] -= f * b[(size_t)k * nrhs + j];
+      for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] = std::fma(-f, b[(size_t)k * nrhs + j], b[(size_t)i * nrhs + j]);
     }
   for (int k = n - 1; k >= 0; --k) {
     double d = lu[(size_t)k * n + k];
     for (long j = 0; j < nrhs; ++j) b[(size_t)k * nrhs + j] /= d;
     for (int i = 0; i < k; ++i) {
       double f = lu[(size_t)i * n + k];
-      for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] -= f * b[(size_t)k * nrhs + j];
+      for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] = std::fma(-f, b[(size_t)k * nrhs + j], b[(size_t)i * nrhs + j]);
     }
   }
 }

@@ -12,8 +12,9 @@
 // hyb.cpp:46-57), edge convolutions (:165-178 with hyb.cpp:59-73 and the time-ordered DLR
 // convolution), the zero-vertex hybridization contraction (:187-227), the K(0) prefactor
 // (hyb.cpp:75-92), the order / direction sign and the 1e-16 contribution guard (:359-366).  Every
-// product and sum is rounded on its own (no fused multiply-add), in the operation order of the CPU
-// restatement, so each item's contribution is bit-identical to it.  The G-side coefficients of an
+// product and sum is rounded exactly as in the operation order of the CPU
+// restatement (one fused multiply-add wherever it fuses one), so each item's contribution is
+// bit-identical to it.  The G-side coefficients of an
 // edge (fc = K^-1 (G_b * prod K) and W fc) depend only on the block and the edge's K factors; they are
 // tabulated once per G by edge_table_kernel.
 #pragma once
@@ -30,10 +31,10 @@ constexpr int WARPS_MAX = 8;
 struct DevBasis {
   int r, p, n, nb, nq, region;  // region: doubles per slab region of a warp, r * max(32, largest dcmax)
   double beta;
-  const double *LUp;    // RP x RP padded LU of K(t_i, om_l): unit L below the diagonal, U on and above; pad: U_kk = 1
+  const double *LUp;    // RP x RP padded LU of K(t_i, om_l), column-major: unit L below the diagonal, U on and above; pad: U_kk = 1
   const int *perm;      // RP: row gathered into position i by the pivoting (-1 beyond r)
-  const double *Wp;     // RP x RP: W[l][k] = K(0, om_k) / (om_k - om_l), 0 on the diagonal and in the pad
-  const double *BKp;    // RP x RP: beta * K(t_i, om_l), 0 in the pad
+  const double *Wp;     // RP x RP column-major: W[l][k] = K(0, om_k) / (om_k - om_l), 0 on the diagonal and in the pad
+  const double *BKp;    // RP x RP column-major: beta * K(t_i, om_l), 0 in the pad
   const double *tabs;   // r: absolute t_i
   const double *k0;     // r: K(0, om_l)
   const double *kitp;   // r x p: K(t_i, +beta w_l)
@@ -70,36 +71,39 @@ struct WorkUnit {
   int count;
 };
 
-// Arithmetic of the plain FP64 path: every product and sum rounded on its own (no contraction).
+// Arithmetic of the plain FP64 path: the fused multiply-adds and the separately rounded products and
+// sums of the CPU restatement, at the same places and in the same order.
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double fmad(double a, double b, double c) { return __fma_rn(a, b, c); }
 
 __device__ __forceinline__ double warp_max(double v) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
-// x <- K^{-1} x for one register-resident column (already gathered through perm): forward unit-lower
-// then backward upper substitution in dtrsm column order.  Padding rows stay zero.
+// x <- K^{-1} x for one register-resident column (already gathered through the pivoting): forward
+// unit-lower then backward upper substitution in dtrsm column order.  LUT is the LU factor stored
+// column-major (LUT[k * RP + i] = LU[i][k]).  Padding rows stay zero.
 template <int RP>
-__device__ __forceinline__ void lu_solve_reg(const double *__restrict__ LU, double (&x)[RP]) {
+__device__ __forceinline__ void lu_solve_reg(const double *__restrict__ LUT, double (&x)[RP]) {
 #pragma unroll
   for (int k = 0; k < RP; ++k) {
 #pragma unroll
-    for (int i = k + 1; i < RP; ++i) x[i] = sub(x[i], mul(LU[i * RP + k], x[k]));
+    for (int i = k + 1; i < RP; ++i) x[i] = fmad(-LUT[k * RP + i], x[k], x[i]);
   }
 #pragma unroll
   for (int k = RP - 1; k >= 0; --k) {
-    x[k] = __ddiv_rn(x[k], LU[k * RP + k]);
+    x[k] = __ddiv_rn(x[k], LUT[k * RP + k]);
 #pragma unroll
-    for (int i = 0; i < k; ++i) x[i] = sub(x[i], mul(LU[i * RP + k], x[k]));
+    for (int i = 0; i < k; ++i) x[i] = fmad(-LUT[k * RP + i], x[k], x[i]);
   }
 }
 
-// y_l = sum_k M[l][k] x_k for l < r (each sum from zero, k ascending); y written with stride `ld`.
+// y_l = sum_k M[l][k] x_k for l < r (fused multiply-adds from zero, k ascending), with MT = M stored
+// column-major (MT[k * RP + l]); y written with stride `ld`.
 template <int RP>
-__device__ __forceinline__ void matvec_reg(const double *__restrict__ M, const double (&x)[RP], int r, double *y, int ld) {
+__device__ __forceinline__ void matvec_reg(const double *__restrict__ MT, const double (&x)[RP], int r, double *y, int ld) {
   constexpr int CH = 8;
 #pragma unroll 1
   for (int l0 = 0; l0 < RP; l0 += CH) {
@@ -110,7 +114,7 @@ __device__ __forceinline__ void matvec_reg(const double *__restrict__ M, const d
 #pragma unroll
     for (int k = 0; k < RP; ++k) {
 #pragma unroll
-      for (int j = 0; j < CH; ++j) acc[j] = add(acc[j], mul(M[(l0 + j) * RP + k], x[k]));
+      for (int j = 0; j < CH; ++j) acc[j] = fmad(MT[k * RP + l0 + j], x[k], acc[j]);
     }
 #pragma unroll
     for (int j = 0; j < CH; ++j)

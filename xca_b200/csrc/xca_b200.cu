@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(128) edge_table_kernel(DevBasis B, const doubl
   }
 }
 
-// Dynamic shared memory: LU | W | BK (3 RP^2 doubles) | perm (RP ints) | per warp: 32 item states,
-// NSLAB slab regions of B.region doubles, r * nmax^2 doubles of accumulator.
+// Dynamic shared memory: LU | W | BK (3 RP^2 doubles, column-major) | perm (RP ints) | per warp: 32 item
+// states, NSLAB slab regions of B.region doubles, r * nmax^2 doubles of accumulator.
 template <int RP>
 __global__ void __launch_bounds__(32 * WARPS_MAX) sigma_items_kernel(DevBasis B, const ClassRec *__restrict__ classes,
                                                                       const WorkUnit *__restrict__ units, int n_units,
@@ -169,13 +169,13 @@ __global__ void __launch_bounds__(32 * WARPS_MAX) sigma_items_kernel(DevBasis B,
     u = __shfl_sync(0xffffffffu, u, 0);
     if (u >= n_units) break;
     const WorkUnit wu = units[u];
-    const ClassRec C = classes[wu.cls];
+    const ClassRec &C = classes[wu.cls];
     const int m = C.m, vct0 = C.vct0;
     const int d0 = C.bdims[0], d1 = C.bdims[1];
     const int dout = C.bdims[2 * m];
-    const int cap = C.batch;  // items per lockstep batch; cap * (largest d * c of the chain) <= 32
+    const int cap = C.batch;       // items per lockstep batch; cap * (largest d * c of the chain) <= 32
     const int slab = r * C.dcmax;  // item j's T / X / Y slabs are j-strided within each of the three regions
-    double *regT = slabs, *regX = slabs + B.region, *regY = slabs + 2 * (size_t)B.region;
+    const int nops = 4 * m - 3;    // V E ... Z ... E V: 2 (vct0 - 1) + 1 + 2 (2m - 1 - vct0)
     for (int i = lane; i < r * dout * d0; i += 32) acc[i] = 0.0;
     bool any = false;
 
@@ -185,9 +185,7 @@ __global__ void __launch_bounds__(32 * WARPS_MAX) sigma_items_kernel(DevBasis B,
       if (lane < nb_items) {
         ItemState &S = ist[lane];
         int q = wu.first + first + lane;
-        S.lpole[0] = 0;
-        S.caseA[0] = 0;
-        for (int i = 1; i < MAXM; ++i) { S.lpole[i] = 0; S.caseA[i] = 0; }
+        for (int i = 0; i < MAXM; ++i) { S.lpole[i] = 0; S.caseA[i] = 0; }
         for (int i = 1; i < m; ++i) {
           S.lpole[i] = q % p;
           q /= p;
@@ -207,235 +205,234 @@ __global__ void __launch_bounds__(32 * WARPS_MAX) sigma_items_kernel(DevBasis B,
         if (!(C.fbmask & 1)) dsign = -dsign;
         S.scale = mul(pf, (double)(psign * dsign));
       }
+      double *T = slabs, *X = slabs + B.region, *Y = slabs + 2 * (size_t)B.region;
       // T := G[ind_path[0]] (d1 x d1) for every item
       {
         const double *g = G + B.goff[C.ind_path[0]];
         const int sz = r * d1 * d1;
         for (int idx = lane; idx < nb_items * sz; idx += 32) {
           int j = idx / sz;
-          regT[(size_t)j * slab + (idx - j * sz)] = g[idx - j * sz];
+          T[(size_t)j * slab + (idx - j * sz)] = g[idx - j * sz];
         }
       }
       __syncwarp();
-      double *T = regT, *X = regX, *Y = regY;
 
-      // ---- vertex v: T(t) <- k(t) F T(t)  (multiply_left_vertex)
-      auto vertex = [&](int v, int ncol) {
-        const int line = C.vline[v];
-        const int b = C.ind_path[v - 1];
-        const int dv = C.bdims[v], dvp = C.bdims[v + 1];
-        const int s = C.vset[v], qo = C.vqo[v];
-        if (lane < nb_items) {
-          ItemState &S = ist[lane];
-          const int l = S.lpole[line];
-          long off;
-          switch (C.vkind[v]) {
-            case 0: off = B.F_off[s * B.nb + b] + (long)qo * dvp * dv; break;
-            case 1: off = B.Fd_off[s * B.nb + b] + (long)qo * dvp * dv; break;
-            case 2: off = B.Fb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
-            default: off = B.Fdb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
-          }
-          S.opoff = off;
-          S.kcol = -1;
-          if (line > 0 && S.caseA[line]) {
-            int fwd = (C.fbmask >> line) & 1;
-            int ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
-            S.kcol = l;
-            S.kneg = ks < 0;
-          }
-        }
-        __syncwarp();
-        const int per = r * dvp * ncol;
-        for (int idx = lane; idx < nb_items * per; idx += 32) {
-          int j = idx / per;
-          int rem = idx - j * per;
-          int t = rem / (dvp * ncol);
-          int r2 = rem - t * dvp * ncol;
-          int x = r2 / ncol, z = r2 - x * ncol;
-          const ItemState &S = ist[j];
-          const double *F = B.ops + S.opoff;
-          const double *Tt = T + (size_t)j * slab + t * dv * ncol;
-          double a = 0.0;
-          for (int y = 0; y < dv; ++y) a = add(a, mul(F[x * dv + y], Tt[y * ncol + z]));
-          if (S.kcol >= 0) a = mul(a, (S.kneg ? B.kitm : B.kitp)[(size_t)t * p + S.kcol]);
-          X[(size_t)j * slab + rem] = a;
-        }
-        __syncwarp();
-        double *tmp = T; T = X; X = tmp;
-      };
+      for (int op = 0; op < nops; ++op) {
+        // op order: for v < vct0: vertex v, edge v; zero vertex; for v > vct0: edge v - 1, vertex v
+        int kind, v;
+        const int pre = 2 * (vct0 - 1);
+        if (op < pre) { v = 1 + op / 2; kind = (op & 1) ? 1 : 0; }
+        else if (op == pre) { v = vct0; kind = 2; }
+        else { int q = op - pre - 1; v = vct0 + 1 + q / 2; kind = (q & 1) ? 0 : 1; }
+        const int ncol = v < vct0 ? d1 : d0;
 
-      // ---- edge e: T <- conv(G_b * prod K, T)  (integrate_left_edge, time-ordered DLR convolution)
-      auto edge = [&](int e, int ncol) {
-        const int b = C.ind_path[e];
-        const int d = C.bdims[e + 1];
-        const int dd = d * d, dc = d * ncol;
-        if (lane < nb_items) {
-          ItemState &S = ist[lane];
-          int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
-          for (int i = 1; i < m; ++i)
-            if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
-              sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
-              lp[nf] = S.lpole[i];
-              nf++;
+        if (kind == 0) {
+          // ---- vertex v: T(t) <- k(t) F T(t)  (multiply_left_vertex)
+          const int line = C.vline[v];
+          const int b = C.ind_path[v - 1];
+          const int dv = C.bdims[v], dvp = C.bdims[v + 1];
+          const int s = C.vset[v], qo = C.vqo[v];
+          if (lane < nb_items) {
+            ItemState &S = ist[lane];
+            const int l = S.lpole[line];
+            long off;
+            switch (C.vkind[v]) {
+              case 0: off = B.F_off[s * B.nb + b] + (long)qo * dvp * dv; break;
+              case 1: off = B.Fd_off[s * B.nb + b] + (long)qo * dvp * dv; break;
+              case 2: off = B.Fb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
+              default: off = B.Fdb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
             }
-          long sig = 0;
-          if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
-          if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
-          S.taboff = B.tab_off[b] + sig * 2 * r * dd;
-        }
-        __syncwarp();
-        // (a) gc = K^-1 T (in place, column per lane) and Gt = W gc (into X)
-        for (int cl = lane; cl < nb_items * dc; cl += 32) {
-          const int j = cl / dc, col = cl - j * dc;
-          double *Tj = T + (size_t)j * slab;
-          double x[RP];
-#pragma unroll
-          for (int i = 0; i < RP; ++i) {
-            int src = sPerm[i];
-            x[i] = src >= 0 ? Tj[src * dc + col] : 0.0;
-          }
-          lu_solve_reg<RP>(sLU, x);
-#pragma unroll
-          for (int i = 0; i < RP; ++i)
-            if (i < r) Tj[i * dc + col] = x[i];
-          matvec_reg<RP>(sW, x, r, X + (size_t)j * slab + col, dc);
-        }
-        __syncwarp();
-        // (b) Q_l = Ft_l gc_l + fc_l Gt_l  (into Y)
-        const int per = r * dc;
-        for (int idx = lane; idx < nb_items * per; idx += 32) {
-          int j = idx / per;
-          int rem = idx - j * per;
-          int l = rem / dc;
-          int r2 = rem - l * dc;
-          int x = r2 / ncol, z = r2 - x * ncol;
-          const double *tb = B.tab + ist[j].taboff;
-          const double *fl = tb + l * dd, *ftl = tb + (long)r * dd + l * dd;
-          const double *gl = T + (size_t)j * slab + l * dc, *gtl = X + (size_t)j * slab + l * dc;
-          double a = 0.0;
-          for (int y = 0; y < d; ++y) a = add(a, add(mul(ftl[x * d + y], gl[y * ncol + z]), mul(fl[x * d + y], gtl[y * ncol + z])));
-          Y[(size_t)j * slab + rem] = a;
-        }
-        __syncwarp();
-        // (c) h1 = (beta K) Q  (into X, Gt no longer needed)
-        for (int cl = lane; cl < nb_items * dc; cl += 32) {
-          const int j = cl / dc, col = cl - j * dc;
-          const double *Yj = Y + (size_t)j * slab;
-          double q[RP];
-#pragma unroll
-          for (int i = 0; i < RP; ++i) q[i] = i < r ? Yj[i * dc + col] : 0.0;
-          matvec_reg<RP>(sBK, q, r, X + (size_t)j * slab + col, dc);
-        }
-        __syncwarp();
-        // (d) P'_l = K(0, om_l) (fc_l gc_l)  (into Y)
-        for (int idx = lane; idx < nb_items * per; idx += 32) {
-          int j = idx / per;
-          int rem = idx - j * per;
-          int l = rem / dc;
-          int r2 = rem - l * dc;
-          int x = r2 / ncol, z = r2 - x * ncol;
-          const double *fl = B.tab + ist[j].taboff + l * dd;
-          const double *gl = T + (size_t)j * slab + l * dc;
-          double a = 0.0;
-          for (int y = 0; y < d; ++y) a = add(a, mul(fl[x * d + y], gl[y * ncol + z]));
-          Y[(size_t)j * slab + rem] = mul(B.k0[l], a);
-        }
-        __syncwarp();
-        // (e) h = h1 + t_i (beta K) P'  (into T)
-        for (int cl = lane; cl < nb_items * dc; cl += 32) {
-          const int j = cl / dc, col = cl - j * dc;
-          const double *Yj = Y + (size_t)j * slab;
-          double q[RP];
-#pragma unroll
-          for (int i = 0; i < RP; ++i) q[i] = i < r ? Yj[i * dc + col] : 0.0;
-          double *Tj = T + (size_t)j * slab;
-          const double *h1 = X + (size_t)j * slab;
-          constexpr int CH = 8;
-#pragma unroll 1
-          for (int l0 = 0; l0 < RP; l0 += CH) {
-            if (l0 >= r) break;
-            double a[CH];
-#pragma unroll
-            for (int jj = 0; jj < CH; ++jj) a[jj] = 0.0;
-#pragma unroll
-            for (int k = 0; k < RP; ++k) {
-#pragma unroll
-              for (int jj = 0; jj < CH; ++jj) a[jj] = add(a[jj], mul(sBK[(l0 + jj) * RP + k], q[k]));
-            }
-#pragma unroll
-            for (int jj = 0; jj < CH; ++jj) {
-              int i = l0 + jj;
-              if (i < r) Tj[i * dc + col] = add(h1[i * dc + col], mul(B.tabs[i], a[jj]));
+            S.opoff = off;
+            S.kcol = -1;
+            if (line > 0 && S.caseA[line]) {
+              int fwd = (C.fbmask >> line) & 1;
+              int ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
+              S.kcol = l;
+              S.kneg = ks < 0;
             }
           }
-        }
-        __syncwarp();
-      };
-
-      for (int v = 1; v < vct0; ++v) {
-        vertex(v, d1);
-        edge(v, d1);
-      }
-      // ---- zero vertex (multiply_left_vertex_and_right_zero_vertex)
-      {
-        const int v = vct0;
-        const int b_mu = C.ind_path[v - 1];
-        const int dv = C.bdims[v], dvp = C.bdims[v + 1];
-        const bool fwd = C.fbmask & 1;
-        const int pk = C.pk;
-        const long ok_off = fwd ? B.F_off[pk * B.nb + C.b_out] : B.Fd_off[pk * B.nb + C.b_out];
-        const long om_off = fwd ? B.Fd_off[pk * B.nb + b_mu] : B.F_off[pk * B.nb + b_mu];
-        const double hs = fwd ? 1.0 : -1.0;
-        int qs = 0;
-        for (int i = 0; i < n; ++i)
-          if (B.set_to_orb[pk * n + i] >= 0) qs = i + 1;
-        const int pout = r * dvp * d0, pmid = r * dv * d0;
-        for (int idx = lane; idx < nb_items * pout; idx += 32) {
-          int j = idx / pout;
-          X[(size_t)j * slab + (idx - j * pout)] = 0.0;
-        }
-        __syncwarp();
-        for (int mu = 0; mu < qs; ++mu) {
-          const int om = B.set_to_orb[pk * n + mu];
-          for (int idx = lane; idx < nb_items * pmid; idx += 32) {
-            int j = idx / pmid;
-            int rem = idx - j * pmid;
-            int t = rem / (dv * d0);
-            int r2 = rem - t * dv * d0;
-            int x = r2 / d0, z = r2 - x * d0;
-            const double *Tt = T + (size_t)j * slab + t * dv * d1;
+          __syncwarp();
+          const int per = r * dvp * ncol;
+          for (int idx = lane; idx < nb_items * per; idx += 32) {
+            int j = idx / per;
+            int rem = idx - j * per;
+            int t = rem / (dvp * ncol);
+            int r2 = rem - t * dvp * ncol;
+            int x = r2 / ncol, z = r2 - x * ncol;
+            const ItemState &S = ist[j];
+            const double *F = B.ops + S.opoff;
+            const double *Tt = T + (size_t)j * slab + t * dv * ncol;
             double a = 0.0;
-            for (int kap = 0; kap < qs; ++kap) {
-              const int ok = B.set_to_orb[pk * n + kap];
-              double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
-              if (h == 0.0) continue;
-              const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0;
-              double tf = 0.0;
-              for (int y = 0; y < d1; ++y) tf = add(tf, mul(Tt[x * d1 + y], Fk[y * d0 + z]));
-              a = add(a, mul(mul(hs, h), tf));
+            for (int y = 0; y < dv; ++y) a = fmad(F[x * dv + y], Tt[y * ncol + z], a);
+            if (S.kcol >= 0) a = mul(a, (S.kneg ? B.kitm : B.kitp)[(size_t)t * p + S.kcol]);
+            X[(size_t)j * slab + rem] = a;
+          }
+          __syncwarp();
+          double *tmp = T; T = X; X = tmp;
+        } else if (kind == 1) {
+          // ---- edge e: T <- conv(G_b * prod K, T)  (integrate_left_edge, time-ordered convolution);
+          // edge v follows vertex v before the zero vertex, edge v - 1 precedes vertex v after it
+          const int e = v < vct0 ? v : v - 1;
+          const int b = C.ind_path[e];
+          const int d = C.bdims[e + 1];
+          const int dd = d * d, dc = d * ncol;
+          if (lane < nb_items) {
+            ItemState &S = ist[lane];
+            int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
+            for (int i = 1; i < m; ++i)
+              if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
+                sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
+                lp[nf] = S.lpole[i];
+                nf++;
+              }
+            long sig = 0;
+            if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
+            if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
+            S.taboff = B.tab_off[b] + sig * 2 * r * dd;
+          }
+          __syncwarp();
+          // (a) gc = K^-1 T (in place) and Gt = W gc (into X), one (item, column) per lane
+          for (int cl = lane; cl < nb_items * dc; cl += 32) {
+            const int j = cl / dc, col = cl - j * dc;
+            double *Tj = T + (size_t)j * slab;
+            double x[RP];
+#pragma unroll
+            for (int i = 0; i < RP; ++i) {
+              int src = sPerm[i];
+              x[i] = src >= 0 ? Tj[src * dc + col] : 0.0;
             }
+            lu_solve_reg<RP>(sLU, x);
+#pragma unroll
+            for (int i = 0; i < RP; ++i)
+              if (i < r) Tj[i * dc + col] = x[i];
+            matvec_reg<RP>(sW, x, r, X + (size_t)j * slab + col, dc);
+          }
+          __syncwarp();
+          // (b) Q_l = Ft_l gc_l + fc_l Gt_l  (into Y)
+          const int per = r * dc;
+          for (int idx = lane; idx < nb_items * per; idx += 32) {
+            int j = idx / per;
+            int rem = idx - j * per;
+            int l = rem / dc;
+            int r2 = rem - l * dc;
+            int x = r2 / ncol, z = r2 - x * ncol;
+            const double *tb = B.tab + ist[j].taboff;
+            const double *fl = tb + l * dd, *ftl = tb + (long)r * dd + l * dd;
+            const double *gl = T + (size_t)j * slab + l * dc, *gtl = X + (size_t)j * slab + l * dc;
+            double a = 0.0;
+            for (int y = 0; y < d; ++y) a = fmad(ftl[x * d + y], gl[y * ncol + z], fmad(fl[x * d + y], gtl[y * ncol + z], a));
             Y[(size_t)j * slab + rem] = a;
           }
           __syncwarp();
-          const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
-          for (int idx = lane; idx < nb_items * pout; idx += 32) {
-            int j = idx / pout;
-            int rem = idx - j * pout;
-            int t = rem / (dvp * d0);
-            int r2 = rem - t * dvp * d0;
-            int x = r2 / d0, z = r2 - x * d0;
-            const double *Yt = Y + (size_t)j * slab + t * dv * d0;
-            double a = 0.0;
-            for (int y = 0; y < dv; ++y) a = add(a, mul(Fm[x * dv + y], Yt[y * d0 + z]));
-            X[(size_t)j * slab + rem] = add(X[(size_t)j * slab + rem], a);
+          // (c) h1 = (beta K) Q  (into X, Gt no longer needed)
+          for (int cl = lane; cl < nb_items * dc; cl += 32) {
+            const int j = cl / dc, col = cl - j * dc;
+            const double *Yj = Y + (size_t)j * slab;
+            double q[RP];
+#pragma unroll
+            for (int i = 0; i < RP; ++i) q[i] = i < r ? Yj[i * dc + col] : 0.0;
+            matvec_reg<RP>(sBK, q, r, X + (size_t)j * slab + col, dc);
           }
           __syncwarp();
+          // (d) P'_l = K(0, om_l) (fc_l gc_l)  (into Y)
+          for (int idx = lane; idx < nb_items * per; idx += 32) {
+            int j = idx / per;
+            int rem = idx - j * per;
+            int l = rem / dc;
+            int r2 = rem - l * dc;
+            int x = r2 / ncol, z = r2 - x * ncol;
+            const double *fl = B.tab + ist[j].taboff + l * dd;
+            const double *gl = T + (size_t)j * slab + l * dc;
+            double a = 0.0;
+            for (int y = 0; y < d; ++y) a = fmad(fl[x * d + y], gl[y * ncol + z], a);
+            Y[(size_t)j * slab + rem] = mul(B.k0[l], a);
+          }
+          __syncwarp();
+          // (e) h = h1 + t_i (beta K) P'  (into T)
+          for (int cl = lane; cl < nb_items * dc; cl += 32) {
+            const int j = cl / dc, col = cl - j * dc;
+            const double *Yj = Y + (size_t)j * slab;
+            double q[RP];
+#pragma unroll
+            for (int i = 0; i < RP; ++i) q[i] = i < r ? Yj[i * dc + col] : 0.0;
+            double *Tj = T + (size_t)j * slab;
+            const double *h1 = X + (size_t)j * slab;
+            constexpr int CH = 8;
+#pragma unroll 1
+            for (int l0 = 0; l0 < RP; l0 += CH) {
+              if (l0 >= r) break;
+              double a[CH];
+#pragma unroll
+              for (int jj = 0; jj < CH; ++jj) a[jj] = 0.0;
+#pragma unroll
+              for (int k = 0; k < RP; ++k) {
+#pragma unroll
+                for (int jj = 0; jj < CH; ++jj) a[jj] = fmad(sBK[k * RP + l0 + jj], q[k], a[jj]);
+              }
+#pragma unroll
+              for (int jj = 0; jj < CH; ++jj) {
+                int i = l0 + jj;
+                if (i < r) Tj[i * dc + col] = fmad(B.tabs[i], a[jj], h1[i * dc + col]);
+              }
+            }
+          }
+          __syncwarp();
+        } else {
+          // ---- zero vertex (multiply_left_vertex_and_right_zero_vertex)
+          const int b_mu = C.ind_path[v - 1];
+          const int dv = C.bdims[v], dvp = C.bdims[v + 1];
+          const bool fwd = C.fbmask & 1;
+          const int pk = C.pk;
+          const long ok_off = fwd ? B.F_off[pk * B.nb + C.b_out] : B.Fd_off[pk * B.nb + C.b_out];
+          const long om_off = fwd ? B.Fd_off[pk * B.nb + b_mu] : B.F_off[pk * B.nb + b_mu];
+          const double hs = fwd ? 1.0 : -1.0;
+          int qs = 0;
+          for (int i = 0; i < n; ++i)
+            if (B.set_to_orb[pk * n + i] >= 0) qs = i + 1;
+          const int pout = r * dvp * d0, pmid = r * dv * d0;
+          for (int idx = lane; idx < nb_items * pout; idx += 32) {
+            int j = idx / pout;
+            X[(size_t)j * slab + (idx - j * pout)] = 0.0;
+          }
+          __syncwarp();
+          for (int mu = 0; mu < qs; ++mu) {
+            const int om = B.set_to_orb[pk * n + mu];
+            for (int idx = lane; idx < nb_items * pmid; idx += 32) {
+              int j = idx / pmid;
+              int rem = idx - j * pmid;
+              int t = rem / (dv * d0);
+              int r2 = rem - t * dv * d0;
+              int x = r2 / d0, z = r2 - x * d0;
+              const double *Tt = T + (size_t)j * slab + t * dv * d1;
+              double a = 0.0;
+              for (int kap = 0; kap < qs; ++kap) {
+                const int ok = B.set_to_orb[pk * n + kap];
+                double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
+                if (h == 0.0) continue;
+                const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0;
+                double tf = 0.0;
+                for (int y = 0; y < d1; ++y) tf = fmad(Tt[x * d1 + y], Fk[y * d0 + z], tf);
+                a = fmad(mul(hs, h), tf, a);
+              }
+              Y[(size_t)j * slab + rem] = a;
+            }
+            __syncwarp();
+            const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
+            for (int idx = lane; idx < nb_items * pout; idx += 32) {
+              int j = idx / pout;
+              int rem = idx - j * pout;
+              int t = rem / (dvp * d0);
+              int r2 = rem - t * dvp * d0;
+              int x = r2 / d0, z = r2 - x * d0;
+              const double *Yt = Y + (size_t)j * slab + t * dv * d0;
+              double a = 0.0;
+              for (int y = 0; y < dv; ++y) a = fmad(Fm[x * dv + y], Yt[y * d0 + z], a);
+              X[(size_t)j * slab + rem] = add(X[(size_t)j * slab + rem], a);
+            }
+            __syncwarp();
+          }
+          double *tmp = T; T = X; X = tmp;
         }
-        double *tmp = T; T = X; X = tmp;
-      }
-      for (int v = vct0 + 1; v < 2 * m; ++v) {
-        edge(v - 1, d0);
-        vertex(v, d0);
       }
       // ---- prefactor and signs, the |T| > 1e-16 guard, accumulation in item order
       const int tot = r * dout * d0;
@@ -1070,12 +1067,13 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
   c->LUp.assign((size_t)RP * RP, 0.0); c->Wp.assign((size_t)RP * RP, 0.0); c->BKp.assign((size_t)RP * RP, 0.0);
   for (int i = 0; i < RP; ++i)
     for (int k = 0; k < RP; ++k) {
+      // column-major: element (row i, column k) at k * RP + i
       if (i < r && k < r) {
-        c->LUp[(size_t)i * RP + k] = c->LU[(size_t)i * r + k];
-        c->Wp[(size_t)i * RP + k] = c->W[(size_t)i * r + k];
-        c->BKp[(size_t)i * RP + k] = beta * c->Kit[(size_t)i * r + k];
+        c->LUp[(size_t)k * RP + i] = c->LU[(size_t)i * r + k];
+        c->Wp[(size_t)k * RP + i] = c->W[(size_t)i * r + k];
+        c->BKp[(size_t)k * RP + i] = beta * c->Kit[(size_t)i * r + k];
       } else if (i == k) {
-        c->LUp[(size_t)i * RP + k] = 1.0;
+        c->LUp[(size_t)k * RP + i] = 1.0;
       }
     }
   c->perm.assign(RP, -1);
