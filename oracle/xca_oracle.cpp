@@ -141,7 +141,7 @@ struct Dlr {
     for (int i = 0; i < r; ++i)
       for (long j = 0; j < ncol; ++j) {
         cd s = 0;
-        for (int l = 0; l < r; ++l) s += refl[(size_t)i * r + l] * c[(size_t)l * ncol + j];
+        for (int l = 0; l < r; ++l) s = dfma(refl[(size_t)i * r + l], c[(size_t)l * ncol + j], s);
         out[(size_t)i * ncol + j] = s;
       }
   }
@@ -777,13 +777,13 @@ void eval_correlator(const Evaluator &E, const Backbone &B, const BlockG &G, con
         for (int i = 0; i < c2; ++i)
           for (int j = 0; j < c0; ++j) {
             cd s = 0;
-            for (int k = 0; k < c1; ++k) s += Omu[i * c1 + k] * Rt[k * c0 + j];
+            for (int k = 0; k < c1; ++k) s = cfma(Omu[i * c1 + k], Rt[k * c0 + j], s);
             tmp[i * c0 + j] = s;
           }
         for (int i = 0; i < c3; ++i)
           for (int j = 0; j < c0; ++j) {
             cd s = 0;
-            for (int k = 0; k < c2; ++k) s += Lt[i * lC[e1] + k] * tmp[k * c0 + j];
+            for (int k = 0; k < c2; ++k) s = cfma(Lt[i * lC[e1] + k], tmp[k * c0 + j], s);
             tmuop[i * c0 + j] = s;
           }
         for (int ka = 0; ka < nka; ++ka) {
@@ -791,7 +791,7 @@ void eval_correlator(const Evaluator &E, const Backbone &B, const BlockG &G, con
           const cd *Ok = kap_ops[ka].blk[e2];  // (c0 x c3)
           cd s = 0;
           for (int i = 0; i < c3; ++i)
-            for (int j = 0; j < c0; ++j) s += tmuop[i * c0 + j] * Ok[j * c3 + i];
+            for (int j = 0; j < c0; ++j) s = cfma(tmuop[i * c0 + j], Ok[j * c3 + i], s);
           corr[((size_t)t * nmu + mu) * nka + ka] += s;
         }
       }
