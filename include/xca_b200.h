@@ -92,6 +92,22 @@ int xca_compute_self_energy_device(xca_ctx *ctx, const double *G_dev, int m, con
 int xca_compute_self_energy_device_shard(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
                                          double *Sigma_dev, int shard, int n_shards);
 
+/* Allocation-free variant of xca_compute_self_energy_device, for callers that must not allocate device
+ * memory while they run: code that works inside a pre-sized memory pool or arena (a serving process that
+ * reserved its HBM up front, a solver embedded in a framework that owns the device allocator), where a
+ * cudaMalloc would fail, stall the device or break the owner's accounting.  No counterpart in the
+ * reference.  Same arguments and result as xca_compute_self_energy_device; the per-call scratch (edge
+ * tables, work list, block norms, unit counter) lives in one fixed 64 MiB array compiled into the
+ * library, which every device that loads the library holds until the process exits.  The call itself
+ * makes no cudaMalloc/cudaFree; the evaluator's set-up (xca_evaluator_setup) still allocates its tables
+ * once beforehand.  Sizes whose scratch exceeds 64 MiB are rejected with XCA_ERR_INVALID before any
+ * launch (for example third-order topologies on large bases: the edge tables grow as p^2).  The first
+ * call on a device looks up the array's device address (once per device, with that device current);
+ * make that first call before any stream capture.  All calls on a device share the array: calls that
+ * overlap on the GPU (other contexts or threads on the same device) race and must be serialised. */
+int xca_compute_self_energy_device_noalloc(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
+                                           double *Sigma_dev);
+
 /* Zero n_doubles of device memory on the context's stream. */
 int xca_zero_device(xca_ctx *ctx, double *dev, long n_doubles);
 

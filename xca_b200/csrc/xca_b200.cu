@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -545,6 +546,7 @@ struct Ctx {
   DevBuf<double> d_G, d_Sig, d_maxabs;
   std::vector<std::unique_ptr<DevBuf<double>>> user_bufs;
   std::map<std::string, std::unique_ptr<ClassSet>> class_cache;
+  std::map<std::string, std::unique_ptr<ClassSet>> noalloc_classes;  // host-only work lists of the allocation-free call
   int unit_batches = 4;  // lockstep batches per work unit
   // profiling: CUDA events around every Sigma launch (enabled on request), user events, L2 flush buffer
   bool profile = false;
@@ -591,14 +593,17 @@ static long ipow(long a, int e) {
 // Validity of a block path depends on the directions, the orbital tuple, the output block, the
 // symmetry set and the zero-block flags of G, never on the pole tuple, so it is enumerated once per
 // (topology, zero pattern) and every valid path class stands for p^(m-1) items.
-static ClassSet *get_classes(Ctx *c, const Topology &T, const std::vector<int> &zero) {
+static std::string class_key(const Topology &T, const std::vector<int> &zero) {
   std::ostringstream key;
   key << T.m;
   for (int i = 0; i < T.m; ++i) key << ":" << T.t[i][0] << "," << T.t[i][1];
   key << "|";
   for (int z : zero) key << (z ? '0' : '1');
-  auto itc = c->class_cache.find(key.str());
-  if (itc != c->class_cache.end()) return itc->second.get();
+  return key.str();
+}
+
+// Host side of the work list: the path classes and their work units (no device memory touched).
+static std::unique_ptr<ClassSet> build_classes(Ctx *c, const Topology &T, const std::vector<int> &zero) {
   auto cs = std::make_unique<ClassSet>();
   const int m = T.m, nv = 2 * m, vct0 = T.t[0][1];
   const long fbmax = 1L << m, omax = ipow(c->n, m - 1);
@@ -695,10 +700,18 @@ static ClassSet *get_classes(Ctx *c, const Topology &T, const std::vector<int> &
     }
   }
   cs->n_items = (long long)cs->classes.size() * npt;
+  return cs;
+}
+
+static ClassSet *get_classes(Ctx *c, const Topology &T, const std::vector<int> &zero) {
+  const std::string key = class_key(T, zero);
+  auto itc = c->class_cache.find(key);
+  if (itc != c->class_cache.end()) return itc->second.get();
+  auto cs = build_classes(c, T, zero);
   cs->d_classes.upload(cs->classes, c->stream);
   cs->d_units.upload(cs->units, c->stream);
   ClassSet *ret = cs.get();
-  c->class_cache[key.str()] = std::move(cs);
+  c->class_cache[key] = std::move(cs);
   return ret;
 }
 
@@ -832,6 +845,61 @@ static void real_part(const double *cplx, long n, std::vector<double> &out, cons
       throw Error(XCA_ERR_UNSUPPORTED, std::string(what) + " has a non-zero imaginary part; the device path computes in real FP64");
     out[i] = cplx[2 * i];
   }
+}
+
+
+// -------------------------------------------------------------------------------- allocation-free Sigma
+// xca_compute_self_energy_device_noalloc keeps everything it needs beyond its inputs, its output and the
+// evaluator's set-up tables in this fixed array of the library's device image, so the call itself never
+// allocates device memory.  Every device that loads the library holds the array until the process exits.
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(64) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mu;
+static std::map<int, unsigned char *> g_noalloc_base;  // device ordinal -> device address of the array
+
+// Device address of the scratch array on `device`, which must be current.  In host code the array's name
+// is only a host-side stand-in, so its address is looked up once per device and cached.
+static unsigned char *noalloc_scratch(int device) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  auto it = g_noalloc_base.find(device);
+  if (it != g_noalloc_base.end()) return it->second;
+  void *ptr = nullptr;
+  CUDA_CHECK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+  auto *base = static_cast<unsigned char *>(ptr);
+  g_noalloc_base[device] = base;
+  return base;
+}
+
+static size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+static void noalloc_fits(size_t need, const char *what) {
+  if (need > NOALLOC_SCRATCH_BYTES)
+    throw Error(XCA_ERR_INVALID, std::string("xca_compute_self_energy_device_noalloc: ") + what + " need " +
+                                     std::to_string(need) + " bytes of scratch, the fixed scratch array holds " +
+                                     std::to_string(NOALLOC_SCRATCH_BYTES) + "; use xca_compute_self_energy_device");
+}
+
+template <int RP>
+static void launch_noalloc_rp(Ctx *c, const DevBasis &B, long pairs, const ClassRec *classes, const WorkUnit *units,
+                              int n_units, int *counter, const double *G_dev, double *Sig_dev, double scale) {
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  size_t tsm = (2 * (size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
+  CUDA_CHECK(cudaFuncSetAttribute(edge_table_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+  long tblocks = std::min<long>((pairs + 3) / 4, (long)nsm * 16);
+  edge_table_kernel<RP><<<(int)std::max<long>(1, tblocks), 128, tsm, c->stream>>>(B, G_dev, pairs);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+  if (n_units == 0) return;
+  int warps = sigma_warps(c);
+  size_t smem = sigma_smem_bytes(c, warps);
+  CUDA_CHECK(cudaFuncSetAttribute(sigma_items_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int grid = std::max(1, std::min<int>(nsm, (n_units + warps - 1) / warps));
+  sigma_items_kernel<RP><<<grid, 32 * warps, smem, c->stream>>>(B, classes, units, n_units, counter, G_dev, Sig_dev, scale,
+                                                                c->nmax);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
 }
 
 }  // namespace xca
@@ -1108,6 +1176,7 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
   c->d_dims.upload(c->dims, s); c->d_set_to_orb.upload(c->set_to_orb, s); c->d_goff.upload(c->goff, s);
   c->d_F_off.upload(c->F_off, s); c->d_Fd_off.upload(c->Fd_off, s); c->d_Fb_off.upload(c->Fb_off, s); c->d_Fdb_off.upload(c->Fdb_off, s);
   c->class_cache.clear();
+  c->noalloc_classes.clear();
   CUDA_CHECK(cudaStreamSynchronize(s));
   c->ready = true;
   API_END
@@ -1456,6 +1525,72 @@ int xca_synchronize(xca_ctx *ctx) {
 int xca_kernel_launches(xca_ctx *ctx, long *out) {
   API_BEGIN
   *out = reinterpret_cast<Ctx *>(ctx)->launches;
+  API_END
+}
+
+int xca_compute_self_energy_device_noalloc(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
+                                           double *Sigma_dev) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c->ready) throw Error(XCA_ERR_INVALID, "evaluator not set up");
+  set_device(c);
+  Topology T = parse_topology(m, topology);
+  unsigned char *base = noalloc_scratch(c->device);
+  const int nb = c->nb, r = c->r;
+  const int nsig = (m >= 3) ? (int)c->nsig_alloc : 1 + 2 * c->p;
+  // layout: unit counter | block max |G| | edge-table offsets | edge tables | path classes | work units
+  const size_t off_counter = 0;
+  const size_t off_maxabs = 256;
+  const size_t off_taboff = off_maxabs + align256((size_t)nb * sizeof(double));
+  const size_t off_tab = off_taboff + align256((size_t)nb * sizeof(long));
+  std::vector<long> tab_off(nb);
+  long tab_doubles = 0;
+  for (int b = 0; b < nb; ++b) {
+    tab_off[b] = tab_doubles;
+    tab_doubles += (long)nsig * 2L * r * c->dims[b] * c->dims[b];
+  }
+  const size_t off_classes = off_tab + align256((size_t)tab_doubles * sizeof(double));
+  noalloc_fits(off_classes, "the edge tables of this topology order");
+  // zero-block flags of G (max |G_b| < 1e-16: c++/triqs_xca/block_sparse.cpp:45-49, used at block_sparse_backbone.cpp:248)
+  double *maxabs = reinterpret_cast<double *>(base + off_maxabs);
+  block_maxabs_kernel<<<nb, 256, 0, c->stream>>>(G_dev, c->d_goff.ptr, c->d_dims.ptr, r, nb, maxabs);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+  std::vector<double> mx(nb);
+  CUDA_CHECK(cudaMemcpyAsync(mx.data(), maxabs, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  std::vector<int> zero(nb);
+  for (int b = 0; b < nb; ++b) zero[b] = mx[b] < 1e-16 ? 1 : 0;
+  // host work list, cached per (topology, zero pattern)
+  const std::string key = class_key(T, zero);
+  auto itc = c->noalloc_classes.find(key);
+  if (itc == c->noalloc_classes.end()) itc = c->noalloc_classes.emplace(key, build_classes(c, T, zero)).first;
+  const ClassSet *cs = itc->second.get();
+  const size_t off_units = off_classes + align256(cs->classes.size() * sizeof(ClassRec));
+  noalloc_fits(off_units + cs->units.size() * sizeof(WorkUnit), "the edge tables and work list of this topology");
+  // contents: everything is rewritten before use except the unit counter, which must start at zero
+  auto *d_tab_off = reinterpret_cast<long *>(base + off_taboff);
+  auto *d_classes = reinterpret_cast<ClassRec *>(base + off_classes);
+  auto *d_units = reinterpret_cast<WorkUnit *>(base + off_units);
+  auto *counter = reinterpret_cast<int *>(base + off_counter);
+  CUDA_CHECK(cudaMemcpyAsync(d_tab_off, tab_off.data(), nb * sizeof(long), cudaMemcpyHostToDevice, c->stream));
+  if (!cs->classes.empty())
+    CUDA_CHECK(cudaMemcpyAsync(d_classes, cs->classes.data(), cs->classes.size() * sizeof(ClassRec), cudaMemcpyHostToDevice,
+                               c->stream));
+  if (!cs->units.empty())
+    CUDA_CHECK(cudaMemcpyAsync(d_units, cs->units.data(), cs->units.size() * sizeof(WorkUnit), cudaMemcpyHostToDevice,
+                               c->stream));
+  CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
+  DevBasis B = c->basis(nsig);
+  B.tab = reinterpret_cast<const double *>(base + off_tab);
+  B.tab_off = d_tab_off;
+  const long pairs = (long)nb * nsig;
+  const int n_units = (int)cs->units.size();
+  switch (c->RP) {
+    case 32: launch_noalloc_rp<32>(c, B, pairs, d_classes, d_units, n_units, counter, G_dev, Sigma_dev, scale); break;
+    case 48: launch_noalloc_rp<48>(c, B, pairs, d_classes, d_units, n_units, counter, G_dev, Sigma_dev, scale); break;
+    default: launch_noalloc_rp<64>(c, B, pairs, d_classes, d_units, n_units, counter, G_dev, Sigma_dev, scale); break;
+  }
   API_END
 }
 
