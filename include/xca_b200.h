@@ -66,6 +66,45 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
                         int n_blocks, const int *block_dims, const int *F_index, const double *F_data,
                         const int *Fd_index, const double *Fd_data);
 
+/* DLR basis only (no hybridization, no operators): the state a standalone Dyson solver needs.
+ * dyson_it_ppsc's imtime_ops argument (c++/triqs_xca/dlr_dyson_ppsc.hpp:91-101; Python
+ * DysonItPPSC(beta, itops, g0), python/triqs_xca/dlr_dyson_ppsc.cpp:10-20) for n_blocks blocks of
+ * dimensions block_dims.  xca_evaluator_setup sets the same basis up as part of the evaluator. */
+int xca_basis_setup(xca_ctx *ctx, double beta, double lambda, double eps, int r, const double *rf, const double *it,
+                    int n_blocks, const int *block_dims);
+
+/* dyson_it_ppsc(beta, itops, g0) constructor for every block at once (dlr_dyson_ppsc.hpp:91-116; one
+ * object per block in python/triqs_xca/block_sparse_solver.py:136): uploads G0 (host packed complex
+ * slab, real data) and its DLR coefficients. */
+int xca_dyson_setup(xca_ctx *ctx, const double *G0);
+
+/* dyson_it_ppsc::solve(sig, eta) for every block (dlr_dyson_ppsc.hpp:135-168): G solving
+ * (I - G0 * (Sigma + eta)) G = G0 with the time-ordered DLR convolution.  hermitize != 0 adds the
+ * step of solve_dyson (python/triqs_xca/block_sparse_solver.py:582-586), G(t) <- (G(t) + G(t)^T) / 2.
+ * Host packed complex slabs in and out.  A singular system matrix gives XCA_ERR_RUNTIME. */
+int xca_dyson_solve(xca_ctx *ctx, const double *Sigma, double eta, int hermitize, double *G_out);
+
+/* Same on device-resident real slabs, asynchronous on the context's stream; a singular system is
+ * reported by the next xca_normalize_device or xca_dyson_solve. */
+int xca_dyson_solve_device(xca_ctx *ctx, const double *Sigma_dev, double eta, int hermitize, double *G_dev);
+
+/* trace(G) = sum_b Tr G_b(beta) by DLR evaluation at tau = beta (c++/triqs_xca/block_sparse.cpp:852-861);
+ * tr_out = (re, im).  Host packed complex slab or device real slab. */
+int xca_trace(xca_ctx *ctx, const double *G, double *tr_out);
+int xca_trace_device(xca_ctx *ctx, const double *G_dev, double *tr_out);
+
+/* normalize_pseudo_particle_gf (python/triqs_xca/block_sparse_solver.py:427-449) on a device slab:
+ * Z = -Re trace(G), deta = log|Z| / beta, G(tau) <- G(tau) exp(-tau deta); returns Z and deta (the
+ * caller adds deta to eta). */
+int xca_normalize_device(xca_ctx *ctx, double *G_dev, double *Z, double *deta);
+
+/* max_abs_diff_BlockGf (python/triqs_xca/block_sparse_solver.py:1379-1380) of two device slabs. */
+int xca_max_abs_diff_device(xca_ctx *ctx, const double *a_dev, const double *b_dev, double *out);
+
+/* y <- alpha x + beta y on device slabs: the mixing step G = mix G_new + (1 - mix) G of
+ * python/triqs_xca/block_sparse_solver.py:346. */
+int xca_axpby_device(xca_ctx *ctx, double alpha, const double *x_dev, double beta, double *y_dev);
+
 /* DiagramEvaluator::get_num_self_energy_backbones, c++/triqs_xca/block_sparse_backbone.cpp:721-724. */
 int xca_num_self_energy_backbones(xca_ctx *ctx, int m, const int *topology, long *out);
 

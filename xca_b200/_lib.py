@@ -36,6 +36,15 @@ SIGNATURES = {
     "xca_ctx_create": [I, ctypes.POINTER(P)],
     "xca_ctx_destroy": [P],
     "xca_evaluator_setup": [P, D, D, D, I, dp, dp, I, dp, dp, I, lp, I, ip, ip, dp, ip, dp],
+    "xca_basis_setup": [P, D, D, D, I, dp, dp, I, ip],
+    "xca_dyson_setup": [P, dp],
+    "xca_dyson_solve": [P, dp, D, I, dp],
+    "xca_dyson_solve_device": [P, P, D, I, P],
+    "xca_trace": [P, dp, dp],
+    "xca_trace_device": [P, P, dp],
+    "xca_normalize_device": [P, P, dp, dp],
+    "xca_max_abs_diff_device": [P, P, P, dp],
+    "xca_axpby_device": [P, D, P, D, P],
     "xca_num_self_energy_backbones": [P, I, ip, lp],
     "xca_num_single_ptcle_gf_backbones": [P, I, ip, lp],
     "xca_compute_self_energy": [P, dp, I, ip, lp, L, dp],

@@ -191,7 +191,45 @@ class DiagramEvaluator:
                                            rows_n, ctypes.byref(n)))
         return rows[:rows_n]
 
+    def trace(self, G_ppsc):
+        """sum_b Tr G_b(beta) from the DLR expansion of each block (``trace``, block_sparse.cpp:852-861)."""
+        g = self.pack(G_ppsc)
+        out = np.zeros(2)
+        _lib.check(_lib.lib().xca_trace(self._ctx, _lib.as_dp(g.view(np.float64)), _lib.as_dp(out)))
+        return complex(out[0], out[1])
+
     # ---------------------------------------------------------------- device-resident use
+    def dyson_setup(self, G0):
+        """Dyson solvers of every block for the atomic propagator G0 (``DysonItPPSC(beta, itops, G0_b)`` for each
+        block, block_sparse_solver.py:136)."""
+        g0 = self.pack(G0)
+        _lib.check(_lib.lib().xca_dyson_setup(self._ctx, _lib.as_dp(g0.view(np.float64))))
+
+    def dyson_solve_device(self, Sigma_dev, eta, G_dev, hermitize=True):
+        _lib.check(_lib.lib().xca_dyson_solve_device(self._ctx, ctypes.c_void_p(Sigma_dev), float(eta), int(bool(hermitize)),
+                                                     ctypes.c_void_p(G_dev)))
+
+    def normalize_device(self, G_dev):
+        """Classic normalisation of a device slab in place; returns (Z, deta)."""
+        Z, de = ctypes.c_double(), ctypes.c_double()
+        _lib.check(_lib.lib().xca_normalize_device(self._ctx, ctypes.c_void_p(G_dev), ctypes.byref(Z), ctypes.byref(de)))
+        return Z.value, de.value
+
+    def trace_device(self, G_dev):
+        out = np.zeros(2)
+        _lib.check(_lib.lib().xca_trace_device(self._ctx, ctypes.c_void_p(G_dev), _lib.as_dp(out)))
+        return complex(out[0], out[1])
+
+    def max_abs_diff_device(self, a_dev, b_dev):
+        out = ctypes.c_double()
+        _lib.check(_lib.lib().xca_max_abs_diff_device(self._ctx, ctypes.c_void_p(a_dev), ctypes.c_void_p(b_dev),
+                                                      ctypes.byref(out)))
+        return out.value
+
+    def axpby_device(self, alpha, x_dev, beta, y_dev):
+        _lib.check(_lib.lib().xca_axpby_device(self._ctx, float(alpha), ctypes.c_void_p(x_dev), float(beta),
+                                               ctypes.c_void_p(y_dev)))
+
     def device_buffer(self, slot, n_doubles):
         ptr = ctypes.POINTER(ctypes.c_double)()
         _lib.check(_lib.lib().xca_device_buffer(self._ctx, int(slot), int(n_doubles) * 8, ctypes.byref(ptr)))

@@ -1,0 +1,149 @@
+"""Self-consistent pseudo-particle solve with the reference's Python interface
+(``BlockSparseSolver``, ``python/triqs_xca/block_sparse_solver.py:36-355``), device resident.
+
+The pseudo-particle propagator, self-energy and Dyson state stay in GPU memory across iterations; each
+iteration launches the Sigma evaluation of every order and topology (accumulated with the reference's
+signs, :597-640), the Dyson solve with hermitization (:572-590), the 'classic' normalisation
+(:427-449) and the convergence test (:338, :1379-1380); only three scalars per iteration (Z, deta,
+diff_G) come back to the host.
+
+TRIQS is not available here, so the local problem is given as an ``xca_b200.atom_diag.AtomDiag`` and the
+hybridization as a dense ``(r, n, n)`` array of Delta(tau) on the DLR nodes (``Delta_tau``); with
+``hyb_comp=False`` the solver fits it on the DLR poles exactly as the reference does (:171-176).
+Adapol pole compression (``hyb_comp=True``) is not available.
+"""
+
+import time
+
+import numpy as np
+
+from . import diag
+from .atom_diag import atomic_pseudo_particle_greens_function
+from .block_sparse import BlockOpSymQuartet, DiagramEvaluator
+from .models import dlr_fit_hybridization, rel2abs
+from .pycppdlr import MeshDLRImTime
+
+# device buffer slots of the solver's slabs (the evaluator's buffers 0..9 stay free for callers)
+_SLOTS = {"G": 10, "Gn": 11, "S": 12}
+
+
+class BlockSparseSolver:
+    def __init__(self, atom_diag, beta, w_max, eps, device=0, verbose=False):
+        self.ad = atom_diag
+        self.beta = float(beta)
+        self.w_max = float(w_max)
+        self.eps = float(eps)
+        self.device = device
+        self.verbose = verbose
+        self.mesh_tau = MeshDLRImTime(beta=self.beta, statistic="Fermion", w_max=self.w_max, eps=self.eps)
+        self.rf = self.mesh_tau.dlr_rf
+        self.it = self.mesh_tau.dlr_it.it
+        self.r = len(self.rf)
+        self.n = atom_diag.n
+        self.tau = self.beta * rel2abs(self.it)
+        self.Delta_tau = np.zeros((self.r, self.n, self.n), np.complex128)
+        self.G0, self.eta0 = atomic_pseudo_particle_greens_function(atom_diag, self.beta, self.tau)
+        self.G = [g.copy() for g in self.G0]
+        self.Sigma = [np.zeros_like(g) for g in self.G0]
+        self.eta = 0.0
+        self.Fq = BlockOpSymQuartet.from_atom_diag(atom_diag)
+        self.d = None
+        self.G_tau = None
+        self.timings = {}
+
+    # -- hybridization (hyb_comp=False path of fit_hybridization, block_sparse_solver.py:146-185)
+    def fit_hybridization(self, compression=False):
+        if compression:
+            raise NotImplementedError("adapol pole compression is not available; use hyb_comp=False")
+        self.hyb_poles, self.hyb_coeffs = dlr_fit_hybridization(self.rf, self.it, self.beta, self.Delta_tau)
+
+    def init_diagram_evaluator(self):
+        self.d = DiagramEvaluator.from_arrays(self.beta, self.beta * self.w_max, self.eps, self.rf, self.it, self.hyb_poles,
+                                              self.hyb_coeffs, self.Fq, device=self.device)
+        self.d.dyson_setup(self.G0)
+        self._buf = {k: self.d.device_buffer(slot, self.d.slab) for k, slot in _SLOTS.items()}
+
+    def _ensure_evaluator(self):
+        if self.d is None:
+            self.fit_hybridization()
+            self.init_diagram_evaluator()
+
+    def _upload(self, key, blocks):
+        self.d.to_device(self._buf[key], np.concatenate([np.asarray(g).real.ravel() for g in blocks]))
+
+    def _download(self, key):
+        return [x.astype(np.complex128) for x in self.d.unpack(self.d.to_host(self._buf[key], self.d.slab))]
+
+    def _sigma_device(self, max_order):
+        d = self.d
+        d.zero_device(self._buf["S"], d.slab)
+        for order in range(1, max_order + 1):
+            for sign, topo in diag.all_connected_pairings(order):
+                # (-1)^order * parity * (-1)^(order+1): the order loop's and the topology loop's signs
+                fac = (-1) ** order * sign * (-1) ** (order + 1)
+                d.compute_self_energy_device(self._buf["G"], topo, float(fac), self._buf["S"])
+
+    def solve(self, max_order, tol=1e-4, maxiter=10, mix=1.0, hyb_comp=False, normalization="classic", spgf_max_order=None,
+              verbose=None):
+        """BlockSparseSolver.solve (block_sparse_solver.py:240-355) with the 'classic' normalisation."""
+        if normalization != "classic":
+            raise NotImplementedError(f"normalization {normalization!r} is not available on the device path")
+        verbose = self.verbose if verbose is None else verbose
+        self.max_order = max_order
+        self.spgf_max_order = spgf_max_order if spgf_max_order is not None else max_order
+        self.fit_hybridization(compression=hyb_comp and max_order > 1)
+        self.init_diagram_evaluator()
+        d = self.d
+        self._upload("G", self.G)
+        it = 0
+        t0 = time.perf_counter()
+        for it in range(1, maxiter + 1):
+            self._sigma_device(max_order)
+            d.dyson_solve_device(self._buf["S"], self.eta, self._buf["Gn"], hermitize=True)
+            Z, deta = d.normalize_device(self._buf["Gn"])
+            self.eta += deta
+            self.diff_G = d.max_abs_diff_device(self._buf["Gn"], self._buf["G"])
+            if verbose:
+                print(f"iter = {it}, diff_G = {self.diff_G:2.2E}, Z = {Z:+2.6E}, eta = {self.eta:2.2E}")
+            if self.diff_G < tol:
+                break
+            d.axpby_device(mix, self._buf["Gn"], 1.0 - mix, self._buf["G"])
+        d.synchronize()
+        self.timings["solve_loop_s"] = time.perf_counter() - t0
+        self.n_ppsc_iter = it
+        self.G = self._download("G")
+        self.Sigma = self._download("S")
+        self.G_tau = None
+        if self.spgf_max_order > 0:
+            self.G_tau = self.eval_single_particle_greens_function(self.G, self.spgf_max_order)
+        return self
+
+    def eval_pseudo_particle_self_energy(self, G, max_order):
+        """Sigma of orders 1..max_order for a host G (block_sparse_solver.py:597-640)."""
+        self._ensure_evaluator()
+        self._upload("G", G)
+        self._sigma_device(max_order)
+        self.d.synchronize()
+        return self._download("S")
+
+    def solve_dyson(self, Sigma, eta):
+        """solve_dyson (block_sparse_solver.py:572-590): per-block Dyson solve, hermitized."""
+        self._ensure_evaluator()
+        self._upload("S", Sigma)
+        self.d.dyson_solve_device(self._buf["S"], eta, self._buf["Gn"], hermitize=True)
+        self.d.synchronize()
+        return self._download("Gn")
+
+    def eval_single_particle_greens_function(self, G, max_order):
+        """Single-particle G(tau) of orders 1..max_order (block_sparse_solver.py:657-698)."""
+        self._ensure_evaluator()
+        g = np.zeros((self.r, self.n, self.n), np.complex128)
+        for order in range(1, max_order + 1):
+            for sign, topo in diag.all_connected_pairings(order):
+                g += (-1) ** order * sign * self.d.compute_single_ptcle_gf(G, topo)
+        return g
+
+    def partition_function_from_ppgf(self, G):
+        """Z = -Re sum_b Tr G_b(beta) (block_sparse_solver.py:482-487)."""
+        self._ensure_evaluator()
+        return -self.d.trace(G).real

@@ -1,0 +1,383 @@
+// Pseudo-particle Dyson solve, trace and normalisation on the device (plain FP64 path).
+//
+// Per Fock-space block b (d = d_b, N = r d), following cppdlr's dyson_it_ppsc::solve
+// (c++/triqs_xca/dlr_dyson_ppsc.hpp:135-168) as called by solve_dyson
+// (python/triqs_xca/block_sparse_solver.py:572-590):
+//   sigc = K^-1 Sigma_b                                  (vals2coefs)
+//   ggs  = -(conv_TO(g0c, sigc) + eta G0_b)              (time-ordered DLR convolution, closed form)
+//   f    = K^-1 ggs,  ft = W f                           (coefficients of the system kernel)
+//   M    = convmat(f): (M g)(t_i) = int_0^tau f(tau - s) g(s) ds on the nodes, M = A K^-1
+//   (I + M) G = G0                                       (getrf with partial pivoting, getrs)
+//   G   <- (G + G^T) / 2                                 (hermitize, real data)
+// Matrices of all blocks are factorised concurrently, one CTA per block, in global memory (L2 resident
+// for the block sizes of the configurations here: sum_b (r d_b)^2 doubles).
+#pragma once
+#include "sigma_kernel.cuh"
+
+namespace xca {
+
+struct DysonBasis {
+  int r, nb;
+  double beta;
+  const double *LUp, *Wp, *BKp;  // RP x RP column-major (as DevBasis)
+  const int *perm;
+  const double *tabs, *k0, *k1;  // r: absolute t_i, K(0, om_l), K(1, om_l)
+  const double *rf;              // r: DLR frequencies om_l
+  const long *goff;              // nb: block offsets in a packed slab
+  const int *dims;               // nb
+  const long *woff;              // nb: per-block work offsets (6 r d^2 doubles each)
+  const long *moff;              // nb: per-block system matrix offsets ((r d)^2 doubles each)
+  const double *g0, *g0c, *g0t;  // packed slabs: G0 values, K^-1 G0, W K^-1 G0
+  double *work;
+  double *mats;
+};
+
+// K^T z = a for one register-resident row vector, with K = P L U (the factors of lu_factor): U^T y = a
+// row by row (i ascending: subtract U_ki y_k for k < i ascending, then divide by U_ii), L^T w = y
+// (i descending: subtract L_ki w_k for k > i ascending), each product and difference separately
+// rounded; then z = P w, i.e. z[perm[i]] = w[i] (the caller scatters).  Padding rows of LUT are the
+// identity.  LUT is column-major: LUT[i * RP + k] = LU(row k, column i).
+template <int RP>
+__device__ __forceinline__ void lu_solve_transposed_reg(const double *__restrict__ LUT, double (&x)[RP]) {
+#pragma unroll
+  for (int i = 0; i < RP; ++i) {
+#pragma unroll
+    for (int k = 0; k < i; ++k) x[i] = __dsub_rn(x[i], mul(LUT[i * RP + k], x[k]));
+    x[i] = __ddiv_rn(x[i], LUT[i * RP + i]);
+  }
+#pragma unroll
+  for (int i = RP - 1; i >= 0; --i) {
+#pragma unroll
+    for (int k = i + 1; k < RP; ++k) x[i] = __dsub_rn(x[i], mul(LUT[i * RP + k], x[k]));
+  }
+}
+
+// y_l = sum_k M[l][k] x_k for l < r with every product and sum separately rounded, k ascending from zero
+// (MT = M column-major); y written with stride `ld`.
+template <int RP>
+__device__ __forceinline__ void matvec_sep_reg(const double *__restrict__ MT, const double (&x)[RP], int r, double *y, int ld) {
+  constexpr int CH = 8;
+#pragma unroll 1
+  for (int l0 = 0; l0 < RP; l0 += CH) {
+    if (l0 >= r) break;
+    double acc[CH];
+#pragma unroll
+    for (int j = 0; j < CH; ++j) acc[j] = 0.0;
+#pragma unroll
+    for (int k = 0; k < RP; ++k) {
+#pragma unroll
+      for (int j = 0; j < CH; ++j) acc[j] = add(acc[j], mul(MT[k * RP + l0 + j], x[k]));
+    }
+#pragma unroll
+    for (int j = 0; j < CH; ++j)
+      if (l0 + j < r) y[(l0 + j) * ld] = acc[j];
+  }
+}
+
+// Stage the padded LU and W into shared memory (2 RP^2 doubles) and the pivot gather (RP ints).
+template <int RP>
+__device__ __forceinline__ void stage_lu_w(const DysonBasis &B, double *sLU, double *sW, int *sPerm) {
+  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
+    sLU[i] = B.LUp[i];
+    sW[i] = B.Wp[i];
+  }
+  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
+  __syncthreads();
+}
+
+// Columns (r-vectors with stride dd) of `src`: coefficients K^-1 src into `c` and W K^-1 src into `ct`
+// (fused multiply-adds as the convolution's Hilbert sums, or separately rounded as the convolution matrix's).
+template <int RP, bool FUSED>
+__device__ __forceinline__ void coefs_and_hilbert(const double *sLU, const double *sW, const int *sPerm, int r, int dd,
+                                                  const double *src, double *c, double *ct) {
+  for (int col = threadIdx.x; col < dd; col += blockDim.x) {
+    double x[RP];
+#pragma unroll
+    for (int i = 0; i < RP; ++i) {
+      const int s = sPerm[i];
+      x[i] = s >= 0 ? src[(size_t)s * dd + col] : 0.0;
+    }
+    lu_solve_reg<RP>(sLU, x);
+#pragma unroll
+    for (int i = 0; i < RP; ++i)
+      if (i < r) c[(size_t)i * dd + col] = x[i];
+    if (FUSED)
+      matvec_reg<RP>(sW, x, r, ct + col, dd);
+    else
+      matvec_sep_reg<RP>(sW, x, r, ct + col, dd);
+  }
+}
+
+// One CTA per block: sigc, gt, Q, P', ggs, then f = K^-1 ggs and ft = W f into the block's work area
+// [sigc | gt | Q | P' | f | ft], each r d^2 doubles.
+template <int RP>
+__global__ void __launch_bounds__(256) dyson_coef_kernel(DysonBasis B, const double *__restrict__ Sigma, double eta) {
+  extern __shared__ double smem[];
+  double *sLU = smem;
+  double *sW = sLU + RP * RP;
+  int *sPerm = reinterpret_cast<int *>(sW + RP * RP);
+  const int b = blockIdx.x;
+  if (b >= B.nb) return;
+  stage_lu_w<RP>(B, sLU, sW, sPerm);
+  const int r = B.r, d = B.dims[b], dd = d * d;
+  const long rdd = (long)r * dd;
+  double *w = B.work + B.woff[b];
+  double *sigc = w, *gt = w + rdd, *Q = w + 2 * rdd, *P = w + 3 * rdd, *f = w + 4 * rdd, *ft = w + 5 * rdd;
+  const double *sig = Sigma + B.goff[b];
+  const double *g0 = B.g0 + B.goff[b], *g0c = B.g0c + B.goff[b], *g0t = B.g0t + B.goff[b];
+  coefs_and_hilbert<RP, true>(sLU, sW, sPerm, r, dd, sig, sigc, gt);
+  __syncthreads();
+  // Q_l = ft_l g_l + f_l gt_l and P'_l = K_l(0) (f_l g_l) with f = g0c, g = sigc
+  for (long e = threadIdx.x; e < rdd; e += blockDim.x) {
+    const int l = (int)(e / dd), xz = (int)(e - (long)l * dd), x = xz / d, z = xz - x * d;
+    const double *fl = g0c + (long)l * dd, *fhl = g0t + (long)l * dd, *gl = sigc + (long)l * dd, *ghl = gt + (long)l * dd;
+    double sq = 0.0, sp = 0.0;
+    for (int y = 0; y < d; ++y) {
+      sq = fmad(fhl[x * d + y], gl[y * d + z], fmad(fl[x * d + y], ghl[y * d + z], sq));
+      sp = fmad(fl[x * d + y], gl[y * d + z], sp);
+    }
+    Q[e] = sq;
+    P[e] = mul(B.k0[l], sp);
+  }
+  __syncthreads();
+  // ggs(t_i) = -(h(t_i) + eta G0(t_i)), h = fma(t_i, h2, h1); stored in the sigc slot (no longer read)
+  for (long e = threadIdx.x; e < rdd; e += blockDim.x) {
+    const int i = (int)(e / dd), xz = (int)(e - (long)i * dd);
+    double h1 = 0.0, h2 = 0.0;
+    for (int l = 0; l < r; ++l) {
+      const double bk = B.BKp[l * RP + i];
+      h1 = fmad(bk, Q[(long)l * dd + xz], h1);
+      h2 = fmad(bk, P[(long)l * dd + xz], h2);
+    }
+    const double h = fmad(B.tabs[i], h2, h1);
+    sigc[e] = -add(h, mul(eta, g0[e]));
+  }
+  __syncthreads();
+  coefs_and_hilbert<RP, false>(sLU, sW, sPerm, r, dd, sigc, f, ft);
+}
+
+// Rows of the system matrix I + M, one thread per (block, i, x, y) row vector of A (convmat_inplace,
+// cppdlr; call site dlr_dyson_ppsc.hpp:149), in the operation order of the CPU restatement:
+//   A[i][k](x,y) = (beta K_ik) (ft_k + (t_i K_k(0)) f_k) + sum_{l != k, ascending} [((beta K_il) K_k(0)) / (om_k - om_l)] f_l
+// then M[(i,x), (i',y)] = (A K^-1)[i'] through K^T z = a.  grid.y = block, 64 threads per CTA.
+template <int RP>
+__global__ void __launch_bounds__(64) dyson_convmat_kernel(DysonBasis B) {
+  __shared__ double sf[RP * 64];
+  const int b = blockIdx.y;
+  const int r = B.r, d = B.dims[b], dd = d * d;
+  const long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = row < (long)r * dd;
+  const int i = active ? (int)(row / dd) : 0;
+  const int xy = active ? (int)(row - (long)i * dd) : 0;
+  const double *w = B.work + B.woff[b];
+  const long rdd = (long)r * dd;
+  const double *f = w + 4 * rdd, *ft = w + 5 * rdd;
+  // f_l of this thread's (x, y), one column of sf per thread
+  for (int l = 0; l < RP; ++l) sf[l * 64 + threadIdx.x] = (active && l < r) ? f[(long)l * dd + xy] : 0.0;
+  if (!active) return;
+  const double ti = B.tabs[i];
+  double a[RP];
+#pragma unroll
+  for (int k = 0; k < RP; ++k) {
+    double acc = 0.0;
+    if (k < r) {
+      const double k0k = B.k0[k], rfk = B.rf[k];
+      acc = mul(B.BKp[k * RP + i], add(ft[(long)k * dd + xy], mul(mul(ti, k0k), sf[k * 64 + threadIdx.x])));
+      for (int l = 0; l < r; ++l) {
+        if (l == k) continue;
+        const double wl = __ddiv_rn(mul(B.BKp[l * RP + i], k0k), __dsub_rn(rfk, B.rf[l]));
+        acc = add(acc, mul(wl, sf[l * 64 + threadIdx.x]));
+      }
+    }
+    a[k] = acc;
+  }
+  lu_solve_transposed_reg<RP>(B.LUp, a);
+  const int x = xy / d, y = xy - x * d;
+  const long N = (long)r * d;
+  double *Mrow = B.mats + B.moff[b] + ((long)i * d + x) * N;
+#pragma unroll
+  for (int k = 0; k < RP; ++k) {
+    if (k < r) {
+      const int ip = B.perm[k];  // z[perm[k]] = w[k]
+      Mrow[(long)ip * d + y] = (ip == i && x == y) ? add(a[k], 1.0) : a[k];
+    }
+  }
+}
+
+// (value, row) arg-max reduction within a CTA; ties keep the smaller row (idamax returns the first).
+__device__ __forceinline__ void argmax_combine(double &v, int &ix, double v2, int ix2) {
+  if (v2 > v || (v2 == v && ix2 < ix)) { v = v2; ix = ix2; }
+}
+
+// One CTA per block: LU with partial pivoting of the N x N system (row-major in global memory; elimination
+// updates a_ij - l_ik u_kj separately rounded, as the CPU restatement's getrf), then the
+// solve with the d right-hand-side columns G0 (rows (t, i), columns j: the packed slab layout), row
+// interchanges, unit-lower forward and upper backward substitution, and the (optional) hermitization
+// G(t) <- (G(t) + G(t)^T) / 2 into G_out.  rhs is the block's scratch copy of G0.
+__global__ void __launch_bounds__(1024) dyson_lu_solve_kernel(DysonBasis B, double *__restrict__ rhs, double *__restrict__ G_out,
+                                                              int hermitize, int *__restrict__ status) {
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  __shared__ int s_piv;
+  const int b = blockIdx.x;
+  if (b >= B.nb) return;
+  const int r = B.r, d = B.dims[b], dd = d * d;
+  const int N = r * d;
+  double *A = B.mats + B.moff[b];
+  double *x = rhs + B.goff[b];
+  const double *g0 = B.g0 + B.goff[b];
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  for (long e = tid; e < (long)N * d; e += nt) x[e] = g0[e];
+  bool singular = false;
+  for (int k = 0; k < N; ++k) {
+    // pivot search in column k, rows k..N-1
+    double bv = -1.0;
+    int bi = N;
+    for (int i = k + tid; i < N; i += nt) argmax_combine(bv, bi, fabs(A[(long)i * N + k]), i);
+    for (int o = 16; o > 0; o >>= 1) {
+      double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+      int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+      argmax_combine(bv, bi, v2, i2);
+    }
+    if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+    __syncthreads();
+    if (warp == 0) {
+      bv = lane < (nt >> 5) ? red_v[lane] : -1.0;
+      bi = lane < (nt >> 5) ? red_i[lane] : N;
+      for (int o = 16; o > 0; o >>= 1) {
+        double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+        int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        argmax_combine(bv, bi, v2, i2);
+      }
+      if (lane == 0) s_piv = bi;
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p >= N) { singular = true; break; }  // only when the column is NaN
+    if (p != k) {
+      for (int j = tid; j < N; j += nt) {
+        const double t = A[(long)k * N + j];
+        A[(long)k * N + j] = A[(long)p * N + j];
+        A[(long)p * N + j] = t;
+      }
+      for (int j = tid; j < d; j += nt) {
+        const double t = x[(long)k * d + j];
+        x[(long)k * d + j] = x[(long)p * d + j];
+        x[(long)p * d + j] = t;
+      }
+    }
+    __syncthreads();
+    const double piv = A[(long)k * N + k];
+    if (piv == 0.0) { singular = true; break; }
+    for (int i = k + 1 + tid; i < N; i += nt) A[(long)i * N + k] = __ddiv_rn(A[(long)i * N + k], piv);
+    __syncthreads();
+    const int m = N - k - 1;
+    for (long e = tid; e < (long)m * m; e += nt) {
+      const int i = k + 1 + (int)(e / m), j = k + 1 + (int)(e - (e / m) * m);
+      A[(long)i * N + j] = __dsub_rn(A[(long)i * N + j], mul(A[(long)i * N + k], A[(long)k * N + j]));
+    }
+    __syncthreads();
+  }
+  if (singular) {
+    if (tid == 0) atomicExch(status, 1);
+    return;
+  }
+  // forward substitution with the unit lower factor (the row interchanges were applied above)
+  for (int k = 0; k < N - 1; ++k) {
+    const int m = N - k - 1;
+    for (int e = tid; e < m * d; e += nt) {
+      const int i = k + 1 + e / d, j = e - (e / d) * d;
+      x[(long)i * d + j] = fmad(-A[(long)i * N + k], x[(long)k * d + j], x[(long)i * d + j]);
+    }
+    __syncthreads();
+  }
+  // backward substitution with the upper factor
+  for (int k = N - 1; k >= 0; --k) {
+    for (int j = tid; j < d; j += nt) x[(long)k * d + j] = __ddiv_rn(x[(long)k * d + j], A[(long)k * N + k]);
+    __syncthreads();
+    for (int e = tid; e < k * d; e += nt) {
+      const int i = e / d, j = e - i * d;
+      x[(long)i * d + j] = fmad(-A[(long)i * N + k], x[(long)k * d + j], x[(long)i * d + j]);
+    }
+    __syncthreads();
+  }
+  double *g = G_out + B.goff[b];
+  for (long e = tid; e < (long)r * dd; e += nt) {
+    const int t = (int)(e / dd), ij = (int)(e - (long)t * dd), i = ij / d, j = ij - i * d;
+    const double v = x[e];
+    g[e] = hermitize ? mul(0.5, add(v, x[(long)t * dd + j * d + i])) : v;
+  }
+}
+
+// Per block: sum_x G_b(beta)[x][x] = sum_x sum_l K(1, om_l) (K^-1 G_b)_l[x][x], one lane per diagonal entry.
+template <int RP>
+__global__ void __launch_bounds__(128) trace_beta_kernel(DysonBasis B, const double *__restrict__ G, double *__restrict__ out) {
+  extern __shared__ double smem[];
+  double *sLU = smem;
+  int *sPerm = reinterpret_cast<int *>(sLU + RP * RP);
+  __shared__ double part[128];
+  const int b = blockIdx.x;
+  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) sLU[i] = B.LUp[i];
+  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
+  __syncthreads();
+  const int r = B.r, d = B.dims[b], dd = d * d;
+  const double *g = G + B.goff[b];
+  double s = 0.0;
+  for (int xx = threadIdx.x; xx < d; xx += blockDim.x) {
+    double x[RP];
+#pragma unroll
+    for (int i = 0; i < RP; ++i) {
+      const int src = sPerm[i];
+      x[i] = src >= 0 ? g[(long)src * dd + xx * d + xx] : 0.0;
+    }
+    lu_solve_reg<RP>(sLU, x);
+    double v = 0.0;
+#pragma unroll
+    for (int l = 0; l < RP; ++l)
+      if (l < r) v = add(v, mul(B.k1[l], x[l]));
+    s = add(s, v);
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < (int)blockDim.x; ++i) t = add(t, part[i]);
+    out[b] = t;
+  }
+}
+
+// G(tau_i) <- G(tau_i) exp(-tau_i deta), tau_i = beta t_i (energy_shift_ppgf, block_sparse_solver.py:436-441).
+__global__ void energy_shift_kernel(DysonBasis B, double *__restrict__ G, double deta) {
+  const int b = blockIdx.y;
+  const int dd = B.dims[b] * B.dims[b];
+  const long n = (long)B.r * dd;
+  double *g = G + B.goff[b];
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+    const int t = (int)(e / dd);
+    g[e] = mul(g[e], exp(-mul(mul(B.beta, B.tabs[t]), deta)));
+  }
+}
+
+// Partial maxima of |a - b| over a packed slab (one per CTA; the host takes the max of the partials).
+__global__ void __launch_bounds__(256) max_abs_diff_kernel(const double *__restrict__ a, const double *__restrict__ b, long n,
+                                                           double *__restrict__ out) {
+  __shared__ double red[256];
+  double m = 0.0;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(a[e] - b[e]));
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
+// y <- alpha x + beta y (two rounded products, one rounded sum: mix * G_new + (1 - mix) * G).
+__global__ void axpby_kernel(double alpha, const double *__restrict__ x, double beta, double *__restrict__ y, long n) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+    y[e] = add(mul(alpha, x[e]), mul(beta, y[e]));
+}
+
+}  // namespace xca

@@ -22,6 +22,7 @@
 #include "../../include/xca_b200.h"
 #include "dlr_host.hpp"
 #include "sigma_kernel.cuh"
+#include "dyson_kernel.cuh"
 
 namespace xca {
 
@@ -553,6 +554,14 @@ struct Ctx {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
   cudaEvent_t user_events[8] = {nullptr};
   DevBuf<double> d_flush;
+  // Dyson solve state (basis-only contexts and evaluators alike)
+  bool basis_ready = false, dyson_ready = false;
+  std::vector<double> k1;                 // K(1, om_l)
+  std::vector<long> woff, moff;           // per-block work and system-matrix offsets
+  long n_conv_rows = 0;                   // largest r d_b^2 (rows of the convolution-matrix kernel grid)
+  DevBuf<double> d_k1, d_rf, d_g0, d_g0c, d_g0t, d_dwork, d_mats, d_rhs, d_red;
+  DevBuf<long> d_woff, d_moff;
+  DevBuf<int> d_status;
 
   DevBasis basis(int nsig) const {
     DevBasis B;
@@ -581,6 +590,67 @@ static Topology parse_topology(int m, const int *topo) {
   }
   if (T.t[0][0] != 0) throw Error(XCA_ERR_INVALID, "topology(0,0) must be 0");
   return T;
+}
+
+// DLR basis of a context: block structure, K(t_i, om_l) and its LU factors, the Hilbert weights W, and
+// the padded column-major copies the register-column kernels stage (imtime_ops, cppdlr; call sites
+// block_sparse_backbone.cpp:68-70, dlr_dyson_ppsc.hpp:57-76).  Uploads them to the device.
+static void setup_basis(Ctx *c, double beta, double lambda, double eps, int r, const double *rf, const double *it, int n_blocks,
+                        const int *block_dims) {
+  if (r <= 0 || n_blocks <= 0) throw Error(XCA_ERR_INVALID, "empty DLR basis or block structure");
+  if (r > 64) throw Error(XCA_ERR_UNSUPPORTED, "DLR rank " + std::to_string(r) + " above 64 is not supported by the device kernels");
+  c->basis_ready = false;
+  c->dyson_ready = false;
+  c->r = r; c->nb = n_blocks; c->beta = beta; c->lam = lambda; c->eps = eps;
+  c->rf.assign(rf, rf + r);
+  c->it.assign(it, it + r);
+  c->dims.assign(block_dims, block_dims + n_blocks);
+  c->nmax = 1;
+  for (int b = 0; b < n_blocks; ++b) {
+    if (block_dims[b] <= 0) throw Error(XCA_ERR_INVALID, "block dimension must be positive");
+    c->nmax = std::max(c->nmax, block_dims[b]);
+  }
+  c->goff.resize(n_blocks);
+  long off = 0;
+  for (int b = 0; b < n_blocks; ++b) { c->goff[b] = off; off += (long)r * block_dims[b] * block_dims[b]; }
+  c->slab = off;
+  c->tabs.resize(r); c->k0.resize(r); c->k1.resize(r);
+  for (int i = 0; i < r; ++i) c->tabs[i] = it[i] < 0 ? 1.0 + it[i] : it[i];
+  for (int l = 0; l < r; ++l) { c->k0[l] = k_abs(0.0, rf[l]); c->k1[l] = k_abs(1.0, rf[l]); }
+  c->Kit.resize((size_t)r * r); c->W.assign((size_t)r * r, 0.0);
+  for (int i = 0; i < r; ++i)
+    for (int l = 0; l < r; ++l) c->Kit[(size_t)i * r + l] = k_it(it[i], rf[l]);
+  for (int l = 0; l < r; ++l)
+    for (int k = 0; k < r; ++k)
+      if (k != l) c->W[(size_t)l * r + k] = c->k0[k] / (rf[k] - rf[l]);
+  c->LU = c->Kit;
+  lu_factor(c->LU, r, c->piv);
+  c->RP = r <= 32 ? 32 : (r <= 48 ? 48 : 64);
+  const int RP = c->RP;
+  c->LUp.assign((size_t)RP * RP, 0.0); c->Wp.assign((size_t)RP * RP, 0.0); c->BKp.assign((size_t)RP * RP, 0.0);
+  for (int i = 0; i < RP; ++i)
+    for (int k = 0; k < RP; ++k) {
+      // column-major: element (row i, column k) at k * RP + i
+      if (i < r && k < r) {
+        c->LUp[(size_t)k * RP + i] = c->LU[(size_t)i * r + k];
+        c->Wp[(size_t)k * RP + i] = c->W[(size_t)i * r + k];
+        c->BKp[(size_t)k * RP + i] = beta * c->Kit[(size_t)i * r + k];
+      } else if (i == k) {
+        c->LUp[(size_t)k * RP + i] = 1.0;
+      }
+    }
+  c->perm.assign(RP, -1);
+  {
+    std::vector<int> idx(r);
+    for (int i = 0; i < r; ++i) idx[i] = i;
+    for (int k = 0; k < r; ++k) std::swap(idx[k], idx[c->piv[k]]);
+    for (int i = 0; i < r; ++i) c->perm[i] = idx[i];
+  }
+  cudaStream_t s = c->stream;
+  c->d_LUp.upload(c->LUp, s); c->d_Wp.upload(c->Wp, s); c->d_BKp.upload(c->BKp, s); c->d_perm.upload(c->perm, s);
+  c->d_tabs.upload(c->tabs, s); c->d_k0.upload(c->k0, s); c->d_k1.upload(c->k1, s); c->d_rf.upload(c->rf, s);
+  c->d_dims.upload(c->dims, s); c->d_goff.upload(c->goff, s);
+  c->basis_ready = true;
 }
 
 static long ipow(long a, int e) {
@@ -848,6 +918,91 @@ static void real_part(const double *cplx, long n, std::vector<double> &out, cons
 }
 
 
+// -------------------------------------------------------------------------------- Dyson, trace, normalisation
+static DysonBasis dyson_basis(Ctx *c) {
+  DysonBasis B;
+  B.r = c->r; B.nb = c->nb; B.beta = c->beta;
+  B.LUp = c->d_LUp.ptr; B.Wp = c->d_Wp.ptr; B.BKp = c->d_BKp.ptr; B.perm = c->d_perm.ptr;
+  B.tabs = c->d_tabs.ptr; B.k0 = c->d_k0.ptr; B.k1 = c->d_k1.ptr; B.rf = c->d_rf.ptr;
+  B.goff = c->d_goff.ptr; B.dims = c->d_dims.ptr; B.woff = c->d_woff.ptr; B.moff = c->d_moff.ptr;
+  B.g0 = c->d_g0.ptr; B.g0c = c->d_g0c.ptr; B.g0t = c->d_g0t.ptr;
+  B.work = c->d_dwork.ptr; B.mats = c->d_mats.ptr;
+  return B;
+}
+
+static void require_basis(const Ctx *c) {
+  if (!c->basis_ready) throw Error(XCA_ERR_INVALID, "no DLR basis set up on this context");
+}
+
+static void require_dyson(const Ctx *c) {
+  require_basis(c);
+  if (!c->dyson_ready) throw Error(XCA_ERR_INVALID, "Dyson solver not set up (xca_dyson_setup)");
+}
+
+template <int RP>
+static void launch_dyson_rp(Ctx *c, const double *Sig_dev, double eta, int hermitize, double *G_dev) {
+  DysonBasis B = dyson_basis(c);
+  size_t sm = (2 * (size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
+  CUDA_CHECK(cudaFuncSetAttribute(dyson_coef_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  dyson_coef_kernel<RP><<<c->nb, 256, sm, c->stream>>>(B, Sig_dev, eta);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+  dim3 grid((unsigned)((c->n_conv_rows + 63) / 64), (unsigned)c->nb);
+  dyson_convmat_kernel<RP><<<grid, 64, 0, c->stream>>>(B);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+  dyson_lu_solve_kernel<<<c->nb, 1024, 0, c->stream>>>(B, c->d_rhs.ptr, G_dev, hermitize, c->d_status.ptr);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+}
+
+static void launch_dyson(Ctx *c, const double *Sig_dev, double eta, int hermitize, double *G_dev) {
+  CUDA_CHECK(cudaMemsetAsync(c->d_status.ptr, 0, sizeof(int), c->stream));
+  switch (c->RP) {
+    case 32: launch_dyson_rp<32>(c, Sig_dev, eta, hermitize, G_dev); break;
+    case 48: launch_dyson_rp<48>(c, Sig_dev, eta, hermitize, G_dev); break;
+    default: launch_dyson_rp<64>(c, Sig_dev, eta, hermitize, G_dev); break;
+  }
+}
+
+// Raise if a Dyson solve since the last check met a singular system matrix (call after a synchronize).
+static void check_dyson_status(Ctx *c) {
+  if (!c->d_status.ptr) return;
+  int st = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&st, c->d_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  if (st) {
+    CUDA_CHECK(cudaMemsetAsync(c->d_status.ptr, 0, sizeof(int), c->stream));
+    throw Error(XCA_ERR_RUNTIME, "Dyson solve: singular system matrix (getrf info > 0)");
+  }
+}
+
+template <int RP>
+static double trace_beta_rp(Ctx *c, const double *G_dev) {
+  DysonBasis B = dyson_basis(c);
+  size_t sm = ((size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
+  CUDA_CHECK(cudaFuncSetAttribute(trace_beta_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  c->d_red.resize(std::max(c->nb, 256));
+  trace_beta_kernel<RP><<<c->nb, 128, sm, c->stream>>>(B, G_dev, c->d_red.ptr);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+  std::vector<double> part(c->nb);
+  CUDA_CHECK(cudaMemcpyAsync(part.data(), c->d_red.ptr, c->nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  double s = 0;
+  for (double x : part) s += x;
+  return s;
+}
+
+// sum_b Tr G_b(beta) (trace, block_sparse.cpp:852-861)
+static double trace_beta(Ctx *c, const double *G_dev) {
+  switch (c->RP) {
+    case 32: return trace_beta_rp<32>(c, G_dev);
+    case 48: return trace_beta_rp<48>(c, G_dev);
+    default: return trace_beta_rp<64>(c, G_dev);
+  }
+}
+
 // -------------------------------------------------------------------------------- allocation-free Sigma
 // xca_compute_self_energy_device_noalloc keeps everything it needs beyond its inputs, its output and the
 // evaluator's set-up tables in this fixed array of the library's device image, so the call itself never
@@ -985,10 +1140,9 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
   auto *c = reinterpret_cast<Ctx *>(ctx);
   set_device(c);
   if (r <= 0 || p <= 0 || n <= 0 || n_blocks <= 0) throw Error(XCA_ERR_INVALID, "empty basis, hybridization or block structure");
-  c->r = r; c->p = p; c->n = n; c->nb = n_blocks; c->beta = beta; c->lam = lambda; c->eps = eps;
-  c->rf.assign(rf, rf + r);
-  c->it.assign(it, it + r);
-  c->dims.assign(block_dims, block_dims + n_blocks);
+  c->ready = false;
+  setup_basis(c, beta, lambda, eps, r, rf, it, n_blocks, block_dims);
+  c->p = p; c->n = n;
   c->labels.assign(labels, labels + n);
   long nq = 0;
   for (int i = 0; i < n; ++i) {
@@ -1004,15 +1158,6 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
   }
   for (long s = 0; s < nq; ++s)
     if (c->ssizes[s] == 0) throw Error(XCA_ERR_INVALID, "BlockOpSymQuartet: symmetry set " + std::to_string(s) + " has no orbital");
-  c->nmax = 1;
-  for (int b = 0; b < n_blocks; ++b) {
-    if (block_dims[b] <= 0) throw Error(XCA_ERR_INVALID, "block dimension must be positive");
-    c->nmax = std::max(c->nmax, block_dims[b]);
-  }
-  c->goff.resize(n_blocks);
-  long off = 0;
-  for (int b = 0; b < n_blocks; ++b) { c->goff[b] = off; off += (long)r * block_dims[b] * block_dims[b]; }
-  c->slab = off;
   // hybridization coefficients: real part, block-diagonality in the symmetry sets (block_sparse.cpp:443-492)
   std::vector<double> coef;
   real_part(hyb_coeffs, (long)p * n * n, coef, "hyb_coeffs");
@@ -1083,18 +1228,6 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
           }
         }
   }
-  // DLR basis matrices
-  c->tabs.resize(r); c->k0.resize(r);
-  for (int i = 0; i < r; ++i) c->tabs[i] = it[i] < 0 ? 1.0 + it[i] : it[i];
-  for (int l = 0; l < r; ++l) c->k0[l] = k_abs(0.0, rf[l]);
-  c->Kit.resize((size_t)r * r); c->W.assign((size_t)r * r, 0.0);
-  for (int i = 0; i < r; ++i)
-    for (int l = 0; l < r; ++l) c->Kit[(size_t)i * r + l] = k_it(it[i], rf[l]);
-  for (int l = 0; l < r; ++l)
-    for (int k = 0; k < r; ++k)
-      if (k != l) c->W[(size_t)l * r + k] = c->k0[k] / (rf[k] - rf[l]);
-  c->LU = c->Kit;
-  lu_factor(c->LU, r, c->piv);
   // hybridization tables (Hybridization ctor, hyb.cpp:15-44)
   c->polesb.resize(p); c->kitp.resize((size_t)r * p); c->kitm.resize((size_t)r * p); c->k0p.resize(p); c->k0m.resize(p);
   for (int l = 0; l < p; ++l) {
@@ -1125,31 +1258,8 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
     for (int i = 0; i < r; ++i)
       for (int l = 0; l < r; ++l) {
         double k = k_it(it[i], -rf[l]);
-        for (long j = 0; j < nc; ++j) c->hrefl[(size_t)i * nc + j] += k * cfs[(size_t)l * nc + j];
+        for (long j = 0; j < nc; ++j) c->hrefl[(size_t)i * nc + j] = std::fma(k, cfs[(size_t)l * nc + j], c->hrefl[(size_t)i * nc + j]);
       }
-  }
-  // padded matrices of the register-resident column kernels
-  if (r > 64) throw Error(XCA_ERR_UNSUPPORTED, "DLR rank " + std::to_string(r) + " above 64 is not supported by the device kernels");
-  c->RP = r <= 32 ? 32 : (r <= 48 ? 48 : 64);
-  const int RP = c->RP;
-  c->LUp.assign((size_t)RP * RP, 0.0); c->Wp.assign((size_t)RP * RP, 0.0); c->BKp.assign((size_t)RP * RP, 0.0);
-  for (int i = 0; i < RP; ++i)
-    for (int k = 0; k < RP; ++k) {
-      // column-major: element (row i, column k) at k * RP + i
-      if (i < r && k < r) {
-        c->LUp[(size_t)k * RP + i] = c->LU[(size_t)i * r + k];
-        c->Wp[(size_t)k * RP + i] = c->W[(size_t)i * r + k];
-        c->BKp[(size_t)k * RP + i] = beta * c->Kit[(size_t)i * r + k];
-      } else if (i == k) {
-        c->LUp[(size_t)k * RP + i] = 1.0;
-      }
-    }
-  c->perm.assign(RP, -1);
-  {
-    std::vector<int> idx(r);
-    for (int i = 0; i < r; ++i) idx[i] = i;
-    for (int k = 0; k < r; ++k) std::swap(idx[k], idx[c->piv[k]]);
-    for (int i = 0; i < r; ++i) c->perm[i] = idx[i];
   }
   // edge tables: per block, 1 + 2p + 4p^2 signatures of [fc | W fc] (r d^2 each)
   c->nsig_alloc = 1 + 2L * p + 4L * p * p;
@@ -1168,12 +1278,11 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
   }
   // upload
   cudaStream_t s = c->stream;
-  c->d_LUp.upload(c->LUp, s); c->d_Wp.upload(c->Wp, s); c->d_BKp.upload(c->BKp, s); c->d_perm.upload(c->perm, s);
   c->d_tab_off.upload(c->tab_off, s);
-  c->d_tabs.upload(c->tabs, s); c->d_k0.upload(c->k0, s); c->d_kitp.upload(c->kitp, s); c->d_kitm.upload(c->kitm, s);
+  c->d_kitp.upload(c->kitp, s); c->d_kitm.upload(c->kitm, s);
   c->d_kpow.upload(c->kpow, s); c->d_polesb.upload(c->polesb, s);
   c->d_hval.upload(c->hval, s); c->d_hrefl.upload(c->hrefl, s); c->d_ops.upload(c->ops, s);
-  c->d_dims.upload(c->dims, s); c->d_set_to_orb.upload(c->set_to_orb, s); c->d_goff.upload(c->goff, s);
+  c->d_set_to_orb.upload(c->set_to_orb, s);
   c->d_F_off.upload(c->F_off, s); c->d_Fd_off.upload(c->Fd_off, s); c->d_Fb_off.upload(c->Fb_off, s); c->d_Fdb_off.upload(c->Fdb_off, s);
   c->class_cache.clear();
   c->noalloc_classes.clear();
@@ -1239,6 +1348,162 @@ int xca_compute_self_energy_device_shard(xca_ctx *ctx, const double *G_dev, int 
     }
     launch_sigma(c, it->second.get(), G_dev, Sigma_dev, scale, nsig);
   }
+  API_END
+}
+
+int xca_basis_setup(xca_ctx *ctx, double beta, double lambda, double eps, int r, const double *rf, const double *it,
+                    int n_blocks, const int *block_dims) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  set_device(c);
+  c->ready = false;
+  setup_basis(c, beta, lambda, eps, r, rf, it, n_blocks, block_dims);
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  API_END
+}
+
+int xca_dyson_setup(xca_ctx *ctx, const double *G0) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_basis(c);
+  set_device(c);
+  c->dyson_ready = false;
+  std::vector<double> g0;
+  real_part(G0, c->slab, g0, "G0");
+  // DLR coefficients of G0 (vals2coefs, dlr_dyson_ppsc.hpp:106) and their Hilbert transform W g0c
+  std::vector<double> g0c = g0, g0t(c->slab, 0.0);
+  const int r = c->r;
+  c->woff.assign(c->nb, 0);
+  c->moff.assign(c->nb, 0);
+  long wo = 0, mo = 0;
+  c->n_conv_rows = 0;
+  for (int b = 0; b < c->nb; ++b) {
+    const long dd = (long)c->dims[b] * c->dims[b];
+    double *gc = g0c.data() + c->goff[b];
+    lu_solve(c->LU, r, c->piv, gc, dd);
+    double *gt = g0t.data() + c->goff[b];
+    for (int l = 0; l < r; ++l)
+      for (int k = 0; k < r; ++k) {
+        const double w = c->W[(size_t)l * r + k];
+        for (long x = 0; x < dd; ++x) gt[l * dd + x] = std::fma(w, gc[k * dd + x], gt[l * dd + x]);
+      }
+    c->woff[b] = wo;
+    wo += 6L * r * dd;
+    c->moff[b] = mo;
+    mo += (long)r * c->dims[b] * (long)r * c->dims[b];
+    c->n_conv_rows = std::max(c->n_conv_rows, (long)r * dd);
+  }
+  cudaStream_t s = c->stream;
+  c->d_g0.upload(g0, s); c->d_g0c.upload(g0c, s); c->d_g0t.upload(g0t, s);
+  c->d_woff.upload(c->woff, s); c->d_moff.upload(c->moff, s);
+  c->d_dwork.resize(std::max(wo, 1L));
+  c->d_mats.resize(std::max(mo, 1L));
+  c->d_rhs.resize(std::max(c->slab, 1L));
+  c->d_red.resize(std::max(c->nb, 256));
+  c->d_status.resize(1);
+  CUDA_CHECK(cudaMemsetAsync(c->d_status.ptr, 0, sizeof(int), s));
+  CUDA_CHECK(cudaStreamSynchronize(s));
+  c->dyson_ready = true;
+  API_END
+}
+
+int xca_dyson_solve(xca_ctx *ctx, const double *Sigma, double eta, int hermitize, double *G_out) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_dyson(c);
+  set_device(c);
+  std::vector<double> sg;
+  real_part(Sigma, c->slab, sg, "Sigma");
+  c->d_Sig.resize(c->slab);
+  c->d_G.resize(c->slab);
+  CUDA_CHECK(cudaMemcpyAsync(c->d_Sig.ptr, sg.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  launch_dyson(c, c->d_Sig.ptr, eta, hermitize, c->d_G.ptr);
+  std::vector<double> g(c->slab);
+  CUDA_CHECK(cudaMemcpyAsync(g.data(), c->d_G.ptr, c->slab * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  check_dyson_status(c);
+  for (long i = 0; i < c->slab; ++i) { G_out[2 * i] = g[i]; G_out[2 * i + 1] = 0.0; }
+  API_END
+}
+
+int xca_dyson_solve_device(xca_ctx *ctx, const double *Sigma_dev, double eta, int hermitize, double *G_dev) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_dyson(c);
+  set_device(c);
+  launch_dyson(c, Sigma_dev, eta, hermitize, G_dev);
+  API_END
+}
+
+int xca_trace(xca_ctx *ctx, const double *G, double *tr_out) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_basis(c);
+  set_device(c);
+  std::vector<double> g;
+  real_part(G, c->slab, g, "G");
+  c->d_G.resize(c->slab);
+  CUDA_CHECK(cudaMemcpyAsync(c->d_G.ptr, g.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  tr_out[0] = trace_beta(c, c->d_G.ptr);
+  tr_out[1] = 0.0;
+  API_END
+}
+
+int xca_trace_device(xca_ctx *ctx, const double *G_dev, double *tr_out) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_basis(c);
+  set_device(c);
+  tr_out[0] = trace_beta(c, G_dev);
+  tr_out[1] = 0.0;
+  API_END
+}
+
+int xca_normalize_device(xca_ctx *ctx, double *G_dev, double *Z, double *deta) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_basis(c);
+  set_device(c);
+  check_dyson_status(c);
+  const double z = -trace_beta(c, G_dev);
+  const double de = std::log(std::fabs(z)) / c->beta;
+  dim3 grid(64, (unsigned)c->nb);
+  energy_shift_kernel<<<grid, 256, 0, c->stream>>>(dyson_basis(c), G_dev, de);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+  *Z = z;
+  *deta = de;
+  API_END
+}
+
+int xca_max_abs_diff_device(xca_ctx *ctx, const double *a_dev, const double *b_dev, double *out) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_basis(c);
+  set_device(c);
+  const int blocks = 256;
+  c->d_red.resize(std::max(c->nb, blocks));
+  max_abs_diff_kernel<<<blocks, 256, 0, c->stream>>>(a_dev, b_dev, c->slab, c->d_red.ptr);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+  std::vector<double> part(blocks);
+  CUDA_CHECK(cudaMemcpyAsync(part.data(), c->d_red.ptr, blocks * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  double m = 0.0;
+  for (double x : part) m = std::max(m, x);
+  *out = m;
+  API_END
+}
+
+int xca_axpby_device(xca_ctx *ctx, double alpha, const double *x_dev, double beta, double *y_dev) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_basis(c);
+  set_device(c);
+  const long n = c->slab;
+  axpby_kernel<<<(int)std::max<long>(1, std::min<long>(1184, (n + 255) / 256)), 256, 0, c->stream>>>(alpha, x_dev, beta, y_dev, n);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
   API_END
 }
 
