@@ -37,6 +37,7 @@ def parse():
     ap.add_argument("--impl", default="xca", choices=["xca", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-API measurement (profiling runs)")
     return ap.parse_args()
 
 
@@ -102,6 +103,20 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def profiled_traffic():
+    """DRAM bytes (read + write) per Sigma-kernel launch of this workload from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "sigma_items_kernel_kanamori_2orb_tca.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if "traffic_bytes_per_launch:" in line:
+            try:
+                return int(line.split("traffic_bytes_per_launch:")[1].split("*")[0].strip())
+            except ValueError:
+                return None
+    return None
 
 
 def cpu_sigma_rate(m, G, seconds, nthreads=0):
@@ -227,7 +242,7 @@ def main():
 
     # end to end through the public host API: host G in, host Sigma out, every step (rank 0 only)
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.no_e2e:
         def host_eval():
             acc = [np.zeros_like(g) for g in G]
             for _, t, fac in topos:
@@ -247,13 +262,7 @@ def main():
     peak = ev.fp64_fma_peak()
     kernel_s = sigma_ms * 1e-3 / max(args.steps, 1)
     achieved = alg_flops / world / kernel_s / 1e12 if kernel_s > 0 else None
-    traffic = None
-    prof_path = os.path.join(ROOT, "profiles", "sigma_items_kernel_kanamori_2orb.json")
-    if os.path.exists(prof_path):
-        try:
-            traffic = json.load(open(prof_path)).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_sigma_rate(m, G, args.cpu_seconds)
