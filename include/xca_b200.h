@@ -147,6 +147,17 @@ int xca_compute_self_energy_device_shard(xca_ctx *ctx, const double *G_dev, int 
 int xca_compute_self_energy_device_noalloc(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
                                            double *Sigma_dev);
 
+/* DiagramEvaluator::compute_single_ptcle_gf(G, topology[, f_ix_vec])
+ * (c++/triqs_xca/block_sparse_backbone.cpp:779-821, eval_correlator :528-706): the single-particle
+ * correlator g(tau)[mu][ka] of one topology over every flat index (f_ix == NULL) or the n_fix listed
+ * ones (out of range: XCA_ERR_RUNTIME).  G is a host packed complex slab; g_out is r x n x n complex. */
+int xca_compute_single_ptcle_gf(xca_ctx *ctx, const double *G, int m, const int *topology, const long *f_ix, long n_fix,
+                                double *g_out);
+
+/* Same on device-resident real data, accumulating g_dev (r x n x n real) += scale * g. */
+int xca_compute_single_ptcle_gf_device(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
+                                       double *g_dev);
+
 /* Zero n_doubles of device memory on the context's stream. */
 int xca_zero_device(xca_ctx *ctx, double *dev, long n_doubles);
 

@@ -131,11 +131,11 @@ def test_anderson_self_consistent_solve_vs_oracle(max_order):
     delta[:, 0, 0] = dv
     delta[:, 1, 1] = dv
     S.Delta_tau = delta
-    S.solve(max_order=max_order, tol=1e-10, maxiter=60, mix=1.0, spgf_max_order=0)
+    S.solve(max_order=max_order, tol=1e-10, maxiter=60, mix=1.0)
 
     d = O.Dlr(lam, eps, rf=S.rf, it=S.it)
     ev = O.Evaluator(d, beta, S.hyb_poles, S.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
-    G, Sig, eta, _, n_iter, diff = O.solve(d, ev, beta, m.G0, max_order, 1e-10, 60, mix=1.0, spgf_max_order=1)
+    G, Sig, eta, g, n_iter, diff = O.solve(d, ev, beta, m.G0, max_order, 1e-10, 60, mix=1.0, spgf_max_order=max_order)
     assert diff < 1e-10 and S.diff_G < 1e-10
     assert abs(S.n_ppsc_iter - n_iter) <= 1
     assert abs(S.eta - eta) < 1e-10
@@ -143,3 +143,6 @@ def test_anderson_self_consistent_solve_vs_oracle(max_order):
         assert np.max(np.abs(a - b)) < 1e-10
     for a, b in zip(S.Sigma, Sig):
         assert np.max(np.abs(a - b)) < 1e-10 * max(1.0, np.max(np.abs(b)))
+    # single-particle G(tau) of the converged propagator, orders 1..max_order
+    assert np.max(np.abs(S.G_tau - g)) < 1e-10
+    assert np.max(np.abs(g)) > 0.1

@@ -51,6 +51,8 @@ SIGNATURES = {
     "xca_compute_self_energy_device": [P, P, I, ip, D, P],
     "xca_compute_self_energy_device_shard": [P, P, I, ip, D, P, I, I],
     "xca_compute_self_energy_device_noalloc": [P, P, I, ip, D, P],
+    "xca_compute_single_ptcle_gf": [P, dp, I, ip, lp, L, dp],
+    "xca_compute_single_ptcle_gf_device": [P, P, I, ip, D, P],
     "xca_zero_device": [P, P, L],
     "xca_self_energy_items": [P, dp, I, ip, lp, L, lp],
     "xca_self_energy_flops": [P, dp, I, ip, dp, lp],

@@ -178,6 +178,25 @@ class DiagramEvaluator:
                                                       _lib.as_dp(out.view(np.float64))))
         return self.unpack(out)
 
+    def compute_single_ptcle_gf(self, G_ppsc, topology, f_ix=None):
+        """Single-particle correlator g(tau)[mu][ka] of one topology, (r, n, n) complex (bsb.cpp:779-821)."""
+        t, m = self._topo(topology)
+        g = self.pack(G_ppsc)
+        out = np.zeros((self.r, self.n, self.n), np.complex128)
+        if f_ix is None:
+            fp, nf = None, 0
+        else:
+            fix = np.ascontiguousarray(np.atleast_1d(f_ix), dtype=np.int64)
+            fp, nf = _lib.as_lp(fix), len(fix)
+        _lib.check(_lib.lib().xca_compute_single_ptcle_gf(self._ctx, _lib.as_dp(g.view(np.float64)), m, _lib.as_ip(t), fp, nf,
+                                                          _lib.as_dp(out.view(np.float64))))
+        return out
+
+    def compute_single_ptcle_gf_device(self, G_dev, topology, scale, g_dev):
+        t, m = self._topo(topology)
+        _lib.check(_lib.lib().xca_compute_single_ptcle_gf_device(self._ctx, ctypes.c_void_p(G_dev), m, _lib.as_ip(t), float(scale),
+                                                                 ctypes.c_void_p(g_dev)))
+
     def self_energy_items(self, G_ppsc, topology, max_rows=None):
         """Valid (f_ix, b_ix, p_kap, ind_path...) items of find_path_self_energy in flat-index order."""
         t, m = self._topo(topology)

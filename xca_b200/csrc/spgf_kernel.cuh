@@ -1,0 +1,356 @@
+// Single-particle Green's function backbones on the device (plain FP64 path).
+//
+// DiagramEvaluator::compute_single_ptcle_gf (c++/triqs_xca/block_sparse_backbone.cpp:779-821) sums, over
+// the flat indices of a CorrelatorBackbone (c++/triqs_xca/backbone.cpp:239-292), eval_correlator
+// (block_sparse_backbone.cpp:528-706):
+//   right chains  (vertices 1 .. vct0-1 on [0, tau]): T = G_b, then vertex, edge, ... (multiply_left_vertex,
+//                 integrate_left_edge), scaled by the prefactor and its sign;
+//   left chains   (vertices 2m-1 .. vct0+1 on [tau, beta]): U = G, then vertex, edge, ... from the right
+//                 (multiply_right_vertex, integrate_right_edge, :463-515), then U <- reflect(U) (:648);
+//   contraction   g(t)[mu][ka] += Tr[L(t) F_mu R(t) F^dag_ka] over the blocks that close the trace.
+// Everything that does not depend on the pole tuple (directions, orbitals, block paths, which chains
+// close a trace) is a correlator class built on the host; a warp evaluates the pole tuples of a class
+// one at a time, its lanes striding over matrix entries and register-resident columns, with per-warp
+// scratch in global memory.  Every product and sum is rounded as in the CPU restatement.
+#pragma once
+#include "sigma_kernel.cuh"
+
+namespace xca {
+
+struct CorrChain {
+  int gblock;               // block of G the chain starts from
+  int start;                // right: ind_path[0]; left: ind_path[vct0]
+  int path[MAXV];           // ind_path entries of the chain's segment (-1 elsewhere)
+  int bd[MAXV + 1];         // block_dims entries of the chain's segment
+  int rows, cols;           // result per tau: right R x d1, left nrow x C
+};
+
+struct CorrTerm {
+  int mu, ka;               // orbitals of F_mu (at vct0) and F^dag_ka (at 0)
+  int rchain, lchain;       // chain indices within the class (right, left)
+  int e0, e2;               // column blocks of F_mu and F^dag_ka
+  int c0, c1, c2, c3;       // dims: right cols, right rows, F_mu rows, left rows
+};
+
+struct CorrClass {
+  int m, vct0, fbmask;      // fbmask bit i (i >= 1): line i forward
+  int la[MAXM], lb[MAXM];
+  int vkind[MAXV], vset[MAXV], vqo[MAXV], vline[MAXV];
+  int chain0, n_right, n_left;  // chains [chain0, chain0 + n_right) right, then n_left left
+  int term0, n_terms;
+};
+
+struct CorrBasis {
+  const double *RFp;        // RP x RP column-major: K(t_i, -om_l) (reflect), 0 in the pad
+  const long *mu_off;       // [o * nb + b]: offset of F_o's (d_target x d_b) slab in ops (-1: none)
+  const long *ka_off;       // [o * nb + b]: offset of F^dag_o's slab in ops (-1: none)
+};
+
+// Per-item pole data, decoded as Backbone::set_pole_inds (c++/triqs_xca/backbone.cpp:86-150).
+struct CorrItem {
+  int lpole[MAXM];
+  int caseA[MAXM];
+  double scale;             // prefactor * prefactor sign
+};
+
+__device__ __forceinline__ CorrItem corr_decode(const DevBasis &B, const CorrClass &C, int q) {
+  CorrItem S;
+  const int m = C.m, p = B.p;
+  for (int i = 0; i < MAXM; ++i) { S.lpole[i] = 0; S.caseA[i] = 0; }
+  for (int i = 1; i < m; ++i) {
+    S.lpole[i] = q % p;
+    q /= p;
+  }
+  double pf = 1.0;
+  int psign = 1;
+  for (int i = 1; i < m; ++i) {
+    const int fwd = (C.fbmask >> i) & 1;
+    const double w = B.polesb[S.lpole[i]];
+    S.caseA[i] = fwd ? (w <= 0.0) : (w >= 0.0);
+    if (!fwd) psign = -psign;
+    const int row = S.caseA[i] ? (fwd ? 1 : 0) : (fwd ? 0 : 1);
+    const int ex = S.caseA[i] ? 1 : C.lb[i] - C.la[i] - 1;
+    if (ex != 0) pf = mul(pf, B.kpow[((size_t)row * p + S.lpole[i]) * (MAXE + 1) + ex]);
+  }
+  S.scale = mul(pf, (double)psign);
+  return S;
+}
+
+// Operator slab of vertex v acting on block b, and the K-factor table of the vertex (nullptr: none).
+// right = true selects the sign convention of multiply_right_vertex (block_sparse_backbone.cpp:488-495).
+__device__ __forceinline__ const double *corr_vertex_op(const DevBasis &B, const CorrClass &C, const CorrItem &S, int v, int b,
+                                                        int dvp, int dv, bool right, const double **ktab, int *kcol) {
+  const int line = C.vline[v], s = C.vset[v], qo = C.vqo[v], p = B.p;
+  const int l = S.lpole[line];
+  long off;
+  switch (C.vkind[v]) {
+    case 0: off = B.F_off[s * B.nb + b] + (long)qo * dvp * dv; break;
+    case 1: off = B.Fd_off[s * B.nb + b] + (long)qo * dvp * dv; break;
+    case 2: off = B.Fb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
+    default: off = B.Fdb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
+  }
+  *ktab = nullptr;
+  *kcol = 0;
+  if (line > 0 && S.caseA[line]) {
+    const int fwd = (C.fbmask >> line) & 1;
+    const int ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
+    const bool neg = right ? (ks > 0) : (ks < 0);
+    *ktab = neg ? B.kitm : B.kitp;
+    *kcol = l;
+  }
+  return B.ops + off;
+}
+
+// Edge-table offset of edge e of block b (fc = K^-1 (G_b prod K), then W fc).
+__device__ __forceinline__ long corr_edge_tab(const DevBasis &B, const CorrClass &C, const CorrItem &S, int e, int b, int dd) {
+  const int m = C.m, p = B.p, r = B.r;
+  int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
+  for (int i = 1; i < m; ++i)
+    if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
+      sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
+      lp[nf] = S.lpole[i];
+      nf++;
+    }
+  long sig = 0;
+  if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
+  if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
+  return B.tab_off[b] + sig * 2 * r * dd;
+}
+
+// Time-ordered DLR convolution of one edge for one item, in place in T (r x rows x cols), X and Y scratch.
+// LEFT: T <- conv(GK, T) with GK (d x d) = table, T (d x cols) (integrate_left_edge);
+// RIGHT: T <- conv(T, GK) with T (rows x d) (integrate_right_edge).  The table holds fc = K^-1 GK and W fc.
+template <int RP, bool LEFT>
+__device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, const double *sW, const double *sBK, const int *sPerm,
+                                          const double *tb, int rows, int cols, int d, double *T, double *X, double *Y, int lane) {
+  const int r = B.r, dc = rows * cols, dd = d * d;
+  // (a) coefficients of T (in place) and their Hilbert transform W Tc (into X), one column per lane
+  for (int col = lane; col < dc; col += 32) {
+    double x[RP];
+#pragma unroll
+    for (int i = 0; i < RP; ++i) {
+      const int src = sPerm[i];
+      x[i] = src >= 0 ? T[src * dc + col] : 0.0;
+    }
+    lu_solve_reg<RP>(sLU, x);
+#pragma unroll
+    for (int i = 0; i < RP; ++i)
+      if (i < r) T[i * dc + col] = x[i];
+    matvec_reg<RP>(sW, x, r, X + col, dc);
+  }
+  __syncwarp();
+  const double *fc = tb, *fw = tb + (long)r * dd;
+  // (b) Q_l (into Y)
+  for (int idx = lane; idx < r * dc; idx += 32) {
+    const int l = idx / dc, rem = idx - l * dc, x = rem / cols, z = rem - x * cols;
+    double a = 0.0;
+    if (LEFT) {
+      // f = table (d x d), g = T coefficients (d x cols): fma(Wf, g, fma(f, Wg, a))
+      const double *f = fc + l * dd, *ft = fw + l * dd, *g = T + l * dc, *gt = X + l * dc;
+      for (int y = 0; y < d; ++y) a = fmad(ft[x * d + y], g[y * cols + z], fmad(f[x * d + y], gt[y * cols + z], a));
+    } else {
+      // f = T coefficients (rows x d), g = table (d x d)
+      const double *f = T + l * dc, *ft = X + l * dc, *g = fc + l * dd, *gt = fw + l * dd;
+      for (int y = 0; y < d; ++y) a = fmad(ft[x * d + y], g[y * d + z], fmad(f[x * d + y], gt[y * d + z], a));
+    }
+    Y[idx] = a;
+  }
+  __syncwarp();
+  // (c) h1 = (beta K) Q (into X)
+  for (int col = lane; col < dc; col += 32) {
+    double q[RP];
+#pragma unroll
+    for (int i = 0; i < RP; ++i) q[i] = i < r ? Y[i * dc + col] : 0.0;
+    matvec_reg<RP>(sBK, q, r, X + col, dc);
+  }
+  __syncwarp();
+  // (d) P'_l = K(0, om_l) (f_l g_l) (into Y)
+  for (int idx = lane; idx < r * dc; idx += 32) {
+    const int l = idx / dc, rem = idx - l * dc, x = rem / cols, z = rem - x * cols;
+    double a = 0.0;
+    if (LEFT) {
+      const double *f = fc + l * dd, *g = T + l * dc;
+      for (int y = 0; y < d; ++y) a = fmad(f[x * d + y], g[y * cols + z], a);
+    } else {
+      const double *f = T + l * dc, *g = fc + l * dd;
+      for (int y = 0; y < d; ++y) a = fmad(f[x * d + y], g[y * d + z], a);
+    }
+    Y[idx] = mul(B.k0[l], a);
+  }
+  __syncwarp();
+  // (e) h = h1 + t_i (beta K) P' (into T)
+  for (int col = lane; col < dc; col += 32) {
+    double q[RP];
+#pragma unroll
+    for (int i = 0; i < RP; ++i) q[i] = i < r ? Y[i * dc + col] : 0.0;
+    constexpr int CH = 8;
+#pragma unroll 1
+    for (int l0 = 0; l0 < RP; l0 += CH) {
+      if (l0 >= r) break;
+      double a[CH];
+#pragma unroll
+      for (int jj = 0; jj < CH; ++jj) a[jj] = 0.0;
+#pragma unroll
+      for (int k = 0; k < RP; ++k) {
+#pragma unroll
+        for (int jj = 0; jj < CH; ++jj) a[jj] = fmad(sBK[k * RP + l0 + jj], q[k], a[jj]);
+      }
+#pragma unroll
+      for (int jj = 0; jj < CH; ++jj) {
+        const int i = l0 + jj;
+        if (i < r) T[i * dc + col] = fmad(B.tabs[i], a[jj], X[i * dc + col]);
+      }
+    }
+  }
+  __syncwarp();
+}
+
+// Dynamic shared memory: LU | W | BK | RF (4 RP^2 doubles, column-major) | perm (RP ints).
+// Per-warp global scratch (`warp_doubles` each): T | X | Y (r * nmax^2 each), right chains and left chains
+// (nb slots of r * nmax^2 each), accumulator (r * n * n).
+template <int RP>
+__global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis CB, const CorrClass *__restrict__ classes,
+                                                         const CorrChain *__restrict__ chains, const CorrTerm *__restrict__ terms,
+                                                         const WorkUnit *__restrict__ units, int n_units, int *__restrict__ unit_counter,
+                                                         const double *__restrict__ G, double *__restrict__ gout, double scale,
+                                                         int nmax, double *__restrict__ scratch, long warp_doubles) {
+  extern __shared__ double smem[];
+  double *sLU = smem, *sW = sLU + RP * RP, *sBK = sW + RP * RP, *sRF = sBK + RP * RP;
+  int *sPerm = reinterpret_cast<int *>(sRF + RP * RP);
+  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
+    sLU[i] = B.LUp[i];
+    sW[i] = B.Wp[i];
+    sBK[i] = B.BKp[i];
+    sRF[i] = CB.RFp[i];
+  }
+  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
+  __syncthreads();
+  const int r = B.r, n = B.n, nb = B.nb;
+  const int lane = threadIdx.x & 31;
+  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long slab = (long)r * nmax * nmax;
+  double *wb = scratch + gw * warp_doubles;
+  double *T = wb, *X = wb + slab, *Y = wb + 2 * slab;
+  double *Rs = wb + 3 * slab, *Ls = Rs + (long)nb * slab;
+  double *acc = Ls + (long)nb * slab;
+  for (int i = lane; i < r * n * n; i += 32) acc[i] = 0.0;
+  __syncwarp();
+  bool any = false;
+  while (true) {
+    int u = 0;
+    if (lane == 0) u = atomicAdd(unit_counter, 1);
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= n_units) break;
+    const WorkUnit wu = units[u];
+    const CorrClass &C = classes[wu.cls];
+    const int m = C.m, vct0 = C.vct0;
+    any = true;
+    for (int it = 0; it < wu.count; ++it) {
+      const CorrItem S = corr_decode(B, C, wu.first + it);
+      // ---- right chains
+      for (int j = 0; j < C.n_right; ++j) {
+        const CorrChain &H = chains[C.chain0 + j];
+        const int d1 = H.bd[1];
+        const double *g = G + B.goff[H.gblock];
+        for (int i = lane; i < r * d1 * d1; i += 32) T[i] = g[i];
+        __syncwarp();
+        for (int v = 1; v < vct0; ++v) {
+          const int b = H.path[v - 1], dv = H.bd[v], dvp = H.bd[v + 1];
+          const double *ktab;
+          int kcol;
+          const double *F = corr_vertex_op(B, C, S, v, b, dvp, dv, false, &ktab, &kcol);
+          const int per = r * dvp * d1;
+          for (int idx = lane; idx < per; idx += 32) {
+            const int t = idx / (dvp * d1), rem = idx - t * dvp * d1, x = rem / d1, z = rem - x * d1;
+            const double *Tt = T + t * dv * d1;
+            double a = 0.0;
+            for (int y = 0; y < dv; ++y) a = fmad(F[x * dv + y], Tt[y * d1 + z], a);
+            if (ktab) a = mul(a, ktab[(size_t)t * B.p + kcol]);
+            X[idx] = a;
+          }
+          __syncwarp();
+          for (int idx = lane; idx < per; idx += 32) T[idx] = X[idx];
+          __syncwarp();
+          const int eb = H.path[v], d = H.bd[v + 1];
+          corr_edge<RP, true>(B, sLU, sW, sBK, sPerm, B.tab + corr_edge_tab(B, C, S, v, eb, d * d), d, d1, d, T, X, Y, lane);
+        }
+        double *R = Rs + (long)j * slab;
+        for (int i = lane; i < r * H.rows * H.cols; i += 32) R[i] = mul(T[i], S.scale);
+        __syncwarp();
+      }
+      // ---- left chains
+      for (int j = 0; j < C.n_left; ++j) {
+        const CorrChain &H = chains[C.chain0 + C.n_right + j];
+        const int nrow = H.bd[2 * m];
+        const double *g = G + B.goff[H.gblock];
+        for (int i = lane; i < r * nrow * nrow; i += 32) T[i] = g[i];
+        __syncwarp();
+        for (int v = 2 * m - 1; v > vct0; --v) {
+          // U(t) <- U(t) F (nrow x bd(v+1)) (bd(v+1) x bd(v)), K factor
+          const int b = H.path[v - 1], K = H.bd[v], Rr = H.bd[v + 1];
+          const double *ktab;
+          int kcol;
+          const double *F = corr_vertex_op(B, C, S, v, b, Rr, K, true, &ktab, &kcol);
+          const int per = r * nrow * K;
+          for (int idx = lane; idx < per; idx += 32) {
+            const int t = idx / (nrow * K), rem = idx - t * nrow * K, x = rem / K, z = rem - x * K;
+            const double *Ut = T + t * nrow * Rr;
+            double a = 0.0;
+            for (int y = 0; y < Rr; ++y) a = fmad(Ut[x * Rr + y], F[y * K + z], a);
+            if (ktab) a = mul(a, ktab[(size_t)t * B.p + kcol]);
+            X[idx] = a;
+          }
+          __syncwarp();
+          for (int idx = lane; idx < per; idx += 32) T[idx] = X[idx];
+          __syncwarp();
+          const int eb = H.path[v - 1], d = H.bd[v];
+          corr_edge<RP, false>(B, sLU, sW, sBK, sPerm, B.tab + corr_edge_tab(B, C, S, v - 1, eb, d * d), nrow, d, d, T, X, Y, lane);
+        }
+        // L = reflect(U): K(t_i, -om_l) K^-1 U, one column per lane
+        const int dc = H.rows * H.cols;
+        double *L = Ls + (long)j * slab;
+        for (int col = lane; col < dc; col += 32) {
+          double x[RP];
+#pragma unroll
+          for (int i = 0; i < RP; ++i) {
+            const int src = sPerm[i];
+            x[i] = src >= 0 ? T[src * dc + col] : 0.0;
+          }
+          lu_solve_reg<RP>(sLU, x);
+          matvec_reg<RP>(sRF, x, r, L + col, dc);
+        }
+        __syncwarp();
+      }
+      // ---- trace contraction g(t)[mu][ka] += sum Tr[L F_mu R F^dag_ka]
+      for (int k = 0; k < C.n_terms; ++k) {
+        const CorrTerm &P = terms[C.term0 + k];
+        const double *R = Rs + (long)P.rchain * slab;
+        const double *L = Ls + (long)P.lchain * slab;
+        const double *Om = B.ops + CB.mu_off[P.mu * nb + P.e0];  // (c2 x c1)
+        const double *Ok = B.ops + CB.ka_off[P.ka * nb + P.e2];  // (c0 x c3)
+        const int c0 = P.c0, c1 = P.c1, c2 = P.c2, c3 = P.c3;
+        for (int t = lane; t < r; t += 32) {
+          const double *Rt = R + (long)t * c1 * c0, *Lt = L + (long)t * c3 * c2;
+          double s = 0.0;
+          for (int i = 0; i < c3; ++i)
+            for (int jj = 0; jj < c0; ++jj) {
+              double tm = 0.0;
+              for (int kk = 0; kk < c2; ++kk) {
+                double tp = 0.0;
+                for (int q = 0; q < c1; ++q) tp = fmad(Om[kk * c1 + q], Rt[q * c0 + jj], tp);
+                tm = fmad(Lt[i * c2 + kk], tp, tm);
+              }
+              s = fmad(tm, Ok[jj * c3 + i], s);
+            }
+          double *a = acc + ((long)t * n + P.mu) * n + P.ka;
+          *a = add(*a, s);
+        }
+        __syncwarp();
+      }
+    }
+  }
+  if (any)
+    for (int i = lane; i < r * n * n; i += 32) atomicAdd(gout + i, mul(scale, acc[i]));
+}
+
+}  // namespace xca

@@ -23,6 +23,7 @@
 #include "dlr_host.hpp"
 #include "sigma_kernel.cuh"
 #include "dyson_kernel.cuh"
+#include "spgf_kernel.cuh"
 
 namespace xca {
 
@@ -511,6 +512,18 @@ struct ClassSet {
   std::map<std::pair<int, int>, std::unique_ptr<ClassSet>> shards;
 };
 
+struct CorrSet {
+  std::vector<CorrClass> classes;
+  std::vector<CorrChain> chains;
+  std::vector<CorrTerm> terms;
+  std::vector<WorkUnit> units;
+  std::vector<int> cls_of_fbo;  // (fb * n^(m-1) + o) -> class, -1 when nothing closes a trace
+  DevBuf<CorrClass> d_classes;
+  DevBuf<CorrChain> d_chains;
+  DevBuf<CorrTerm> d_terms;
+  DevBuf<WorkUnit> d_units;
+};
+
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -547,6 +560,10 @@ struct Ctx {
   DevBuf<double> d_G, d_Sig, d_maxabs;
   std::vector<std::unique_ptr<DevBuf<double>>> user_bufs;
   std::map<std::string, std::unique_ptr<ClassSet>> class_cache;
+  std::map<std::string, std::unique_ptr<struct CorrSet>> corr_cache;  // correlator work lists
+  std::vector<double> RFp;                // RP x RP column-major: K(t_i, -om_l)
+  DevBuf<double> d_RFp, d_corr_scratch;
+  DevBuf<long> d_mu_off, d_ka_off;
   std::map<std::string, std::unique_ptr<ClassSet>> noalloc_classes;  // host-only work lists of the allocation-free call
   int unit_batches = 4;  // lockstep batches per work unit
   // profiling: CUDA events around every Sigma launch (enabled on request), user events, L2 flush buffer
@@ -646,8 +663,13 @@ static void setup_basis(Ctx *c, double beta, double lambda, double eps, int r, c
     for (int k = 0; k < r; ++k) std::swap(idx[k], idx[c->piv[k]]);
     for (int i = 0; i < r; ++i) c->perm[i] = idx[i];
   }
+  c->RFp.assign((size_t)RP * RP, 0.0);
+  for (int i = 0; i < r; ++i)
+    for (int l = 0; l < r; ++l) c->RFp[(size_t)l * RP + i] = k_it(it[i], -rf[l]);
   cudaStream_t s = c->stream;
   c->d_LUp.upload(c->LUp, s); c->d_Wp.upload(c->Wp, s); c->d_BKp.upload(c->BKp, s); c->d_perm.upload(c->perm, s);
+  c->d_RFp.upload(c->RFp, s);
+  c->corr_cache.clear();
   c->d_tabs.upload(c->tabs, s); c->d_k0.upload(c->k0, s); c->d_k1.upload(c->k1, s); c->d_rf.upload(c->rf, s);
   c->d_dims.upload(c->dims, s); c->d_goff.upload(c->goff, s);
   c->basis_ready = true;
@@ -917,6 +939,184 @@ static void real_part(const double *cplx, long n, std::vector<double> &out, cons
   }
 }
 
+
+// -------------------------------------------------------------------------------- single-particle correlator
+// Work list of compute_single_ptcle_gf for one topology and zero pattern of G: per (directions, orbital
+// tuple) the right chains (set_directions / eval_correlator's walk over vertices 1 .. vct0-1,
+// block_sparse_backbone.cpp:540-566), the left chains (vertices vct0+1 .. 2m-1, :567-600) and the
+// (mu, b, ka) terms of the trace contraction (:602-706) that close; classes without a term are dropped.
+static CorrSet *get_corr(Ctx *c, const Topology &T, const std::vector<int> &zero) {
+  const std::string key = class_key(T, zero);
+  auto itc = c->corr_cache.find(key);
+  if (itc != c->corr_cache.end()) return itc->second.get();
+  auto cs = std::make_unique<CorrSet>();
+  const int m = T.m, nv = 2 * m, vct0 = T.t[0][1], nb = c->nb, n = c->n;
+  const long fbmax = 1L << (m - 1), omax = ipow(n, m - 1), npt = ipow(c->p, m - 1);
+  if (npt > INT32_MAX) throw Error(XCA_ERR_UNSUPPORTED, "too many pole tuples");
+  cs->cls_of_fbo.assign(fbmax * omax, -1);
+  auto incomplete = [&](int ip) { return ip < 0 || zero[ip]; };
+  for (long fb = 0; fb < fbmax; ++fb)
+    for (long o = 0; o < omax; ++o) {
+      int fbv[MAXM] = {0}, dag[MAXV] = {0}, bar[MAXV] = {0}, orb[MAXV], vline[MAXV];
+      for (int v = 0; v < nv; ++v) { orb[v] = -1; vline[v] = 0; }
+      for (int i = 1; i < m; ++i) fbv[i] = (int)((fb >> (i - 1)) & 1);
+      // CorrelatorBackbone::set_directions (backbone.cpp:241-274)
+      dag[0] = 1; dag[vct0] = 0;
+      for (int i = 1; i < m; ++i) {
+        bar[T.t[i][0]] = 0; bar[T.t[i][1]] = 1;
+        if (fbv[i] == 1) { dag[T.t[i][0]] = 0; dag[T.t[i][1]] = 1; } else { dag[T.t[i][0]] = 1; dag[T.t[i][1]] = 0; }
+        vline[T.t[i][0]] = i; vline[T.t[i][1]] = i;
+      }
+      long oq = o;
+      for (int i = 1; i < m; ++i) {
+        const int ov = (int)(oq % n);
+        oq /= n;
+        orb[T.t[i][0]] = ov;
+        orb[T.t[i][1]] = ov;
+      }
+      auto idx_of = [&](int v, int col) -> int {
+        const int set = (int)c->labels[orb[v]];
+        return dag[v] ? c->Fd_idx[set * nb + col] : c->F_idx[set * nb + col];
+      };
+      CorrClass R;
+      std::memset(&R, 0, sizeof(R));
+      R.m = m; R.vct0 = vct0;
+      for (int i = 1; i < m; ++i) R.fbmask |= fbv[i] << i;
+      for (int i = 0; i < m; ++i) { R.la[i] = T.t[i][0]; R.lb[i] = T.t[i][1]; }
+      for (int v = 0; v < nv; ++v) {
+        R.vline[v] = vline[v];
+        if (v == 0 || v == vct0) continue;
+        R.vkind[v] = bar[v] ? (dag[v] ? 3 : 2) : (dag[v] ? 1 : 0);
+        R.vset[v] = (int)c->labels[orb[v]];
+        R.vqo[v] = (int)c->sinds[orb[v]];
+      }
+      // right chains from every start block
+      std::vector<CorrChain> rch(nb), lch(nb);
+      std::vector<int> rend(nb, -1), lend(nb, -1);
+      for (int b = 0; b < nb; ++b) {
+        CorrChain H;
+        std::memset(&H, 0, sizeof(H));
+        for (int v = 0; v < MAXV; ++v) H.path[v] = -1;
+        H.start = b; H.gblock = b;
+        H.path[0] = b;
+        H.bd[1] = c->dims[b];
+        bool bad = false;
+        int ip = b;
+        for (int v = 1; v < vct0; ++v) {
+          ip = idx_of(v, ip);
+          if (incomplete(ip)) { bad = true; break; }
+          H.path[v] = ip;
+          H.bd[v + 1] = c->dims[ip];
+        }
+        if (bad) continue;
+        H.rows = H.bd[vct0];
+        H.cols = H.bd[1];
+        rch[b] = H;
+        rend[b] = H.path[vct0 - 1];
+      }
+      // left chains from every start block
+      for (int b = 0; b < nb; ++b) {
+        CorrChain H;
+        std::memset(&H, 0, sizeof(H));
+        for (int v = 0; v < MAXV; ++v) H.path[v] = -1;
+        H.start = b;
+        H.path[vct0] = b;
+        H.bd[vct0 + 1] = c->dims[b];
+        bool bad = false;
+        int ip = b;
+        for (int v = vct0 + 1; v < nv; ++v) {
+          ip = idx_of(v, ip);
+          if (incomplete(ip)) { bad = true; break; }
+          H.path[v] = ip;
+          H.bd[v + 1] = c->dims[ip];
+        }
+        if (bad) continue;
+        H.gblock = H.path[nv - 1];
+        H.rows = H.bd[nv];
+        H.cols = H.bd[vct0 + 1];
+        lch[b] = H;
+        lend[b] = H.path[nv - 1];
+      }
+      // closing terms
+      std::vector<CorrTerm> terms;
+      std::vector<int> rused(nb, -1), lused(nb, -1);
+      std::vector<int> rlist, llist;
+      for (int mu = 0; mu < n; ++mu)
+        for (int b = 0; b < nb; ++b) {
+          const int e0 = rend[b];
+          if (incomplete(e0)) continue;
+          const int e1 = c->F_idx[c->labels[mu] * nb + e0];
+          if (incomplete(e1)) continue;
+          const int e2 = lend[e1];
+          if (incomplete(e2)) continue;
+          for (int ka = 0; ka < n; ++ka) {
+            if (c->Fd_idx[c->labels[ka] * nb + e2] != b) continue;
+            if (rused[b] < 0) { rused[b] = (int)rlist.size(); rlist.push_back(b); }
+            if (lused[e1] < 0) { lused[e1] = (int)llist.size(); llist.push_back(e1); }
+            CorrTerm P;
+            P.mu = mu; P.ka = ka; P.rchain = rused[b]; P.lchain = lused[e1]; P.e0 = e0; P.e2 = e2;
+            P.c0 = c->dims[b]; P.c1 = rch[b].rows; P.c2 = c->dims[e1]; P.c3 = lch[e1].rows;
+            terms.push_back(P);
+          }
+        }
+      if (terms.empty()) continue;
+      R.chain0 = (int)cs->chains.size();
+      R.n_right = (int)rlist.size();
+      R.n_left = (int)llist.size();
+      for (int b : rlist) cs->chains.push_back(rch[b]);
+      for (int b : llist) cs->chains.push_back(lch[b]);
+      R.term0 = (int)cs->terms.size();
+      R.n_terms = (int)terms.size();
+      cs->terms.insert(cs->terms.end(), terms.begin(), terms.end());
+      cs->cls_of_fbo[fb * omax + o] = (int)cs->classes.size();
+      cs->classes.push_back(R);
+    }
+  const int usz = 4;
+  for (size_t k = 0; k < cs->classes.size(); ++k)
+    for (long q = 0; q < npt; q += usz) cs->units.push_back(WorkUnit{(int)k, (int)q, (int)std::min<long>(usz, npt - q)});
+  cs->d_classes.upload(cs->classes, c->stream);
+  cs->d_chains.upload(cs->chains, c->stream);
+  cs->d_terms.upload(cs->terms, c->stream);
+  cs->d_units.upload(cs->units, c->stream);
+  CorrSet *ret = cs.get();
+  c->corr_cache[key] = std::move(cs);
+  return ret;
+}
+
+template <int RP>
+static void launch_corr_rp(Ctx *c, CorrSet *cs, const WorkUnit *d_units, int n_units, const double *G_dev, double *g_dev,
+                           double scale, int nsig) {
+  if (n_units == 0) return;
+  const size_t sm = (4 * (size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
+  CUDA_CHECK(cudaFuncSetAttribute(correlator_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  const int warps_per_cta = 4;
+  const int grid = std::max(1, std::min(2 * nsm, (n_units + warps_per_cta - 1) / warps_per_cta));
+  const long slab = (long)c->r * c->nmax * c->nmax;
+  const long warp_doubles = (3 + 2L * c->nb) * slab + (long)c->r * c->n * c->n;
+  c->d_corr_scratch.resize((size_t)grid * warps_per_cta * warp_doubles);
+  c->d_counter.resize(1);
+  CUDA_CHECK(cudaMemsetAsync(c->d_counter.ptr, 0, sizeof(int), c->stream));
+  CorrBasis CB;
+  CB.RFp = c->d_RFp.ptr;
+  CB.mu_off = c->d_mu_off.ptr;
+  CB.ka_off = c->d_ka_off.ptr;
+  correlator_kernel<RP><<<grid, 32 * warps_per_cta, sm, c->stream>>>(c->basis(nsig), CB, cs->d_classes.ptr, cs->d_chains.ptr,
+                                                                     cs->d_terms.ptr, d_units, n_units, c->d_counter.ptr, G_dev,
+                                                                     g_dev, scale, c->nmax, c->d_corr_scratch.ptr, warp_doubles);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+}
+
+static void launch_corr(Ctx *c, CorrSet *cs, const WorkUnit *d_units, int n_units, const double *G_dev, double *g_dev, double scale,
+                        int nsig) {
+  switch (c->RP) {
+    case 32: launch_corr_rp<32>(c, cs, d_units, n_units, G_dev, g_dev, scale, nsig); break;
+    case 48: launch_corr_rp<48>(c, cs, d_units, n_units, G_dev, g_dev, scale, nsig); break;
+    default: launch_corr_rp<64>(c, cs, d_units, n_units, G_dev, g_dev, scale, nsig); break;
+  }
+}
 
 // -------------------------------------------------------------------------------- Dyson, trace, normalisation
 static DysonBasis dyson_basis(Ctx *c) {
@@ -1286,6 +1486,21 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
   c->d_F_off.upload(c->F_off, s); c->d_Fd_off.upload(c->Fd_off, s); c->d_Fb_off.upload(c->Fb_off, s); c->d_Fdb_off.upload(c->Fdb_off, s);
   c->class_cache.clear();
   c->noalloc_classes.clear();
+  c->corr_cache.clear();
+  {
+    // per-orbital F and F^dag slabs (the external operators of the single-particle correlator)
+    std::vector<long> mo((size_t)n * n_blocks, -1), ko((size_t)n * n_blocks, -1);
+    for (int o = 0; o < n; ++o) {
+      const long sset = labels[o], qo = c->sinds[o];
+      for (int b = 0; b < n_blocks; ++b) {
+        const int tf = c->F_idx[sset * n_blocks + b], td = c->Fd_idx[sset * n_blocks + b];
+        if (tf >= 0) mo[(size_t)o * n_blocks + b] = c->F_off[sset * n_blocks + b] + qo * block_dims[tf] * block_dims[b];
+        if (td >= 0) ko[(size_t)o * n_blocks + b] = c->Fd_off[sset * n_blocks + b] + qo * block_dims[td] * block_dims[b];
+      }
+    }
+    c->d_mu_off.upload(mo, s);
+    c->d_ka_off.upload(ko, s);
+  }
   CUDA_CHECK(cudaStreamSynchronize(s));
   c->ready = true;
   API_END
@@ -1504,6 +1719,64 @@ int xca_axpby_device(xca_ctx *ctx, double alpha, const double *x_dev, double bet
   axpby_kernel<<<(int)std::max<long>(1, std::min<long>(1184, (n + 255) / 256)), 256, 0, c->stream>>>(alpha, x_dev, beta, y_dev, n);
   c->launches++;
   CUDA_CHECK(cudaGetLastError());
+  API_END
+}
+
+int xca_compute_single_ptcle_gf_device(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale, double *g_dev) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c->ready) throw Error(XCA_ERR_INVALID, "evaluator not set up");
+  set_device(c);
+  Topology T = parse_topology(m, topology);
+  auto zero = zero_flags_device(c, G_dev);
+  CorrSet *cs = get_corr(c, T, zero);
+  int nsig = prepare_tables(c, G_dev, m);
+  launch_corr(c, cs, cs->d_units.ptr, (int)cs->units.size(), G_dev, g_dev, scale, nsig);
+  API_END
+}
+
+int xca_compute_single_ptcle_gf(xca_ctx *ctx, const double *G, int m, const int *topology, const long *f_ix, long n_fix, double *g_out) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c->ready) throw Error(XCA_ERR_INVALID, "evaluator not set up");
+  set_device(c);
+  Topology T = parse_topology(m, topology);
+  const long omax = ipow(c->n, m - 1), npt = ipow(c->p, m - 1);
+  const long nmaxb = (1L << (m - 1)) * omax * npt;
+  std::vector<double> g;
+  real_part(G, c->slab, g, "G");
+  const long nout = (long)c->r * c->n * c->n;
+  c->d_G.resize(c->slab);
+  c->d_Sig.resize(std::max(c->slab, nout));
+  CUDA_CHECK(cudaMemcpyAsync(c->d_G.ptr, g.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  zero_kernel<<<64, 256, 0, c->stream>>>(c->d_Sig.ptr, nout);
+  c->launches++;
+  auto zero = zero_flags_device(c, c->d_G.ptr);
+  CorrSet *cs = get_corr(c, T, zero);
+  int nsig = prepare_tables(c, c->d_G.ptr, m);
+  if (f_ix == nullptr) {
+    launch_corr(c, cs, cs->d_units.ptr, (int)cs->units.size(), c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
+  } else {
+    std::vector<WorkUnit> units;
+    for (long z = 0; z < n_fix; ++z) {
+      const long f = f_ix[z];
+      if (f < 0 || f >= nmaxb) throw Error(XCA_ERR_RUNTIME, "DiagramEvaluator::compute_single_ptcle_gf: f_ix out of range");
+      const long o = f % omax, q = f / omax, pix = q % npt, fb = q / npt;
+      const int k = cs->cls_of_fbo[fb * omax + o];
+      if (k >= 0) units.push_back(WorkUnit{k, (int)pix, 1});
+    }
+    DevBuf<WorkUnit> du;
+    du.upload(units, c->stream);
+    launch_corr(c, cs, du.ptr, (int)units.size(), c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
+    CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  }
+  std::vector<double> out(nout);
+  CUDA_CHECK(cudaMemcpyAsync(out.data(), c->d_Sig.ptr, nout * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  for (long i = 0; i < nout; ++i) {
+    g_out[2 * i] = out[i];
+    g_out[2 * i + 1] = 0.0;
+  }
   API_END
 }
 
