@@ -42,13 +42,8 @@ def parse():
 
 
 def topologies(max_order=3):
-    from xca_b200.diag import all_connected_pairings
-    out = []
-    for order in range(1, max_order + 1):
-        for sign, topo in all_connected_pairings(order):
-            # Sigma_order += (-1)^order * parity * (-1)^(order+1) * compute_self_energy
-            out.append((order, np.array(topo, np.int32), float((-1) ** order * sign * (-1) ** (order + 1))))
-    return out
+    from xca_b200.distributed import sigma_terms
+    return [(order, np.array(topo, np.int32), fac) for order, topo, fac in sigma_terms(max_order)]
 
 
 def build_model():
@@ -194,14 +189,14 @@ def main():
     S_t = torch.zeros(ev.slab, dtype=torch.float64, device=dev)
     torch.cuda.synchronize()
 
+    from xca_b200.distributed import self_energy_sharded
+
+    def allreduce():
+        dist.all_reduce(S_t)
+        torch.cuda.synchronize()
+
     def step():
-        ev.zero_device(S_t.data_ptr(), ev.slab)
-        for _, t, fac in topos:
-            ev.compute_self_energy_device_shard(G_t.data_ptr(), t, fac, S_t.data_ptr(), rank, world)
-        if world > 1:
-            ev.synchronize()
-            dist.all_reduce(S_t)
-            torch.cuda.synchronize()
+        self_energy_sharded(ev, G_t.data_ptr(), S_t.data_ptr(), topos, rank, world, allreduce if world > 1 else None)
 
     for _ in range(args.warmup):
         step()

@@ -127,3 +127,26 @@ def test_rejects_cross_set_coefficients():
     bad[:, 0, 2] = 0.1  # orbitals 0 and 2 are in different symmetry sets
     with pytest.raises(ValueError):
         DiagramEvaluator.from_arrays(m.beta, m.lam, m.eps, d.rf, d.it, m.hyb_poles, bad, Fq)
+
+
+@pytest.mark.parametrize("n_shards", [1, 3])
+def test_shards_partition_the_work(n_shards):
+    # the work-unit shards of every rank, evaluated one after another on one GPU, add up to the full Sigma
+    from xca_b200.distributed import sigma_terms
+    d = O.Dlr(40.0, 1e-8)
+    m = models.kanamori_2orb(d.rf, d.it, 4.0, 40.0, 1e-8)
+    G = models.seeded_G(m, 2)
+    dev, _ = _pair(m, d)
+    gbuf = dev.device_buffer(0, dev.slab)
+    full = dev.device_buffer(1, dev.slab)
+    part = dev.device_buffer(2, dev.slab)
+    dev.to_device(gbuf, dev.pack(G).real)
+    dev.zero_device(full, dev.slab)
+    dev.zero_device(part, dev.slab)
+    for _, topo, fac in sigma_terms(3):
+        dev.compute_self_energy_device(gbuf, topo, fac, full)
+        for s in range(n_shards):
+            dev.compute_self_energy_device_shard(gbuf, topo, fac, part, s, n_shards)
+    a = dev.unpack(dev.to_host(part, dev.slab))
+    b = dev.unpack(dev.to_host(full, dev.slab))
+    assert _node_rel_err(a, b) <= 1.0
