@@ -71,6 +71,18 @@ struct WorkUnit {
   int count;
 };
 
+// Per-item state of a batch, kept in shared memory.
+struct ItemState {
+  double scale;          // prefactor * prefactor sign * order / direction sign
+  int lpole[MAXM];       // pole index of line i (i >= 1)
+  int caseA[MAXM];       // line i in case 4(a): K on its end vertices; else 4(b): K on the edges it spans
+  long opoff;            // per-step: operator slab offset of this item
+  long taboff;           // per-step: edge-table offset of this item
+  int kcol;              // per-step: K-table column of the vertex (-1: none), sign in kneg
+  int kneg;
+  int keep;              // 1e-16 guard outcome
+};
+
 // Arithmetic of the plain FP64 path: the fused multiply-adds and the separately rounded products and
 // sums of the CPU restatement, at the same places and in the same order.
 __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }

@@ -1,0 +1,432 @@
+// Sigma backbone evaluation on the device, panel form (plain FP64 path).
+//
+// A CTA of PANEL_THREADS threads takes a run of pole tuples of one path class (work unit) and evaluates
+// `batch` of them together.  The T slabs of the batch's items sit side by side as the columns of a
+// shared-memory panel (RP rows = tau nodes, NC columns = item x matrix entry), so every r x r DLR
+// operator of an edge acts on all of them at once:
+//   K^-1 T     one thread per column, the column in registers, substitution in dtrsm order;
+//   W gc, (beta K) Q, (beta K) P'   register-tiled products (TR x TC outputs per thread, operand pairs
+//                                   loaded as double2 from shared memory), each output one chain of
+//                                   fused multiply-adds over k ascending from zero;
+// and the per-item steps (vertex products with the item's operator and K factor, Q and P' with the
+// item's edge table, the zero vertex) run with the threads striding over panel entries.  Every element
+// sees exactly the operations, in the same order, as in the CPU restatement, so each item's contribution
+// is bit-identical to it (sigma_kernel.cuh documents the item arithmetic and its reference lines).
+#pragma once
+#include "sigma_kernel.cuh"
+
+namespace xca {
+
+constexpr int PANEL_THREADS = 256;
+constexpr int PANEL_BMAX = 128;  // items per batch at most
+
+template <int RP>
+struct PanelCfg;
+template <>
+struct PanelCfg<32> { static constexpr int NC = 192, TR = 4, TC = 6; };
+template <>
+struct PanelCfg<48> { static constexpr int NC = 128, TR = 6, TC = 4; };
+template <>
+struct PanelCfg<64> { static constexpr int NC = 64, TR = 4, TC = 4; };
+
+template <int RP>
+__host__ __device__ constexpr int panel_nc() { return PanelCfg<RP>::NC; }
+
+// Dynamic shared memory of the panel kernels, in doubles.
+template <int RP>
+__host__ __device__ constexpr size_t panel_smem_doubles() {
+  return 3 * (size_t)RP * RP + 3 * (size_t)RP * PanelCfg<RP>::NC + (sizeof(ItemState) * PANEL_BMAX + 7) / 8 + (RP + 1) / 2;
+}
+
+// Y[i][c] = sum_{k < r} M[i][k] X[k][c] for i < r, c < ncols (M column-major RP x RP; X, Y panels with row
+// stride NC).  EPI: Y[i][c] = fma(t_i, (M X)[i][c], H1[i][c]).  Each thread owns a TR x TC tile; the
+// threads of a warp share the row tile, so the M operands are broadcasts.
+template <int RP, bool EPI>
+__device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const double *__restrict__ X, double *__restrict__ Y, int r,
+                                           int ncols, const double *__restrict__ tabs, const double *__restrict__ H1) {
+  constexpr int NC = PanelCfg<RP>::NC, TR = PanelCfg<RP>::TR, TC = PanelCfg<RP>::TC;
+  constexpr int CT = NC / TC;
+  static_assert((RP / TR) * CT == PANEL_THREADS, "panel tiling must cover the CTA");
+  const int rt = threadIdx.x / CT, ct = threadIdx.x - rt * CT;
+  const int i0 = rt * TR, c0 = ct * TC;
+  if (i0 >= r || c0 >= ncols) return;
+  double acc[TR][TC];
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b) acc[a][b] = 0.0;
+#pragma unroll 2
+  for (int k = 0; k < r; ++k) {
+    double mv[TR], xv[TC];
+    const double2 *mp = reinterpret_cast<const double2 *>(sM + k * RP + i0);
+    const double2 *xp = reinterpret_cast<const double2 *>(X + k * NC + c0);
+#pragma unroll
+    for (int a = 0; a < TR / 2; ++a) {
+      const double2 t = mp[a];
+      mv[2 * a] = t.x;
+      mv[2 * a + 1] = t.y;
+    }
+#pragma unroll
+    for (int b = 0; b < TC / 2; ++b) {
+      const double2 t = xp[b];
+      xv[2 * b] = t.x;
+      xv[2 * b + 1] = t.y;
+    }
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) acc[a][b] = fmad(mv[a], xv[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int a = 0; a < TR; ++a) {
+    const int i = i0 + a;
+    if (i >= r) break;
+#pragma unroll
+    for (int b = 0; b < TC; ++b) {
+      const int c = c0 + b;
+      if (c < ncols) Y[i * NC + c] = EPI ? fmad(tabs[i], acc[a][b], H1[i * NC + c]) : acc[a][b];
+    }
+  }
+}
+
+// P[:, c] <- K^-1 P[:, c] for c < ncols, one column per thread (gathered through the pivots, LU
+// substitution in registers, written back in place).
+template <int RP>
+__device__ __forceinline__ void panel_lu_solve(const double *__restrict__ sLU, const int *__restrict__ sPerm, double *P, int r,
+                                               int ncols) {
+  constexpr int NC = PanelCfg<RP>::NC;
+  for (int c = threadIdx.x; c < ncols; c += PANEL_THREADS) {
+    double x[RP];
+#pragma unroll
+    for (int i = 0; i < RP; ++i) {
+      const int s = sPerm[i];
+      x[i] = s >= 0 ? P[s * NC + c] : 0.0;
+    }
+    lu_solve_reg<RP>(sLU, x);
+#pragma unroll
+    for (int i = 0; i < RP; ++i)
+      if (i < r) P[i * NC + c] = x[i];
+  }
+}
+
+template <int RP>
+__device__ __forceinline__ void stage_basis(const DevBasis &B, double *sLU, double *sW, double *sBK, int *sPerm) {
+  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
+    sLU[i] = B.LUp[i];
+    sW[i] = B.Wp[i];
+    sBK[i] = B.BKp[i];
+  }
+  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
+  __syncthreads();
+}
+
+// Edge tables (see edge_table_kernel): for block b and signature sig, fc = K^-1 (G_b prod K) and W fc.
+// A CTA takes NC consecutive (sig, entry) columns of one block: gather with the K factors, K^-1, write fc,
+// W fc, write.  `chunks` lists (block, first column) pairs.
+template <int RP>
+__global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(DevBasis B, const double *__restrict__ G,
+                                                                              const int2 *__restrict__ chunks, int n_chunks) {
+  constexpr int NC = PanelCfg<RP>::NC;
+  extern __shared__ double smem[];
+  double *sLU = smem, *sW = sLU + RP * RP, *sBK = sW + RP * RP;
+  double *PA = sBK + RP * RP, *PB = PA + RP * NC;
+  int *sPerm = reinterpret_cast<int *>(PB + RP * NC);
+  stage_basis<RP>(B, sLU, sW, sBK, sPerm);
+  const int r = B.r, p = B.p;
+  for (int ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
+    const int b = chunks[ch].x, col0 = chunks[ch].y;
+    const int d = B.dims[b], dd = d * d;
+    const long total = (long)B.nsig * dd;
+    const int ncols = (int)min((long)NC, total - col0);
+    const double *g = G + B.goff[b];
+    // gather: column c is (sig, e) = divmod(col0 + c, dd); rows are the tau nodes
+    for (int idx = threadIdx.x; idx < r * ncols; idx += PANEL_THREADS) {
+      const int t = idx / ncols, c = idx - t * ncols;
+      const long q = col0 + c;
+      const int sig = (int)(q / dd), e = (int)(q - (long)sig * dd);
+      int nf = 0, s1 = 0, l1 = 0, s2 = 0, l2 = 0;
+      if (sig >= 1 && sig < 1 + 2 * p) {
+        nf = 1;
+        s1 = (sig - 1) / p;
+        l1 = (sig - 1) - s1 * p;
+      } else if (sig >= 1 + 2 * p) {
+        nf = 2;
+        const int qq = sig - 1 - 2 * p;
+        const int a = qq / (2 * p), cc = qq - a * (2 * p);
+        s1 = a / p; l1 = a - s1 * p;
+        s2 = cc / p; l2 = cc - s2 * p;
+      }
+      double v = g[t * dd + e];
+      if (nf >= 1) v = mul(v, (s1 ? B.kitm : B.kitp)[(size_t)t * p + l1]);
+      if (nf >= 2) v = mul(v, (s2 ? B.kitm : B.kitp)[(size_t)t * p + l2]);
+      PA[t * NC + c] = v;
+    }
+    __syncthreads();
+    panel_lu_solve<RP>(sLU, sPerm, PA, r, ncols);
+    __syncthreads();
+    panel_gemm<RP, false>(sW, PA, PB, r, ncols, nullptr, nullptr);
+    __syncthreads();
+    double *out = const_cast<double *>(B.tab) + B.tab_off[b];
+    for (int idx = threadIdx.x; idx < r * ncols; idx += PANEL_THREADS) {
+      const int t = idx / ncols, c = idx - t * ncols;
+      const long q = col0 + c;
+      const long sig = q / dd, e = q - sig * dd;
+      double *o = out + sig * 2 * r * dd;
+      o[t * dd + e] = PA[t * NC + c];
+      o[(long)r * dd + t * dd + e] = PB[t * NC + c];
+    }
+    __syncthreads();
+  }
+}
+
+// Dynamic shared memory: LU | W | BK (3 RP^2, column-major) | panels A, B, C (RP x NC each) | item states
+// (PANEL_BMAX) | perm (RP ints).
+template <int RP>
+__global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis B, const ClassRec *__restrict__ classes,
+                                                                        const WorkUnit *__restrict__ units, int n_units,
+                                                                        int *__restrict__ unit_counter, const double *__restrict__ G,
+                                                                        double *__restrict__ Sigma, double scale) {
+  constexpr int NC = PanelCfg<RP>::NC;
+  extern __shared__ double smem[];
+  double *sLU = smem, *sW = sLU + RP * RP, *sBK = sW + RP * RP;
+  double *PA = sBK + RP * RP, *PB = PA + RP * NC, *PC = PB + RP * NC;
+  ItemState *ist = reinterpret_cast<ItemState *>(PC + RP * NC);
+  int *sPerm = reinterpret_cast<int *>(reinterpret_cast<double *>(ist) + (sizeof(ItemState) * PANEL_BMAX + 7) / 8);
+  __shared__ int s_unit;
+  __shared__ unsigned long long s_max[PANEL_BMAX];
+  stage_basis<RP>(B, sLU, sW, sBK, sPerm);
+  const int r = B.r, p = B.p, n = B.n, tid = threadIdx.x;
+
+  while (true) {
+    if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
+    __syncthreads();
+    const int u = s_unit;
+    __syncthreads();
+    if (u >= n_units) break;
+    const WorkUnit wu = units[u];
+    const ClassRec &C = classes[wu.cls];
+    const int m = C.m, vct0 = C.vct0;
+    const int d0 = C.bdims[0], d1 = C.bdims[1];
+    const int dout = C.bdims[2 * m];
+    const int cap = C.batch;
+    const int nops = 4 * m - 3;
+
+    for (int first = 0; first < wu.count; first += cap) {
+      const int nbi = min(cap, wu.count - first);
+      // ---- decode the pole tuples (Backbone::set_pole_inds, backbone.cpp:86-150)
+      if (tid < nbi) {
+        ItemState &S = ist[tid];
+        int q = wu.first + first + tid;
+        for (int i = 0; i < MAXM; ++i) { S.lpole[i] = 0; S.caseA[i] = 0; }
+        for (int i = 1; i < m; ++i) {
+          S.lpole[i] = q % p;
+          q /= p;
+        }
+        double pf = 1.0;
+        int psign = 1;
+        for (int i = 1; i < m; ++i) {
+          const int fwd = (C.fbmask >> i) & 1;
+          const double w = B.polesb[S.lpole[i]];
+          S.caseA[i] = fwd ? (w <= 0.0) : (w >= 0.0);
+          if (!fwd) psign = -psign;
+          const int row = S.caseA[i] ? (fwd ? 1 : 0) : (fwd ? 0 : 1);
+          const int ex = S.caseA[i] ? 1 : C.lb[i] - C.la[i] - 1;
+          if (ex != 0) pf = mul(pf, B.kpow[((size_t)row * p + S.lpole[i]) * (MAXE + 1) + ex]);
+        }
+        int dsign = (m % 2 == 0) ? -1 : 1;
+        if (!(C.fbmask & 1)) dsign = -dsign;
+        S.scale = mul(pf, (double)(psign * dsign));
+        s_max[tid] = 0ull;
+      }
+      double *T = PA, *X = PB, *Y = PC;
+      // T := G[ind_path[0]] (d1 x d1) for every item
+      {
+        const double *g = G + B.goff[C.ind_path[0]];
+        const int dc = d1 * d1, nc = nbi * dc;
+        for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
+          const int t = idx / nc, c = idx - t * nc;
+          T[t * NC + c] = g[t * dc + (c % dc)];
+        }
+      }
+      __syncthreads();
+
+      for (int op = 0; op < nops; ++op) {
+        int kind, v;
+        const int pre = 2 * (vct0 - 1);
+        if (op < pre) { v = 1 + op / 2; kind = (op & 1) ? 1 : 0; }
+        else if (op == pre) { v = vct0; kind = 2; }
+        else { const int q = op - pre - 1; v = vct0 + 1 + q / 2; kind = (q & 1) ? 0 : 1; }
+        const int ncol = v < vct0 ? d1 : d0;
+
+        if (kind == 0) {
+          // ---- vertex v: T(t) <- k(t) F T(t)  (multiply_left_vertex)
+          const int line = C.vline[v];
+          const int b = C.ind_path[v - 1];
+          const int dv = C.bdims[v], dvp = C.bdims[v + 1];
+          const int s = C.vset[v], qo = C.vqo[v];
+          if (tid < nbi) {
+            ItemState &S = ist[tid];
+            const int l = S.lpole[line];
+            long off;
+            switch (C.vkind[v]) {
+              case 0: off = B.F_off[s * B.nb + b] + (long)qo * dvp * dv; break;
+              case 1: off = B.Fd_off[s * B.nb + b] + (long)qo * dvp * dv; break;
+              case 2: off = B.Fb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
+              default: off = B.Fdb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
+            }
+            S.opoff = off;
+            S.kcol = -1;
+            if (line > 0 && S.caseA[line]) {
+              const int fwd = (C.fbmask >> line) & 1;
+              const int ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
+              S.kcol = l;
+              S.kneg = ks < 0;
+            }
+          }
+          __syncthreads();
+          const int dci = dv * ncol, dco = dvp * ncol, nc = nbi * dco;
+          for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
+            const int t = idx / nc, c = idx - t * nc;
+            const int j = c / dco, e = c - j * dco, x = e / ncol, z = e - x * ncol;
+            const ItemState &S = ist[j];
+            const double *F = B.ops + S.opoff;
+            const double *Tt = T + t * NC + j * dci;
+            double a = 0.0;
+            for (int y = 0; y < dv; ++y) a = fmad(F[x * dv + y], Tt[y * ncol + z], a);
+            if (S.kcol >= 0) a = mul(a, (S.kneg ? B.kitm : B.kitp)[(size_t)t * p + S.kcol]);
+            X[t * NC + c] = a;
+          }
+          __syncthreads();
+          double *tmp = T; T = X; X = tmp;
+        } else if (kind == 1) {
+          // ---- edge e: T <- conv(G_b prod K, T)  (integrate_left_edge, time-ordered convolution)
+          const int e = v < vct0 ? v : v - 1;
+          const int b = C.ind_path[e];
+          const int d = C.bdims[e + 1];
+          const int dd = d * d, dc = d * ncol, nc = nbi * dc;
+          if (tid < nbi) {
+            ItemState &S = ist[tid];
+            int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
+            for (int i = 1; i < m; ++i)
+              if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
+                sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
+                lp[nf] = S.lpole[i];
+                nf++;
+              }
+            long sig = 0;
+            if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
+            if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
+            S.taboff = B.tab_off[b] + sig * 2 * r * dd;
+          }
+          // (a) gc = K^-1 T (in place), then Gt = W gc (into X)
+          panel_lu_solve<RP>(sLU, sPerm, T, r, nc);
+          __syncthreads();
+          panel_gemm<RP, false>(sW, T, X, r, nc, nullptr, nullptr);
+          __syncthreads();
+          // (b) Q_l = Ft_l gc_l + fc_l Gt_l (into Y)
+          for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
+            const int l = idx / nc, c = idx - l * nc;
+            const int j = c / dc, ee = c - j * dc, x = ee / ncol, z = ee - x * ncol;
+            const double *tb = B.tab + ist[j].taboff;
+            const double *fl = tb + l * dd, *ftl = tb + (long)r * dd + l * dd;
+            const double *gl = T + l * NC + j * dc, *gtl = X + l * NC + j * dc;
+            double a = 0.0;
+            for (int y = 0; y < d; ++y) a = fmad(ftl[x * d + y], gl[y * ncol + z], fmad(fl[x * d + y], gtl[y * ncol + z], a));
+            Y[l * NC + c] = a;
+          }
+          __syncthreads();
+          // (c) h1 = (beta K) Q (into X; Gt is no longer needed)
+          panel_gemm<RP, false>(sBK, Y, X, r, nc, nullptr, nullptr);
+          __syncthreads();
+          // (d) P'_l = K(0, om_l) (fc_l gc_l) (into Y)
+          for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
+            const int l = idx / nc, c = idx - l * nc;
+            const int j = c / dc, ee = c - j * dc, x = ee / ncol, z = ee - x * ncol;
+            const double *fl = B.tab + ist[j].taboff + l * dd;
+            const double *gl = T + l * NC + j * dc;
+            double a = 0.0;
+            for (int y = 0; y < d; ++y) a = fmad(fl[x * d + y], gl[y * ncol + z], a);
+            Y[l * NC + c] = mul(B.k0[l], a);
+          }
+          __syncthreads();
+          // (e) h = fma(t_i, (beta K) P', h1) (into T)
+          panel_gemm<RP, true>(sBK, Y, T, r, nc, B.tabs, X);
+          __syncthreads();
+        } else {
+          // ---- zero vertex (multiply_left_vertex_and_right_zero_vertex)
+          const int b_mu = C.ind_path[v - 1];
+          const int dv = C.bdims[v], dvp = C.bdims[v + 1];
+          const bool fwd = C.fbmask & 1;
+          const int pk = C.pk;
+          const long ok_off = fwd ? B.F_off[pk * B.nb + C.b_out] : B.Fd_off[pk * B.nb + C.b_out];
+          const long om_off = fwd ? B.Fd_off[pk * B.nb + b_mu] : B.F_off[pk * B.nb + b_mu];
+          const double hs = fwd ? 1.0 : -1.0;
+          int qs = 0;
+          for (int i = 0; i < n; ++i)
+            if (B.set_to_orb[pk * n + i] >= 0) qs = i + 1;
+          const int dci = dv * d1, dmid = dv * d0, dco = dvp * d0;
+          const int ncm = nbi * dmid, nco = nbi * dco;
+          for (int idx = tid; idx < r * nco; idx += PANEL_THREADS) {
+            const int t = idx / nco, c = idx - t * nco;
+            X[t * NC + c] = 0.0;
+          }
+          __syncthreads();
+          for (int mu = 0; mu < qs; ++mu) {
+            const int om = B.set_to_orb[pk * n + mu];
+            for (int idx = tid; idx < r * ncm; idx += PANEL_THREADS) {
+              const int t = idx / ncm, c = idx - t * ncm;
+              const int j = c / dmid, ee = c - j * dmid, x = ee / d0, z = ee - x * d0;
+              const double *Tt = T + t * NC + j * dci;
+              double a = 0.0;
+              for (int kap = 0; kap < qs; ++kap) {
+                const int ok = B.set_to_orb[pk * n + kap];
+                const double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
+                if (h == 0.0) continue;
+                const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0;
+                double tf = 0.0;
+                for (int y = 0; y < d1; ++y) tf = fmad(Tt[x * d1 + y], Fk[y * d0 + z], tf);
+                a = fmad(mul(hs, h), tf, a);
+              }
+              Y[t * NC + c] = a;
+            }
+            __syncthreads();
+            const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
+            for (int idx = tid; idx < r * nco; idx += PANEL_THREADS) {
+              const int t = idx / nco, c = idx - t * nco;
+              const int j = c / dco, ee = c - j * dco, x = ee / d0, z = ee - x * d0;
+              const double *Yt = Y + t * NC + j * dmid;
+              double a = 0.0;
+              for (int y = 0; y < dv; ++y) a = fmad(Fm[x * dv + y], Yt[y * d0 + z], a);
+              X[t * NC + c] = add(X[t * NC + c], a);
+            }
+            __syncthreads();
+          }
+          double *tmp = T; T = X; X = tmp;
+        }
+      }
+      // ---- prefactor and signs, the |T| > 1e-16 guard, accumulation
+      const int dco = dout * d0, nc = nbi * dco;
+      for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
+        const int t = idx / nc, c = idx - t * nc, j = c / dco;
+        const double v = fabs(mul(T[t * NC + c], ist[j].scale));
+        atomicMax(&s_max[j], (unsigned long long)__double_as_longlong(v));  // non-negative doubles order as integers
+      }
+      __syncthreads();
+      double *dst = Sigma + B.goff[C.b_out];
+      for (int idx = tid; idx < r * dco; idx += PANEL_THREADS) {
+        const int t = idx / dco, ee = idx - t * dco;
+        double a = 0.0;
+        bool keep_any = false;
+        for (int j = 0; j < nbi; ++j)
+          if (__longlong_as_double((long long)s_max[j]) > 1e-16) {
+            a = add(a, mul(T[t * NC + j * dco + ee], ist[j].scale));
+            keep_any = true;
+          }
+        if (keep_any) atomicAdd(dst + idx, mul(scale, a));
+      }
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace xca

@@ -22,6 +22,7 @@
 #include "../../include/xca_b200.h"
 #include "dlr_host.hpp"
 #include "sigma_kernel.cuh"
+#include "sigma_panel.cuh"
 #include "dyson_kernel.cuh"
 #include "spgf_kernel.cuh"
 
@@ -62,408 +63,7 @@ struct DevBuf {
   }
 };
 
-// -------------------------------------------------------------------------------- Sigma kernels
-// Per-warp item state kept in shared memory for one batch.
-struct ItemState {
-  double scale;          // prefactor * prefactor sign * order / direction sign
-  int lpole[MAXM];       // pole index of line i (i >= 1)
-  int caseA[MAXM];       // line i in case 4(a): K on its end vertices; else 4(b): K on the edges it spans
-  long opoff;            // per-step scratch: operator slab offset of this item
-  long taboff;           // per-step scratch: edge-table offset of this item
-  int kcol;              // per-step scratch: K-table column of the vertex (-1: none), sign in kneg
-  int kneg;
-  int keep;              // 1e-16 guard outcome
-};
-
-// Edge tables: for block b and K signature sig, fc = K^-1 (G_b * prod K) and Ft = W fc.
-// sig 0: no factor; 1 + s p + l: one factor (s = 0: K(t, +beta w_l), 1: K(t, -beta w_l));
-// 1 + 2p + (s1 p + l1) 2p + s2 p + l2: two factors, the lower line's first.
-template <int RP>
-__global__ void __launch_bounds__(128) edge_table_kernel(DevBasis B, const double *__restrict__ G, long n_pairs) {
-  extern __shared__ double smem[];
-  double *sLU = smem;
-  double *sW = sLU + RP * RP;
-  int *sPerm = reinterpret_cast<int *>(sW + RP * RP);
-  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
-    sLU[i] = B.LUp[i];
-    sW[i] = B.Wp[i];
-  }
-  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
-  __syncthreads();
-  const int r = B.r, p = B.p;
-  const int lane = threadIdx.x & 31;
-  const long warp_global = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
-  for (long pair = warp_global; pair < n_pairs; pair += nwarps) {
-    const int b = (int)(pair / B.nsig);
-    const int sig = (int)(pair - (long)b * B.nsig);
-    const int d = B.dims[b];
-    const int dd = d * d;
-    int nf = 0, s1 = 0, l1 = 0, s2 = 0, l2 = 0;
-    if (sig >= 1 && sig < 1 + 2 * p) {
-      nf = 1;
-      s1 = (sig - 1) / p;
-      l1 = (sig - 1) - s1 * p;
-    } else if (sig >= 1 + 2 * p) {
-      nf = 2;
-      int q = sig - 1 - 2 * p;
-      int a = q / (2 * p), c = q - a * (2 * p);
-      s1 = a / p; l1 = a - s1 * p;
-      s2 = c / p; l2 = c - s2 * p;
-    }
-    const double *g = G + B.goff[b];
-    double *out = const_cast<double *>(B.tab) + B.tab_off[b] + (long)sig * 2 * r * dd;
-    for (int col = lane; col < dd; col += 32) {
-      double x[RP];
-#pragma unroll
-      for (int i = 0; i < RP; ++i) {
-        int src = sPerm[i];
-        double v = 0.0;
-        if (src >= 0) {
-          v = g[src * dd + col];
-          if (nf >= 1) v = mul(v, (s1 ? B.kitm : B.kitp)[(size_t)src * p + l1]);
-          if (nf >= 2) v = mul(v, (s2 ? B.kitm : B.kitp)[(size_t)src * p + l2]);
-        }
-        x[i] = v;
-      }
-      lu_solve_reg<RP>(sLU, x);
-#pragma unroll
-      for (int i = 0; i < RP; ++i)
-        if (i < r) out[i * dd + col] = x[i];
-      matvec_reg<RP>(sW, x, r, out + (long)r * dd + col, dd);
-    }
-  }
-}
-
-// Dynamic shared memory: LU | W | BK (3 RP^2 doubles, column-major) | perm (RP ints) | per warp: 32 item
-// states, NSLAB slab regions of B.region doubles, r * nmax^2 doubles of accumulator.
-template <int RP>
-__global__ void __launch_bounds__(32 * WARPS_MAX) sigma_items_kernel(DevBasis B, const ClassRec *__restrict__ classes,
-                                                                      const WorkUnit *__restrict__ units, int n_units,
-                                                                      int *__restrict__ unit_counter, const double *__restrict__ G,
-                                                                      double *__restrict__ Sigma, double scale, int nmax) {
-  extern __shared__ double smem[];
-  const int r = B.r, p = B.p, n = B.n;
-  double *sLU = smem;
-  double *sW = sLU + RP * RP;
-  double *sBK = sW + RP * RP;
-  int *sPerm = reinterpret_cast<int *>(sBK + RP * RP);
-  double *warp_area = sBK + RP * RP + (RP + 1) / 2;
-  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
-    sLU[i] = B.LUp[i];
-    sW[i] = B.Wp[i];
-    sBK[i] = B.BKp[i];
-  }
-  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
-  __syncthreads();
-
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const size_t items_bytes = ((sizeof(ItemState) * 32 + 15) / 16) * 16;
-  const size_t warp_doubles = items_bytes / 8 + (size_t)NSLAB * B.region + (size_t)r * nmax * nmax;
-  double *wbase = warp_area + (size_t)warp * warp_doubles;
-  ItemState *ist = reinterpret_cast<ItemState *>(wbase);
-  double *slabs = wbase + items_bytes / 8;
-  double *acc = slabs + (size_t)NSLAB * B.region;
-
-  while (true) {
-    int u = 0;
-    if (lane == 0) u = atomicAdd(unit_counter, 1);
-    u = __shfl_sync(0xffffffffu, u, 0);
-    if (u >= n_units) break;
-    const WorkUnit wu = units[u];
-    const ClassRec &C = classes[wu.cls];
-    const int m = C.m, vct0 = C.vct0;
-    const int d0 = C.bdims[0], d1 = C.bdims[1];
-    const int dout = C.bdims[2 * m];
-    const int cap = C.batch;       // items per lockstep batch; cap * (largest d * c of the chain) <= 32
-    const int slab = r * C.dcmax;  // item j's T / X / Y slabs are j-strided within each of the three regions
-    const int nops = 4 * m - 3;    // V E ... Z ... E V: 2 (vct0 - 1) + 1 + 2 (2m - 1 - vct0)
-    for (int i = lane; i < r * dout * d0; i += 32) acc[i] = 0.0;
-    bool any = false;
-
-    for (int first = 0; first < wu.count; first += cap) {
-      const int nb_items = min(cap, wu.count - first);
-      // ---- decode the pole tuples (Backbone::set_pole_inds, backbone.cpp:86-150)
-      if (lane < nb_items) {
-        ItemState &S = ist[lane];
-        int q = wu.first + first + lane;
-        for (int i = 0; i < MAXM; ++i) { S.lpole[i] = 0; S.caseA[i] = 0; }
-        for (int i = 1; i < m; ++i) {
-          S.lpole[i] = q % p;
-          q /= p;
-        }
-        double pf = 1.0;
-        int psign = 1;
-        for (int i = 1; i < m; ++i) {
-          int fwd = (C.fbmask >> i) & 1;
-          double w = B.polesb[S.lpole[i]];
-          S.caseA[i] = fwd ? (w <= 0.0) : (w >= 0.0);
-          if (!fwd) psign = -psign;
-          int row = S.caseA[i] ? (fwd ? 1 : 0) : (fwd ? 0 : 1);
-          int ex = S.caseA[i] ? 1 : C.lb[i] - C.la[i] - 1;
-          if (ex != 0) pf = mul(pf, B.kpow[((size_t)row * p + S.lpole[i]) * (MAXE + 1) + ex]);
-        }
-        int dsign = (m % 2 == 0) ? -1 : 1;
-        if (!(C.fbmask & 1)) dsign = -dsign;
-        S.scale = mul(pf, (double)(psign * dsign));
-      }
-      double *T = slabs, *X = slabs + B.region, *Y = slabs + 2 * (size_t)B.region;
-      // T := G[ind_path[0]] (d1 x d1) for every item
-      {
-        const double *g = G + B.goff[C.ind_path[0]];
-        const int sz = r * d1 * d1;
-        for (int idx = lane; idx < nb_items * sz; idx += 32) {
-          int j = idx / sz;
-          T[(size_t)j * slab + (idx - j * sz)] = g[idx - j * sz];
-        }
-      }
-      __syncwarp();
-
-      for (int op = 0; op < nops; ++op) {
-        // op order: for v < vct0: vertex v, edge v; zero vertex; for v > vct0: edge v - 1, vertex v
-        int kind, v;
-        const int pre = 2 * (vct0 - 1);
-        if (op < pre) { v = 1 + op / 2; kind = (op & 1) ? 1 : 0; }
-        else if (op == pre) { v = vct0; kind = 2; }
-        else { int q = op - pre - 1; v = vct0 + 1 + q / 2; kind = (q & 1) ? 0 : 1; }
-        const int ncol = v < vct0 ? d1 : d0;
-
-        if (kind == 0) {
-          // ---- vertex v: T(t) <- k(t) F T(t)  (multiply_left_vertex)
-          const int line = C.vline[v];
-          const int b = C.ind_path[v - 1];
-          const int dv = C.bdims[v], dvp = C.bdims[v + 1];
-          const int s = C.vset[v], qo = C.vqo[v];
-          if (lane < nb_items) {
-            ItemState &S = ist[lane];
-            const int l = S.lpole[line];
-            long off;
-            switch (C.vkind[v]) {
-              case 0: off = B.F_off[s * B.nb + b] + (long)qo * dvp * dv; break;
-              case 1: off = B.Fd_off[s * B.nb + b] + (long)qo * dvp * dv; break;
-              case 2: off = B.Fb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
-              default: off = B.Fdb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
-            }
-            S.opoff = off;
-            S.kcol = -1;
-            if (line > 0 && S.caseA[line]) {
-              int fwd = (C.fbmask >> line) & 1;
-              int ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
-              S.kcol = l;
-              S.kneg = ks < 0;
-            }
-          }
-          __syncwarp();
-          const int per = r * dvp * ncol;
-          for (int idx = lane; idx < nb_items * per; idx += 32) {
-            int j = idx / per;
-            int rem = idx - j * per;
-            int t = rem / (dvp * ncol);
-            int r2 = rem - t * dvp * ncol;
-            int x = r2 / ncol, z = r2 - x * ncol;
-            const ItemState &S = ist[j];
-            const double *F = B.ops + S.opoff;
-            const double *Tt = T + (size_t)j * slab + t * dv * ncol;
-            double a = 0.0;
-            for (int y = 0; y < dv; ++y) a = fmad(F[x * dv + y], Tt[y * ncol + z], a);
-            if (S.kcol >= 0) a = mul(a, (S.kneg ? B.kitm : B.kitp)[(size_t)t * p + S.kcol]);
-            X[(size_t)j * slab + rem] = a;
-          }
-          __syncwarp();
-          double *tmp = T; T = X; X = tmp;
-        } else if (kind == 1) {
-          // ---- edge e: T <- conv(G_b * prod K, T)  (integrate_left_edge, time-ordered convolution);
-          // edge v follows vertex v before the zero vertex, edge v - 1 precedes vertex v after it
-          const int e = v < vct0 ? v : v - 1;
-          const int b = C.ind_path[e];
-          const int d = C.bdims[e + 1];
-          const int dd = d * d, dc = d * ncol;
-          if (lane < nb_items) {
-            ItemState &S = ist[lane];
-            int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
-            for (int i = 1; i < m; ++i)
-              if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
-                sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
-                lp[nf] = S.lpole[i];
-                nf++;
-              }
-            long sig = 0;
-            if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
-            if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
-            S.taboff = B.tab_off[b] + sig * 2 * r * dd;
-          }
-          __syncwarp();
-          // (a) gc = K^-1 T (in place) and Gt = W gc (into X), one (item, column) per lane
-          for (int cl = lane; cl < nb_items * dc; cl += 32) {
-            const int j = cl / dc, col = cl - j * dc;
-            double *Tj = T + (size_t)j * slab;
-            double x[RP];
-#pragma unroll
-            for (int i = 0; i < RP; ++i) {
-              int src = sPerm[i];
-              x[i] = src >= 0 ? Tj[src * dc + col] : 0.0;
-            }
-            lu_solve_reg<RP>(sLU, x);
-#pragma unroll
-            for (int i = 0; i < RP; ++i)
-              if (i < r) Tj[i * dc + col] = x[i];
-            matvec_reg<RP>(sW, x, r, X + (size_t)j * slab + col, dc);
-          }
-          __syncwarp();
-          // (b) Q_l = Ft_l gc_l + fc_l Gt_l  (into Y)
-          const int per = r * dc;
-          for (int idx = lane; idx < nb_items * per; idx += 32) {
-            int j = idx / per;
-            int rem = idx - j * per;
-            int l = rem / dc;
-            int r2 = rem - l * dc;
-            int x = r2 / ncol, z = r2 - x * ncol;
-            const double *tb = B.tab + ist[j].taboff;
-            const double *fl = tb + l * dd, *ftl = tb + (long)r * dd + l * dd;
-            const double *gl = T + (size_t)j * slab + l * dc, *gtl = X + (size_t)j * slab + l * dc;
-            double a = 0.0;
-            for (int y = 0; y < d; ++y) a = fmad(ftl[x * d + y], gl[y * ncol + z], fmad(fl[x * d + y], gtl[y * ncol + z], a));
-            Y[(size_t)j * slab + rem] = a;
-          }
-          __syncwarp();
-          // (c) h1 = (beta K) Q  (into X, Gt no longer needed)
-          for (int cl = lane; cl < nb_items * dc; cl += 32) {
-            const int j = cl / dc, col = cl - j * dc;
-            const double *Yj = Y + (size_t)j * slab;
-            double q[RP];
-#pragma unroll
-            for (int i = 0; i < RP; ++i) q[i] = i < r ? Yj[i * dc + col] : 0.0;
-            matvec_reg<RP>(sBK, q, r, X + (size_t)j * slab + col, dc);
-          }
-          __syncwarp();
-          // (d) P'_l = K(0, om_l) (fc_l gc_l)  (into Y)
-          for (int idx = lane; idx < nb_items * per; idx += 32) {
-            int j = idx / per;
-            int rem = idx - j * per;
-            int l = rem / dc;
-            int r2 = rem - l * dc;
-            int x = r2 / ncol, z = r2 - x * ncol;
-            const double *fl = B.tab + ist[j].taboff + l * dd;
-            const double *gl = T + (size_t)j * slab + l * dc;
-            double a = 0.0;
-            for (int y = 0; y < d; ++y) a = fmad(fl[x * d + y], gl[y * ncol + z], a);
-            Y[(size_t)j * slab + rem] = mul(B.k0[l], a);
-          }
-          __syncwarp();
-          // (e) h = h1 + t_i (beta K) P'  (into T)
-          for (int cl = lane; cl < nb_items * dc; cl += 32) {
-            const int j = cl / dc, col = cl - j * dc;
-            const double *Yj = Y + (size_t)j * slab;
-            double q[RP];
-#pragma unroll
-            for (int i = 0; i < RP; ++i) q[i] = i < r ? Yj[i * dc + col] : 0.0;
-            double *Tj = T + (size_t)j * slab;
-            const double *h1 = X + (size_t)j * slab;
-            constexpr int CH = 8;
-#pragma unroll 1
-            for (int l0 = 0; l0 < RP; l0 += CH) {
-              if (l0 >= r) break;
-              double a[CH];
-#pragma unroll
-              for (int jj = 0; jj < CH; ++jj) a[jj] = 0.0;
-#pragma unroll
-              for (int k = 0; k < RP; ++k) {
-#pragma unroll
-                for (int jj = 0; jj < CH; ++jj) a[jj] = fmad(sBK[k * RP + l0 + jj], q[k], a[jj]);
-              }
-#pragma unroll
-              for (int jj = 0; jj < CH; ++jj) {
-                int i = l0 + jj;
-                if (i < r) Tj[i * dc + col] = fmad(B.tabs[i], a[jj], h1[i * dc + col]);
-              }
-            }
-          }
-          __syncwarp();
-        } else {
-          // ---- zero vertex (multiply_left_vertex_and_right_zero_vertex)
-          const int b_mu = C.ind_path[v - 1];
-          const int dv = C.bdims[v], dvp = C.bdims[v + 1];
-          const bool fwd = C.fbmask & 1;
-          const int pk = C.pk;
-          const long ok_off = fwd ? B.F_off[pk * B.nb + C.b_out] : B.Fd_off[pk * B.nb + C.b_out];
-          const long om_off = fwd ? B.Fd_off[pk * B.nb + b_mu] : B.F_off[pk * B.nb + b_mu];
-          const double hs = fwd ? 1.0 : -1.0;
-          int qs = 0;
-          for (int i = 0; i < n; ++i)
-            if (B.set_to_orb[pk * n + i] >= 0) qs = i + 1;
-          const int pout = r * dvp * d0, pmid = r * dv * d0;
-          for (int idx = lane; idx < nb_items * pout; idx += 32) {
-            int j = idx / pout;
-            X[(size_t)j * slab + (idx - j * pout)] = 0.0;
-          }
-          __syncwarp();
-          for (int mu = 0; mu < qs; ++mu) {
-            const int om = B.set_to_orb[pk * n + mu];
-            for (int idx = lane; idx < nb_items * pmid; idx += 32) {
-              int j = idx / pmid;
-              int rem = idx - j * pmid;
-              int t = rem / (dv * d0);
-              int r2 = rem - t * dv * d0;
-              int x = r2 / d0, z = r2 - x * d0;
-              const double *Tt = T + (size_t)j * slab + t * dv * d1;
-              double a = 0.0;
-              for (int kap = 0; kap < qs; ++kap) {
-                const int ok = B.set_to_orb[pk * n + kap];
-                double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
-                if (h == 0.0) continue;
-                const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0;
-                double tf = 0.0;
-                for (int y = 0; y < d1; ++y) tf = fmad(Tt[x * d1 + y], Fk[y * d0 + z], tf);
-                a = fmad(mul(hs, h), tf, a);
-              }
-              Y[(size_t)j * slab + rem] = a;
-            }
-            __syncwarp();
-            const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
-            for (int idx = lane; idx < nb_items * pout; idx += 32) {
-              int j = idx / pout;
-              int rem = idx - j * pout;
-              int t = rem / (dvp * d0);
-              int r2 = rem - t * dvp * d0;
-              int x = r2 / d0, z = r2 - x * d0;
-              const double *Yt = Y + (size_t)j * slab + t * dv * d0;
-              double a = 0.0;
-              for (int y = 0; y < dv; ++y) a = fmad(Fm[x * dv + y], Yt[y * d0 + z], a);
-              X[(size_t)j * slab + rem] = add(X[(size_t)j * slab + rem], a);
-            }
-            __syncwarp();
-          }
-          double *tmp = T; T = X; X = tmp;
-        }
-      }
-      // ---- prefactor and signs, the |T| > 1e-16 guard, accumulation in item order
-      const int tot = r * dout * d0;
-      for (int j = 0; j < nb_items; ++j) {
-        const double sc = ist[j].scale;
-        double mx = 0.0;
-        for (int i = lane; i < tot; i += 32) mx = fmax(mx, fabs(mul(T[(size_t)j * slab + i], sc)));
-        mx = warp_max(mx);
-        if (lane == 0) ist[j].keep = mx > 1e-16;
-      }
-      __syncwarp();
-      for (int i = lane; i < tot; i += 32) {
-        double a = acc[i];
-        for (int j = 0; j < nb_items; ++j)
-          if (ist[j].keep) a = add(a, mul(T[(size_t)j * slab + i], ist[j].scale));
-        acc[i] = a;
-      }
-      for (int j = 0; j < nb_items; ++j) any = any || ist[j].keep;
-      __syncwarp();
-    }
-    if (any) {
-      double *dst = Sigma + B.goff[C.b_out];
-      for (int i = lane; i < r * dout * d0; i += 32) atomicAdd(dst + i, mul(scale, acc[i]));
-    }
-    __syncwarp();
-  }
-}
-
+// -------------------------------------------------------------------------------- small kernels
 __global__ void block_maxabs_kernel(const double *G, const long *goff, const int *dims, int r, int nb, double *out) {
   int b = blockIdx.x;
   if (b >= nb) return;
@@ -565,7 +165,8 @@ struct Ctx {
   DevBuf<double> d_RFp, d_corr_scratch;
   DevBuf<long> d_mu_off, d_ka_off;
   std::map<std::string, std::unique_ptr<ClassSet>> noalloc_classes;  // host-only work lists of the allocation-free call
-  int unit_batches = 4;  // lockstep batches per work unit
+  int unit_batches = 4;  // panel batches per work unit
+  std::map<int, std::pair<int, std::unique_ptr<DevBuf<int2>>>> chunk_bufs;  // edge-table panel chunks per signature count
   // profiling: CUDA events around every Sigma launch (enabled on request), user events, L2 flush buffer
   bool profile = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
@@ -618,6 +219,7 @@ static void setup_basis(Ctx *c, double beta, double lambda, double eps, int r, c
   if (r > 64) throw Error(XCA_ERR_UNSUPPORTED, "DLR rank " + std::to_string(r) + " above 64 is not supported by the device kernels");
   c->basis_ready = false;
   c->dyson_ready = false;
+  c->chunk_bufs.clear();
   c->r = r; c->nb = n_blocks; c->beta = beta; c->lam = lambda; c->eps = eps;
   c->rf.assign(rf, rf + r);
   c->it.assign(it, it + r);
@@ -685,6 +287,23 @@ static long ipow(long a, int e) {
 // Validity of a block path depends on the directions, the orbital tuple, the output block, the
 // symmetry set and the zero-block flags of G, never on the pole tuple, so it is enumerated once per
 // (topology, zero pattern) and every valid path class stands for p^(m-1) items.
+static int panel_nc_host(int RP) { return RP == 32 ? panel_nc<32>() : (RP == 48 ? panel_nc<48>() : panel_nc<64>()); }
+
+static size_t panel_smem_bytes(int RP) {
+  return (RP == 32 ? panel_smem_doubles<32>() : (RP == 48 ? panel_smem_doubles<48>() : panel_smem_doubles<64>())) * sizeof(double);
+}
+
+// (block, first column) chunks of the edge-table panels for `nsig` signatures per block.
+static std::vector<int2> table_chunks(const Ctx *c, int nsig) {
+  const int nc = panel_nc_host(c->RP);
+  std::vector<int2> ch;
+  for (int b = 0; b < c->nb; ++b) {
+    const long total = (long)nsig * c->dims[b] * c->dims[b];
+    for (long q = 0; q < total; q += nc) ch.push_back(make_int2(b, (int)q));
+  }
+  return ch;
+}
+
 static std::string class_key(const Topology &T, const std::vector<int> &zero) {
   std::ostringstream key;
   key << T.m;
@@ -768,7 +387,11 @@ static std::unique_ptr<ClassSet> build_classes(Ctx *c, const Topology &T, const 
             int mxb = 0;
             for (int i = 1; i <= nv; ++i) mxb = std::max(mxb, bd[i]);
             R.dcmax = mxb * std::max(bd[0], bd[1]);
-            R.batch = std::max(1, 32 / R.dcmax);
+            const int nc = panel_nc_host(c->RP);
+            if (R.dcmax > nc)
+              throw Error(XCA_ERR_UNSUPPORTED, "block chain too wide for the panel kernel (" + std::to_string(R.dcmax) +
+                                                   " entries per item, panel width " + std::to_string(nc) + ")");
+            R.batch = std::min(PANEL_BMAX, nc / R.dcmax);
           }
           for (int v = 0; v < nv; ++v) {
             R.vline[v] = vline[v];
@@ -807,65 +430,61 @@ static ClassSet *get_classes(Ctx *c, const Topology &T, const std::vector<int> &
   return ret;
 }
 
-static size_t sigma_warp_doubles(const Ctx *c) {
-  size_t items_bytes = ((sizeof(ItemState) * 32 + 15) / 16) * 16;
-  return items_bytes / 8 + (size_t)NSLAB * c->region + (size_t)c->r * c->nmax * c->nmax;
-}
-
-static size_t sigma_smem_bytes(const Ctx *c, int warps) {
-  size_t base = (size_t)3 * c->RP * c->RP + (c->RP + 1) / 2;
-  return (base + sigma_warp_doubles(c) * warps) * sizeof(double);
-}
-
-static int sigma_warps(const Ctx *c) {
-  int maxsm = 0;
-  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
-  int w = WARPS_MAX;
-  while (w > 1 && sigma_smem_bytes(c, w) > (size_t)maxsm) --w;
-  if (sigma_smem_bytes(c, w) > (size_t)maxsm)
-    throw Error(XCA_ERR_UNSUPPORTED, "block dimension too large for the shared-memory Sigma kernel (nmax = " + std::to_string(c->nmax) + ")");
-  return w;
-}
-
 template <int RP>
-static void launch_tables_rp(Ctx *c, const double *G_dev, int nsig) {
-  long pairs = (long)c->nb * nsig;
-  size_t smem = (2 * (size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
-  CUDA_CHECK(cudaFuncSetAttribute(edge_table_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+static void launch_tables_rp(Ctx *c, const double *G_dev, int nsig, const int2 *d_chunks, int n_chunks, const DevBasis &B) {
+  const size_t smem = panel_smem_doubles<RP>() * sizeof(double);
+  CUDA_CHECK(cudaFuncSetAttribute(edge_tables_panel_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  long blocks = std::min<long>((pairs + 3) / 4, (long)nsm * 16);
-  edge_table_kernel<RP><<<(int)std::max<long>(1, blocks), 128, smem, c->stream>>>(c->basis(nsig), G_dev, pairs);
+  const int grid = std::max(1, std::min(n_chunks, nsm));
+  edge_tables_panel_kernel<RP><<<grid, PANEL_THREADS, smem, c->stream>>>(B, G_dev, d_chunks, n_chunks);
   c->launches++;
   CUDA_CHECK(cudaGetLastError());
+}
+
+static void launch_tables(Ctx *c, const double *G_dev, int nsig, const int2 *d_chunks, int n_chunks, const DevBasis &B) {
+  switch (c->RP) {
+    case 32: launch_tables_rp<32>(c, G_dev, nsig, d_chunks, n_chunks, B); break;
+    case 48: launch_tables_rp<48>(c, G_dev, nsig, d_chunks, n_chunks, B); break;
+    default: launch_tables_rp<64>(c, G_dev, nsig, d_chunks, n_chunks, B); break;
+  }
 }
 
 // Edge tables of the current G for every signature an order-m topology can use.
 static int prepare_tables(Ctx *c, const double *G_dev, int m) {
-  int nsig = (m >= 3) ? (int)c->nsig_alloc : 1 + 2 * c->p;
-  switch (c->RP) {
-    case 32: launch_tables_rp<32>(c, G_dev, nsig); break;
-    case 48: launch_tables_rp<48>(c, G_dev, nsig); break;
-    default: launch_tables_rp<64>(c, G_dev, nsig); break;
+  const int nsig = (m >= 3) ? (int)c->nsig_alloc : 1 + 2 * c->p;
+  auto it = c->chunk_bufs.find(nsig);
+  if (it == c->chunk_bufs.end()) {
+    const auto ch = table_chunks(c, nsig);
+    auto buf = std::make_unique<DevBuf<int2>>();
+    buf->upload(ch, c->stream);
+    it = c->chunk_bufs.emplace(nsig, std::make_pair((int)ch.size(), std::move(buf))).first;
   }
+  launch_tables(c, G_dev, nsig, it->second.second->ptr, it->second.first, c->basis(nsig));
   return nsig;
 }
 
 template <int RP>
-static void launch_sigma_rp(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_dev, double scale, int nsig) {
-  int warps = sigma_warps(c);
-  size_t smem = sigma_smem_bytes(c, warps);
-  CUDA_CHECK(cudaFuncSetAttribute(sigma_items_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  c->d_counter.resize(1);
-  CUDA_CHECK(cudaMemsetAsync(c->d_counter.ptr, 0, sizeof(int), c->stream));
+static void launch_sigma_rp(Ctx *c, const DevBasis &B, const ClassRec *d_classes, const WorkUnit *d_units, int n_units, int *counter,
+                            const double *G_dev, double *Sig_dev, double scale) {
+  const size_t smem = panel_smem_doubles<RP>() * sizeof(double);
+  CUDA_CHECK(cudaFuncSetAttribute(sigma_panel_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  int grid = std::max(1, std::min<int>(nsm, (int)((cs->units.size() + warps - 1) / warps)));
-  sigma_items_kernel<RP><<<grid, 32 * warps, smem, c->stream>>>(c->basis(nsig), cs->d_classes.ptr, cs->d_units.ptr,
-                                                                (int)cs->units.size(), c->d_counter.ptr, G_dev, Sig_dev, scale,
-                                                                c->nmax);
+  const int grid = std::max(1, std::min(nsm, n_units));
+  sigma_panel_kernel<RP><<<grid, PANEL_THREADS, smem, c->stream>>>(B, d_classes, d_units, n_units, counter, G_dev, Sig_dev, scale);
   c->launches++;
   CUDA_CHECK(cudaGetLastError());
+}
+
+static void launch_sigma_units(Ctx *c, const DevBasis &B, const ClassRec *d_classes, const WorkUnit *d_units, int n_units, int *counter,
+                               const double *G_dev, double *Sig_dev, double scale) {
+  switch (c->RP) {
+    case 32: launch_sigma_rp<32>(c, B, d_classes, d_units, n_units, counter, G_dev, Sig_dev, scale); break;
+    case 48: launch_sigma_rp<48>(c, B, d_classes, d_units, n_units, counter, G_dev, Sig_dev, scale); break;
+    default: launch_sigma_rp<64>(c, B, d_classes, d_units, n_units, counter, G_dev, Sig_dev, scale); break;
+  }
 }
 
 static std::vector<int> zero_flags_device(Ctx *c, const double *G_dev) {
@@ -889,11 +508,9 @@ static void launch_sigma(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_
     CUDA_CHECK(cudaEventCreate(&e1));
     CUDA_CHECK(cudaEventRecord(e0, c->stream));
   }
-  switch (c->RP) {
-    case 32: launch_sigma_rp<32>(c, cs, G_dev, Sig_dev, scale, nsig); break;
-    case 48: launch_sigma_rp<48>(c, cs, G_dev, Sig_dev, scale, nsig); break;
-    default: launch_sigma_rp<64>(c, cs, G_dev, Sig_dev, scale, nsig); break;
-  }
+  c->d_counter.resize(1);
+  launch_sigma_units(c, c->basis(nsig), cs->d_classes.ptr, cs->d_units.ptr, (int)cs->units.size(), c->d_counter.ptr, G_dev, Sig_dev,
+                     scale);
   if (c->profile) {
     CUDA_CHECK(cudaEventRecord(e1, c->stream));
     c->prof_events.emplace_back(e0, e1);
@@ -1233,28 +850,6 @@ static void noalloc_fits(size_t need, const char *what) {
     throw Error(XCA_ERR_INVALID, std::string("xca_compute_self_energy_device_noalloc: ") + what + " need " +
                                      std::to_string(need) + " bytes of scratch, the fixed scratch array holds " +
                                      std::to_string(NOALLOC_SCRATCH_BYTES) + "; use xca_compute_self_energy_device");
-}
-
-template <int RP>
-static void launch_noalloc_rp(Ctx *c, const DevBasis &B, long pairs, const ClassRec *classes, const WorkUnit *units,
-                              int n_units, int *counter, const double *G_dev, double *Sig_dev, double scale) {
-  int nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  size_t tsm = (2 * (size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
-  CUDA_CHECK(cudaFuncSetAttribute(edge_table_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
-  long tblocks = std::min<long>((pairs + 3) / 4, (long)nsm * 16);
-  edge_table_kernel<RP><<<(int)std::max<long>(1, tblocks), 128, tsm, c->stream>>>(B, G_dev, pairs);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
-  if (n_units == 0) return;
-  int warps = sigma_warps(c);
-  size_t smem = sigma_smem_bytes(c, warps);
-  CUDA_CHECK(cudaFuncSetAttribute(sigma_items_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int grid = std::max(1, std::min<int>(nsm, (n_units + warps - 1) / warps));
-  sigma_items_kernel<RP><<<grid, 32 * warps, smem, c->stream>>>(B, classes, units, n_units, counter, G_dev, Sig_dev, scale,
-                                                                c->nmax);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
 }
 
 }  // namespace xca
@@ -2076,11 +1671,13 @@ int xca_compute_self_energy_device_noalloc(xca_ctx *ctx, const double *G_dev, in
   unsigned char *base = noalloc_scratch(c->device);
   const int nb = c->nb, r = c->r;
   const int nsig = (m >= 3) ? (int)c->nsig_alloc : 1 + 2 * c->p;
-  // layout: unit counter | block max |G| | edge-table offsets | edge tables | path classes | work units
+  const std::vector<int2> chunks = table_chunks(c, nsig);
+  // layout: unit counter | block max |G| | edge-table offsets | table chunks | edge tables | path classes | work units
   const size_t off_counter = 0;
   const size_t off_maxabs = 256;
   const size_t off_taboff = off_maxabs + align256((size_t)nb * sizeof(double));
-  const size_t off_tab = off_taboff + align256((size_t)nb * sizeof(long));
+  const size_t off_chunks = off_taboff + align256((size_t)nb * sizeof(long));
+  const size_t off_tab = off_chunks + align256(chunks.size() * sizeof(int2));
   std::vector<long> tab_off(nb);
   long tab_doubles = 0;
   for (int b = 0; b < nb; ++b) {
@@ -2108,27 +1705,24 @@ int xca_compute_self_energy_device_noalloc(xca_ctx *ctx, const double *G_dev, in
   noalloc_fits(off_units + cs->units.size() * sizeof(WorkUnit), "the edge tables and work list of this topology");
   // contents: everything is rewritten before use except the unit counter, which must start at zero
   auto *d_tab_off = reinterpret_cast<long *>(base + off_taboff);
+  auto *d_chunks = reinterpret_cast<int2 *>(base + off_chunks);
   auto *d_classes = reinterpret_cast<ClassRec *>(base + off_classes);
   auto *d_units = reinterpret_cast<WorkUnit *>(base + off_units);
   auto *counter = reinterpret_cast<int *>(base + off_counter);
   CUDA_CHECK(cudaMemcpyAsync(d_tab_off, tab_off.data(), nb * sizeof(long), cudaMemcpyHostToDevice, c->stream));
+  CUDA_CHECK(cudaMemcpyAsync(d_chunks, chunks.data(), chunks.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
   if (!cs->classes.empty())
     CUDA_CHECK(cudaMemcpyAsync(d_classes, cs->classes.data(), cs->classes.size() * sizeof(ClassRec), cudaMemcpyHostToDevice,
                                c->stream));
   if (!cs->units.empty())
     CUDA_CHECK(cudaMemcpyAsync(d_units, cs->units.data(), cs->units.size() * sizeof(WorkUnit), cudaMemcpyHostToDevice,
                                c->stream));
-  CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
   DevBasis B = c->basis(nsig);
   B.tab = reinterpret_cast<const double *>(base + off_tab);
   B.tab_off = d_tab_off;
-  const long pairs = (long)nb * nsig;
-  const int n_units = (int)cs->units.size();
-  switch (c->RP) {
-    case 32: launch_noalloc_rp<32>(c, B, pairs, d_classes, d_units, n_units, counter, G_dev, Sigma_dev, scale); break;
-    case 48: launch_noalloc_rp<48>(c, B, pairs, d_classes, d_units, n_units, counter, G_dev, Sigma_dev, scale); break;
-    default: launch_noalloc_rp<64>(c, B, pairs, d_classes, d_units, n_units, counter, G_dev, Sigma_dev, scale); break;
-  }
+  launch_tables(c, G_dev, nsig, d_chunks, (int)chunks.size(), B);
+  if (!cs->units.empty())
+    launch_sigma_units(c, B, d_classes, d_units, (int)cs->units.size(), counter, G_dev, Sigma_dev, scale);
   API_END
 }
 
