@@ -107,6 +107,7 @@ struct Dlr {
   std::vector<double> cf2it;                 // r x r : K(t_i, om_l)
   std::vector<double> lu;                    // LU of cf2it
   std::vector<int> piv;
+  std::vector<double> dinv;                  // 1 / U_kk of the LU factors
   std::vector<double> refl;                  // r x r : K(t_i, -om_l)  (values of g(beta - tau))
   Dlr(int r_, const double *rf_, const double *it_) : r(r_), rf(rf_, rf_ + r_), it(it_, it_ + r_) {
     tabs.resize(r); k0.resize(r); k1.resize(r);
@@ -120,11 +121,29 @@ struct Dlr {
       }
     lu = cf2it;
     lu_factor(lu, r, piv);
+    dinv.resize(r);
+    for (int k = 0; k < r; ++k) dinv[k] = 1.0 / lu[(size_t)k * r + k];
   }
   // cppdlr imtime_ops::vals2coefs: coefficients c with sum_l K(t_i, om_l) c_l = g(t_i).
+  // The substitution applies the upper factor's diagonal through its reciprocals (b_k <- b_k * (1 / U_kk)),
+  // as BLAS triangular solves with an inverted packed diagonal do.
   void vals2coefs(const cd *vals, long ncol, cd *coefs) const {
     std::copy(vals, vals + (size_t)r * ncol, coefs);
-    lu_solve(lu, r, piv, coefs, ncol);
+    for (int k = 0; k < r; ++k)
+      if (piv[k] != k)
+        for (long j = 0; j < ncol; ++j) std::swap(coefs[(size_t)k * ncol + j], coefs[(size_t)piv[k] * ncol + j]);
+    for (int k = 0; k < r; ++k)
+      for (int i = k + 1; i < r; ++i) {
+        double f = lu[(size_t)i * r + k];
+        for (long j = 0; j < ncol; ++j) coefs[(size_t)i * ncol + j] = dfma(-f, coefs[(size_t)k * ncol + j], coefs[(size_t)i * ncol + j]);
+      }
+    for (int k = r - 1; k >= 0; --k) {
+      for (long j = 0; j < ncol; ++j) coefs[(size_t)k * ncol + j] *= dinv[k];
+      for (int i = 0; i < k; ++i) {
+        double f = lu[(size_t)i * r + k];
+        for (long j = 0; j < ncol; ++j) coefs[(size_t)i * ncol + j] = dfma(-f, coefs[(size_t)k * ncol + j], coefs[(size_t)i * ncol + j]);
+      }
+    }
   }
   void coefs2vals(const cd *coefs, long ncol, cd *vals) const {
     for (int i = 0; i < r; ++i)

@@ -148,11 +148,20 @@ inline void lu_factor(std::vector<double> &a, int n, std::vector<int> &piv) {
   }
 }
 
-// Solve A X = B in place (B is n x nrhs, row-major) with the factors of lu_factor, in the column order
-// of the reference BLAS dtrsm that LAPACK getrs calls: row interchanges; forward, for k ascending,
-// b_i -= L_ik b_k (i > k); backward, for k descending, b_k /= U_kk then b_i -= U_ik b_k (i < k); every
-// update is one fused multiply-add.
-inline void lu_solve(const std::vector<double> &lu, int n, const std::vector<int> &piv, double *b, long nrhs) {
+// Reciprocals 1 / U_kk of the upper factor's diagonal (each one correctly rounded division).
+inline std::vector<double> lu_diag_reciprocals(const std::vector<double> &lu, int n) {
+  std::vector<double> d(n);
+  for (int k = 0; k < n; ++k) d[k] = 1.0 / lu[(size_t)k * n + k];
+  return d;
+}
+
+// Solve A X = B in place (B is n x nrhs, row-major) with the factors of lu_factor, in the column order of
+// the reference BLAS dtrsm that LAPACK getrs calls: row interchanges; forward, for k ascending,
+// b_i -= L_ik b_k (i > k); backward, for k descending, b_k *= 1 / U_kk (the diagonal's precomputed
+// reciprocal, as BLAS triangular solves with an inverted packed diagonal do), then b_i -= U_ik b_k
+// (i < k); every update one fused multiply-add.  The operation order of the device's DLR transforms.
+inline void lu_solve_recip(const std::vector<double> &lu, const std::vector<double> &dinv, int n, const std::vector<int> &piv, double *b,
+                           long nrhs) {
   for (int k = 0; k < n; ++k)
     if (piv[k] != k)
       for (long j = 0; j < nrhs; ++j) std::swap(b[(size_t)k * nrhs + j], b[(size_t)piv[k] * nrhs + j]);
@@ -162,8 +171,7 @@ inline void lu_solve(const std::vector<double> &lu, int n, const std::vector<int
       for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] = std::fma(-f, b[(size_t)k * nrhs + j], b[(size_t)i * nrhs + j]);
     }
   for (int k = n - 1; k >= 0; --k) {
-    double d = lu[(size_t)k * n + k];
-    for (long j = 0; j < nrhs; ++j) b[(size_t)k * nrhs + j] /= d;
+    for (long j = 0; j < nrhs; ++j) b[(size_t)k * nrhs + j] *= dinv[k];
     for (int i = 0; i < k; ++i) {
       double f = lu[(size_t)i * n + k];
       for (long j = 0; j < nrhs; ++j) b[(size_t)i * nrhs + j] = std::fma(-f, b[(size_t)k * nrhs + j], b[(size_t)i * nrhs + j]);

@@ -74,13 +74,12 @@ __device__ __forceinline__ void matvec_sep_reg(const double *__restrict__ MT, co
   }
 }
 
-// Stage the padded LU and W into shared memory (2 RP^2 doubles) and the pivot gather (RP ints).
+// Stage the padded LU (with its reciprocal diagonal) and W into shared memory (2 RP^2 + RP doubles) and
+// the pivot gather (RP ints).
 template <int RP>
 __device__ __forceinline__ void stage_lu_w(const DysonBasis &B, double *sLU, double *sW, int *sPerm) {
-  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
-    sLU[i] = B.LUp[i];
-    sW[i] = B.Wp[i];
-  }
+  for (int i = threadIdx.x; i < RP * RP + RP; i += blockDim.x) sLU[i] = B.LUp[i];
+  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) sW[i] = B.Wp[i];
   for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
   __syncthreads();
 }
@@ -114,7 +113,7 @@ template <int RP>
 __global__ void __launch_bounds__(256) dyson_coef_kernel(DysonBasis B, const double *__restrict__ Sigma, double eta) {
   extern __shared__ double smem[];
   double *sLU = smem;
-  double *sW = sLU + RP * RP;
+  double *sW = sLU + RP * RP + RP;
   int *sPerm = reinterpret_cast<int *>(sW + RP * RP);
   const int b = blockIdx.x;
   if (b >= B.nb) return;
@@ -314,10 +313,10 @@ template <int RP>
 __global__ void __launch_bounds__(128) trace_beta_kernel(DysonBasis B, const double *__restrict__ G, double *__restrict__ out) {
   extern __shared__ double smem[];
   double *sLU = smem;
-  int *sPerm = reinterpret_cast<int *>(sLU + RP * RP);
+  int *sPerm = reinterpret_cast<int *>(sLU + RP * RP + RP);
   __shared__ double part[128];
   const int b = blockIdx.x;
-  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) sLU[i] = B.LUp[i];
+  for (int i = threadIdx.x; i < RP * RP + RP; i += blockDim.x) sLU[i] = B.LUp[i];
   for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
   __syncthreads();
   const int r = B.r, d = B.dims[b], dd = d * d;

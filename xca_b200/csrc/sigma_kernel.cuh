@@ -31,7 +31,8 @@ constexpr int WARPS_MAX = 8;
 struct DevBasis {
   int r, p, n, nb, nq, region;  // region: doubles per slab region of a warp, r * max(32, largest dcmax)
   double beta;
-  const double *LUp;    // RP x RP padded LU of K(t_i, om_l), column-major: unit L below the diagonal, U on and above; pad: U_kk = 1
+  const double *LUp;    // RP x RP padded LU of K(t_i, om_l), column-major: unit L below the diagonal, U on and above
+                        // (pad: U_kk = 1), followed by the RP reciprocals 1 / U_kk
   const int *perm;      // RP: row gathered into position i by the pivoting (-1 beyond r)
   const double *Wp;     // RP x RP column-major: W[l][k] = K(0, om_k) / (om_k - om_l), 0 on the diagonal and in the pad
   const double *BKp;    // RP x RP column-major: beta * K(t_i, om_l), 0 in the pad
@@ -95,20 +96,37 @@ __device__ __forceinline__ double warp_max(double v) {
 }
 
 // x <- K^{-1} x for one register-resident column (already gathered through the pivoting): forward
-// unit-lower then backward upper substitution in dtrsm column order.  LUT is the LU factor stored
-// column-major (LUT[k * RP + i] = LU[i][k]).  Padding rows stay zero.
+// unit-lower then backward upper substitution in dtrsm column order, the upper factor's diagonal applied
+// as a multiplication by its precomputed reciprocal (x_k <- x_k * (1 / U_kk), as BLAS triangular solves
+// with an inverted packed diagonal do).  LUT is the LU factor stored column-major (LUT[k * RP + i] =
+// LU[i][k]) followed by the RP reciprocals (LUT[RP * RP + k] = 1 / U_kk; 1 in the pad).  Operand pairs
+// at even offsets are loaded together.  Padding rows stay zero.
 template <int RP>
 __device__ __forceinline__ void lu_solve_reg(const double *__restrict__ LUT, double (&x)[RP]) {
 #pragma unroll
   for (int k = 0; k < RP; ++k) {
+    const double xk = x[k];
+    const double *col = LUT + k * RP;
+    if ((k + 1) < RP && ((k + 1) & 1)) x[k + 1] = fmad(-col[k + 1], xk, x[k + 1]);
 #pragma unroll
-    for (int i = k + 1; i < RP; ++i) x[i] = fmad(-LUT[k * RP + i], x[k], x[i]);
+    for (int i = (k + 2) & ~1; i + 1 < RP; i += 2) {
+      const double2 l = *reinterpret_cast<const double2 *>(col + i);
+      x[i] = fmad(-l.x, xk, x[i]);
+      x[i + 1] = fmad(-l.y, xk, x[i + 1]);
+    }
   }
 #pragma unroll
   for (int k = RP - 1; k >= 0; --k) {
-    x[k] = __ddiv_rn(x[k], LUT[k * RP + k]);
+    x[k] = mul(x[k], LUT[RP * RP + k]);
+    const double xk = x[k];
+    const double *col = LUT + k * RP;
 #pragma unroll
-    for (int i = 0; i < k; ++i) x[i] = fmad(-LUT[k * RP + i], x[k], x[i]);
+    for (int i = 0; i + 1 < k; i += 2) {
+      const double2 l = *reinterpret_cast<const double2 *>(col + i);
+      x[i] = fmad(-l.x, xk, x[i]);
+      x[i + 1] = fmad(-l.y, xk, x[i + 1]);
+    }
+    if (k & 1) x[k - 1] = fmad(-col[k - 1], xk, x[k - 1]);
   }
 }
 

@@ -35,12 +35,14 @@ __host__ __device__ constexpr int panel_nc() { return PanelCfg<RP>::NC; }
 // Dynamic shared memory of the panel kernels, in doubles.
 template <int RP>
 __host__ __device__ constexpr size_t panel_smem_doubles() {
-  return 3 * (size_t)RP * RP + 3 * (size_t)RP * PanelCfg<RP>::NC + (sizeof(ItemState) * PANEL_BMAX + 7) / 8 + (RP + 1) / 2;
+  return 3 * (size_t)RP * RP + RP + 3 * (size_t)RP * PanelCfg<RP>::NC + (sizeof(ItemState) * PANEL_BMAX + 7) / 8 + (RP + 1) / 2;
 }
 
 // Y[i][c] = sum_{k < r} M[i][k] X[k][c] for i < r, c < ncols (M column-major RP x RP; X, Y panels with row
-// stride NC).  EPI: Y[i][c] = fma(t_i, (M X)[i][c], H1[i][c]).  Each thread owns a TR x TC tile; the
-// threads of a warp share the row tile, so the M operands are broadcasts.
+// stride NC).  EPI: Y[i][c] = fma(t_i, (M X)[i][c], H1[i][c]).  Each thread owns TR rows x TC columns: the
+// column pairs 2 (ct + q CT) .. + 1 (q < TC / 2), so that the lanes of a warp read consecutive 16-byte
+// pairs of a panel row (no bank conflict); the threads of a warp share the row tile, so the M operands are
+// broadcasts.
 template <int RP, bool EPI>
 __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const double *__restrict__ X, double *__restrict__ Y, int r,
                                            int ncols, const double *__restrict__ tabs, const double *__restrict__ H1) {
@@ -48,8 +50,8 @@ __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const 
   constexpr int CT = NC / TC;
   static_assert((RP / TR) * CT == PANEL_THREADS, "panel tiling must cover the CTA");
   const int rt = threadIdx.x / CT, ct = threadIdx.x - rt * CT;
-  const int i0 = rt * TR, c0 = ct * TC;
-  if (i0 >= r || c0 >= ncols) return;
+  const int i0 = rt * TR;
+  if (i0 >= r || 2 * ct >= ncols) return;
   double acc[TR][TC];
 #pragma unroll
   for (int a = 0; a < TR; ++a)
@@ -59,7 +61,6 @@ __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const 
   for (int k = 0; k < r; ++k) {
     double mv[TR], xv[TC];
     const double2 *mp = reinterpret_cast<const double2 *>(sM + k * RP + i0);
-    const double2 *xp = reinterpret_cast<const double2 *>(X + k * NC + c0);
 #pragma unroll
     for (int a = 0; a < TR / 2; ++a) {
       const double2 t = mp[a];
@@ -67,10 +68,10 @@ __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const 
       mv[2 * a + 1] = t.y;
     }
 #pragma unroll
-    for (int b = 0; b < TC / 2; ++b) {
-      const double2 t = xp[b];
-      xv[2 * b] = t.x;
-      xv[2 * b + 1] = t.y;
+    for (int q = 0; q < TC / 2; ++q) {
+      const double2 t = *reinterpret_cast<const double2 *>(X + k * NC + 2 * (ct + q * CT));
+      xv[2 * q] = t.x;
+      xv[2 * q + 1] = t.y;
     }
 #pragma unroll
     for (int a = 0; a < TR; ++a)
@@ -83,7 +84,7 @@ __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const 
     if (i >= r) break;
 #pragma unroll
     for (int b = 0; b < TC; ++b) {
-      const int c = c0 + b;
+      const int c = 2 * (ct + (b / 2) * CT) + (b & 1);
       if (c < ncols) Y[i * NC + c] = EPI ? fmad(tabs[i], acc[a][b], H1[i * NC + c]) : acc[a][b];
     }
   }
@@ -111,8 +112,8 @@ __device__ __forceinline__ void panel_lu_solve(const double *__restrict__ sLU, c
 
 template <int RP>
 __device__ __forceinline__ void stage_basis(const DevBasis &B, double *sLU, double *sW, double *sBK, int *sPerm) {
+  for (int i = threadIdx.x; i < RP * RP + RP; i += blockDim.x) sLU[i] = B.LUp[i];
   for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
-    sLU[i] = B.LUp[i];
     sW[i] = B.Wp[i];
     sBK[i] = B.BKp[i];
   }
@@ -128,7 +129,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(Dev
                                                                               const int2 *__restrict__ chunks, int n_chunks) {
   constexpr int NC = PanelCfg<RP>::NC;
   extern __shared__ double smem[];
-  double *sLU = smem, *sW = sLU + RP * RP, *sBK = sW + RP * RP;
+  double *sLU = smem, *sW = sLU + RP * RP + RP, *sBK = sW + RP * RP;
   double *PA = sBK + RP * RP, *PB = PA + RP * NC;
   int *sPerm = reinterpret_cast<int *>(PB + RP * NC);
   stage_basis<RP>(B, sLU, sW, sBK, sPerm);
@@ -179,7 +180,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(Dev
   }
 }
 
-// Dynamic shared memory: LU | W | BK (3 RP^2, column-major) | panels A, B, C (RP x NC each) | item states
+// Dynamic shared memory: LU (+ reciprocal diagonal) | W | BK (column-major) | panels A, B, C (RP x NC each) | item states
 // (PANEL_BMAX) | perm (RP ints).
 template <int RP>
 __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis B, const ClassRec *__restrict__ classes,
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
                                                                         double *__restrict__ Sigma, double scale) {
   constexpr int NC = PanelCfg<RP>::NC;
   extern __shared__ double smem[];
-  double *sLU = smem, *sW = sLU + RP * RP, *sBK = sW + RP * RP;
+  double *sLU = smem, *sW = sLU + RP * RP + RP, *sBK = sW + RP * RP;
   double *PA = sBK + RP * RP, *PB = PA + RP * NC, *PC = PB + RP * NC;
   ItemState *ist = reinterpret_cast<ItemState *>(PC + RP * NC);
   int *sPerm = reinterpret_cast<int *>(reinterpret_cast<double *>(ist) + (sizeof(ItemState) * PANEL_BMAX + 7) / 8);

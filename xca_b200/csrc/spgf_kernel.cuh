@@ -205,7 +205,7 @@ __device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, 
   __syncwarp();
 }
 
-// Dynamic shared memory: LU | W | BK | RF (4 RP^2 doubles, column-major) | perm (RP ints).
+// Dynamic shared memory: LU (+ reciprocal diagonal) | W | BK | RF (column-major) | perm (RP ints).
 // Per-warp global scratch (`warp_doubles` each): T | X | Y (r * nmax^2 each), right chains and left chains
 // (nb slots of r * nmax^2 each), accumulator (r * n * n).
 template <int RP>
@@ -215,10 +215,10 @@ __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis C
                                                          const double *__restrict__ G, double *__restrict__ gout, double scale,
                                                          int nmax, double *__restrict__ scratch, long warp_doubles) {
   extern __shared__ double smem[];
-  double *sLU = smem, *sW = sLU + RP * RP, *sBK = sW + RP * RP, *sRF = sBK + RP * RP;
+  double *sLU = smem, *sW = sLU + RP * RP + RP, *sBK = sW + RP * RP, *sRF = sBK + RP * RP;
   int *sPerm = reinterpret_cast<int *>(sRF + RP * RP);
+  for (int i = threadIdx.x; i < RP * RP + RP; i += blockDim.x) sLU[i] = B.LUp[i];
   for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
-    sLU[i] = B.LUp[i];
     sW[i] = B.Wp[i];
     sBK[i] = B.BKp[i];
     sRF[i] = CB.RFp[i];

@@ -142,7 +142,7 @@ struct Ctx {
   std::vector<long> F_off, Fd_off, Fb_off, Fdb_off;
   std::vector<double> ops;
   std::vector<double> hval, hrefl, kitp, kitm, k0p, k0m, kpow;
-  std::vector<double> LU, W, Kit;
+  std::vector<double> LU, W, Kit, Kdinv;     // Kdinv: 1 / U_kk of K's LU factors
   std::vector<int> piv;
   int RP = 0;                                   // padded rank of the register-resident columns
   std::vector<double> LUp, Wp, BKp;             // RP x RP padded matrices
@@ -244,9 +244,11 @@ static void setup_basis(Ctx *c, double beta, double lambda, double eps, int r, c
       if (k != l) c->W[(size_t)l * r + k] = c->k0[k] / (rf[k] - rf[l]);
   c->LU = c->Kit;
   lu_factor(c->LU, r, c->piv);
+  c->Kdinv = lu_diag_reciprocals(c->LU, r);
   c->RP = r <= 32 ? 32 : (r <= 48 ? 48 : 64);
   const int RP = c->RP;
-  c->LUp.assign((size_t)RP * RP, 0.0); c->Wp.assign((size_t)RP * RP, 0.0); c->BKp.assign((size_t)RP * RP, 0.0);
+  c->LUp.assign((size_t)RP * RP + RP, 0.0); c->Wp.assign((size_t)RP * RP, 0.0); c->BKp.assign((size_t)RP * RP, 0.0);
+  for (int k = 0; k < RP; ++k) c->LUp[(size_t)RP * RP + k] = k < r ? c->Kdinv[k] : 1.0;
   for (int i = 0; i < RP; ++i)
     for (int k = 0; k < RP; ++k) {
       // column-major: element (row i, column k) at k * RP + i
@@ -704,7 +706,7 @@ template <int RP>
 static void launch_corr_rp(Ctx *c, CorrSet *cs, const WorkUnit *d_units, int n_units, const double *G_dev, double *g_dev,
                            double scale, int nsig) {
   if (n_units == 0) return;
-  const size_t sm = (4 * (size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
+  const size_t sm = (4 * (size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
   CUDA_CHECK(cudaFuncSetAttribute(correlator_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
@@ -759,7 +761,7 @@ static void require_dyson(const Ctx *c) {
 template <int RP>
 static void launch_dyson_rp(Ctx *c, const double *Sig_dev, double eta, int hermitize, double *G_dev) {
   DysonBasis B = dyson_basis(c);
-  size_t sm = (2 * (size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
+  size_t sm = (2 * (size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
   CUDA_CHECK(cudaFuncSetAttribute(dyson_coef_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   dyson_coef_kernel<RP><<<c->nb, 256, sm, c->stream>>>(B, Sig_dev, eta);
   c->launches++;
@@ -797,7 +799,7 @@ static void check_dyson_status(Ctx *c) {
 template <int RP>
 static double trace_beta_rp(Ctx *c, const double *G_dev) {
   DysonBasis B = dyson_basis(c);
-  size_t sm = ((size_t)RP * RP + (RP + 1) / 2) * sizeof(double);
+  size_t sm = ((size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
   CUDA_CHECK(cudaFuncSetAttribute(trace_beta_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   c->d_red.resize(std::max(c->nb, 256));
   trace_beta_kernel<RP><<<c->nb, 128, sm, c->stream>>>(B, G_dev, c->d_red.ptr);
@@ -1048,7 +1050,7 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
   {
     std::vector<double> cfs = c->hval;
     long nc = (long)n * n;
-    lu_solve(c->LU, r, c->piv, cfs.data(), nc);
+    lu_solve_recip(c->LU, c->Kdinv, r, c->piv, cfs.data(), nc);
     c->hrefl.assign((size_t)r * nc, 0.0);
     for (int i = 0; i < r; ++i)
       for (int l = 0; l < r; ++l) {
@@ -1190,7 +1192,7 @@ int xca_dyson_setup(xca_ctx *ctx, const double *G0) {
   for (int b = 0; b < c->nb; ++b) {
     const long dd = (long)c->dims[b] * c->dims[b];
     double *gc = g0c.data() + c->goff[b];
-    lu_solve(c->LU, r, c->piv, gc, dd);
+    lu_solve_recip(c->LU, c->Kdinv, r, c->piv, gc, dd);
     double *gt = g0t.data() + c->goff[b];
     for (int l = 0; l < r; ++l)
       for (int k = 0; k < r; ++k) {
