@@ -38,18 +38,34 @@ __host__ __device__ constexpr size_t panel_smem_doubles() {
   return 3 * (size_t)RP * RP + RP + 3 * (size_t)RP * PanelCfg<RP>::NC + (sizeof(ItemState) * PANEL_BMAX + 7) / 8 + (RP + 1) / 2;
 }
 
+// A thread group of NT threads working on a panel of NCG columns (row stride NCG).
+template <int RP, int G>
+struct PanelGrp {
+  static constexpr int NT = PANEL_THREADS / G, NCG = PanelCfg<RP>::NC / G;
+  static constexpr int TR = PanelCfg<RP>::TR, TC = PanelCfg<RP>::TC, CT = NCG / TC;
+  static_assert((RP / TR) * CT == NT, "panel tiling must cover the thread group");
+};
+
+// Barrier of thread group g (named barrier 1 + g of NT threads; the whole CTA when G == 1).
+template <int G>
+__device__ __forceinline__ void group_sync(int g) {
+  if (G == 1)
+    __syncthreads();
+  else
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(PANEL_THREADS / G) : "memory");
+}
+
 // Y[i][c] = sum_{k < r} M[i][k] X[k][c] for i < r, c < ncols (M column-major RP x RP; X, Y panels with row
-// stride NC).  EPI: Y[i][c] = fma(t_i, (M X)[i][c], H1[i][c]).  Each thread owns TR rows x TC columns: the
-// column pairs 2 (ct + q CT) .. + 1 (q < TC / 2), so that the lanes of a warp read consecutive 16-byte
-// pairs of a panel row (no bank conflict); the threads of a warp share the row tile, so the M operands are
-// broadcasts.
-template <int RP, bool EPI>
+// stride NCG); t is the thread's index in its group.  EPI: Y[i][c] = fma(t_i, (M X)[i][c], H1[i][c]).
+// Each thread owns TR rows x TC columns: the column pairs 2 (ct + q CT) .. + 1 (q < TC / 2), so that
+// neighbouring lanes read consecutive 16-byte pairs of a panel row (no bank conflict); lanes that share
+// a row tile read the same M operands (broadcasts).
+template <int RP, int G, bool EPI>
 __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const double *__restrict__ X, double *__restrict__ Y, int r,
-                                           int ncols, const double *__restrict__ tabs, const double *__restrict__ H1) {
-  constexpr int NC = PanelCfg<RP>::NC, TR = PanelCfg<RP>::TR, TC = PanelCfg<RP>::TC;
-  constexpr int CT = NC / TC;
-  static_assert((RP / TR) * CT == PANEL_THREADS, "panel tiling must cover the CTA");
-  const int rt = threadIdx.x / CT, ct = threadIdx.x - rt * CT;
+                                           int ncols, const double *__restrict__ tabs, const double *__restrict__ H1, int t) {
+  using P = PanelGrp<RP, G>;
+  constexpr int NCG = P::NCG, TR = P::TR, TC = P::TC, CT = P::CT;
+  const int rt = t / CT, ct = t - rt * CT;
   const int i0 = rt * TR;
   if (i0 >= r || 2 * ct >= ncols) return;
   double acc[TR][TC];
@@ -63,15 +79,15 @@ __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const 
     const double2 *mp = reinterpret_cast<const double2 *>(sM + k * RP + i0);
 #pragma unroll
     for (int a = 0; a < TR / 2; ++a) {
-      const double2 t = mp[a];
-      mv[2 * a] = t.x;
-      mv[2 * a + 1] = t.y;
+      const double2 v = mp[a];
+      mv[2 * a] = v.x;
+      mv[2 * a + 1] = v.y;
     }
 #pragma unroll
     for (int q = 0; q < TC / 2; ++q) {
-      const double2 t = *reinterpret_cast<const double2 *>(X + k * NC + 2 * (ct + q * CT));
-      xv[2 * q] = t.x;
-      xv[2 * q + 1] = t.y;
+      const double2 v = *reinterpret_cast<const double2 *>(X + k * NCG + 2 * (ct + q * CT));
+      xv[2 * q] = v.x;
+      xv[2 * q + 1] = v.y;
     }
 #pragma unroll
     for (int a = 0; a < TR; ++a)
@@ -85,28 +101,27 @@ __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const 
 #pragma unroll
     for (int b = 0; b < TC; ++b) {
       const int c = 2 * (ct + (b / 2) * CT) + (b & 1);
-      if (c < ncols) Y[i * NC + c] = EPI ? fmad(tabs[i], acc[a][b], H1[i * NC + c]) : acc[a][b];
+      if (c < ncols) Y[i * NCG + c] = EPI ? fmad(tabs[i], acc[a][b], H1[i * NCG + c]) : acc[a][b];
     }
   }
 }
 
-// P[:, c] <- K^-1 P[:, c] for c < ncols, one column per thread (gathered through the pivots, LU
-// substitution in registers, written back in place).
-template <int RP>
-__device__ __forceinline__ void panel_lu_solve(const double *__restrict__ sLU, const int *__restrict__ sPerm, double *P, int r,
-                                               int ncols) {
-  constexpr int NC = PanelCfg<RP>::NC;
-  for (int c = threadIdx.x; c < ncols; c += PANEL_THREADS) {
+// P[:, c] <- K^-1 P[:, c] for c < ncols (row stride NCG), one column per thread of the group (gathered
+// through the pivots, LU substitution in registers, written back in place).
+template <int RP, int NCG, int NT>
+__device__ __forceinline__ void panel_lu_solve(const double *__restrict__ sLU, const int *__restrict__ sPerm, double *P, int r, int ncols,
+                                               int t) {
+  for (int c = t; c < ncols; c += NT) {
     double x[RP];
 #pragma unroll
     for (int i = 0; i < RP; ++i) {
       const int s = sPerm[i];
-      x[i] = s >= 0 ? P[s * NC + c] : 0.0;
+      x[i] = s >= 0 ? P[s * NCG + c] : 0.0;
     }
     lu_solve_reg<RP>(sLU, x);
 #pragma unroll
     for (int i = 0; i < RP; ++i)
-      if (i < r) P[i * NC + c] = x[i];
+      if (i < r) P[i * NCG + c] = x[i];
   }
 }
 
@@ -163,9 +178,9 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(Dev
       PA[t * NC + c] = v;
     }
     __syncthreads();
-    panel_lu_solve<RP>(sLU, sPerm, PA, r, ncols);
+    panel_lu_solve<RP, NC, PANEL_THREADS>(sLU, sPerm, PA, r, ncols, threadIdx.x);
     __syncthreads();
-    panel_gemm<RP, false>(sW, PA, PB, r, ncols, nullptr, nullptr);
+    panel_gemm<RP, 1, false>(sW, PA, PB, r, ncols, nullptr, nullptr, threadIdx.x);
     __syncthreads();
     double *out = const_cast<double *>(B.tab) + B.tab_off[b];
     for (int idx = threadIdx.x; idx < r * ncols; idx += PANEL_THREADS) {
@@ -180,29 +195,35 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(Dev
   }
 }
 
-// Dynamic shared memory: LU (+ reciprocal diagonal) | W | BK (column-major) | panels A, B, C (RP x NC each) | item states
-// (PANEL_BMAX) | perm (RP ints).
-template <int RP>
+// Dynamic shared memory: LU (+ reciprocal diagonal) | W | BK (column-major) | per thread group: panels A, B,
+// C (RP x NC / NG each) | per thread group: item states (PANEL_BMAX / NG) | perm (RP ints).  The NG thread
+// groups of the CTA run independent work loops (own units, batches and barriers) over the shared DLR
+// matrices, so that one group's substitution phase overlaps another group's products.
+template <int RP, int NG>
 __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis B, const ClassRec *__restrict__ classes,
                                                                         const WorkUnit *__restrict__ units, int n_units,
                                                                         int *__restrict__ unit_counter, const double *__restrict__ G,
                                                                         double *__restrict__ Sigma, double scale) {
-  constexpr int NC = PanelCfg<RP>::NC;
+  using GP = PanelGrp<RP, NG>;
+  constexpr int NC = GP::NCG, NT = GP::NT, BG = PANEL_BMAX / NG;
   extern __shared__ double smem[];
   double *sLU = smem, *sW = sLU + RP * RP + RP, *sBK = sW + RP * RP;
-  double *PA = sBK + RP * RP, *PB = PA + RP * NC, *PC = PB + RP * NC;
-  ItemState *ist = reinterpret_cast<ItemState *>(PC + RP * NC);
-  int *sPerm = reinterpret_cast<int *>(reinterpret_cast<double *>(ist) + (sizeof(ItemState) * PANEL_BMAX + 7) / 8);
-  __shared__ int s_unit;
-  __shared__ unsigned long long s_max[PANEL_BMAX];
+  const int g = threadIdx.x / NT, tid = threadIdx.x - g * NT;
+  double *PA = sBK + RP * RP + (size_t)g * 3 * RP * NC, *PB = PA + RP * NC, *PC = PB + RP * NC;
+  ItemState *ist = reinterpret_cast<ItemState *>(sBK + RP * RP + (size_t)3 * RP * NC * NG) + g * BG;
+  int *sPerm = reinterpret_cast<int *>(sBK + RP * RP + (size_t)3 * RP * NC * NG + (sizeof(ItemState) * PANEL_BMAX + 7) / 8);
+  __shared__ int s_unit_all[NG];
+  __shared__ unsigned long long s_max_all[PANEL_BMAX];
+  int &s_unit = s_unit_all[g];
+  unsigned long long *s_max = s_max_all + g * BG;
   stage_basis<RP>(B, sLU, sW, sBK, sPerm);
-  const int r = B.r, p = B.p, n = B.n, tid = threadIdx.x;
+  const int r = B.r, p = B.p, n = B.n;
 
   while (true) {
     if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
-    __syncthreads();
+    group_sync<NG>(g);
     const int u = s_unit;
-    __syncthreads();
+    group_sync<NG>(g);
     if (u >= n_units) break;
     const WorkUnit wu = units[u];
     const ClassRec &C = classes[wu.cls];
@@ -243,13 +264,13 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
       // T := G[ind_path[0]] (d1 x d1) for every item
       {
         const double *g = G + B.goff[C.ind_path[0]];
-        const int dc = d1 * d1, nc = nbi * dc;
-        for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
-          const int t = idx / nc, c = idx - t * nc;
-          T[t * NC + c] = g[t * dc + (c % dc)];
+        const int dc = d1 * d1, nc = nbi * dc, tpc = NT / nc, c = tid % nc, t0 = tid / nc;
+        if (t0 < tpc) {
+          const int e = c % dc;
+          for (int t = t0; t < r; t += tpc) T[t * NC + c] = g[t * dc + e];
         }
       }
-      __syncthreads();
+      group_sync<NG>(g);
 
       for (int op = 0; op < nops; ++op) {
         int kind, v;
@@ -284,20 +305,23 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
               S.kneg = ks < 0;
             }
           }
-          __syncthreads();
-          const int dci = dv * ncol, dco = dvp * ncol, nc = nbi * dco;
-          for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
-            const int t = idx / nc, c = idx - t * nc;
+          group_sync<NG>(g);
+          const int dci = dv * ncol, dco = dvp * ncol, nc = nbi * dco, tpc = NT / nc, c = tid % nc, t0 = tid / nc;
+          if (t0 < tpc) {
             const int j = c / dco, e = c - j * dco, x = e / ncol, z = e - x * ncol;
             const ItemState &S = ist[j];
-            const double *F = B.ops + S.opoff;
-            const double *Tt = T + t * NC + j * dci;
-            double a = 0.0;
-            for (int y = 0; y < dv; ++y) a = fmad(F[x * dv + y], Tt[y * ncol + z], a);
-            if (S.kcol >= 0) a = mul(a, (S.kneg ? B.kitm : B.kitp)[(size_t)t * p + S.kcol]);
-            X[t * NC + c] = a;
+            const double *F = B.ops + S.opoff + x * dv;
+            const double *kt = S.kcol >= 0 ? (S.kneg ? B.kitm : B.kitp) + S.kcol : nullptr;
+            const double *Tc = T + j * dci + z;
+            for (int t = t0; t < r; t += tpc) {
+              const double *Tt = Tc + t * NC;
+              double a = 0.0;
+              for (int y = 0; y < dv; ++y) a = fmad(F[y], Tt[y * ncol], a);
+              if (kt) a = mul(a, kt[(size_t)t * p]);
+              X[t * NC + c] = a;
+            }
           }
-          __syncthreads();
+          group_sync<NG>(g);
           double *tmp = T; T = X; X = tmp;
         } else if (kind == 1) {
           // ---- edge e: T <- conv(G_b prod K, T)  (integrate_left_edge, time-ordered convolution)
@@ -320,39 +344,44 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
             S.taboff = B.tab_off[b] + sig * 2 * r * dd;
           }
           // (a) gc = K^-1 T (in place), then Gt = W gc (into X)
-          panel_lu_solve<RP>(sLU, sPerm, T, r, nc);
-          __syncthreads();
-          panel_gemm<RP, false>(sW, T, X, r, nc, nullptr, nullptr);
-          __syncthreads();
+          panel_lu_solve<RP, NC, NT>(sLU, sPerm, T, r, nc, tid);
+          group_sync<NG>(g);
+          panel_gemm<RP, NG, false>(sW, T, X, r, nc, nullptr, nullptr, tid);
+          group_sync<NG>(g);
           // (b) Q_l = Ft_l gc_l + fc_l Gt_l (into Y)
-          for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
-            const int l = idx / nc, c = idx - l * nc;
-            const int j = c / dc, ee = c - j * dc, x = ee / ncol, z = ee - x * ncol;
-            const double *tb = B.tab + ist[j].taboff;
-            const double *fl = tb + l * dd, *ftl = tb + (long)r * dd + l * dd;
-            const double *gl = T + l * NC + j * dc, *gtl = X + l * NC + j * dc;
-            double a = 0.0;
-            for (int y = 0; y < d; ++y) a = fmad(ftl[x * d + y], gl[y * ncol + z], fmad(fl[x * d + y], gtl[y * ncol + z], a));
-            Y[l * NC + c] = a;
+          const int tpc = NT / nc, cq = tid % nc, t0 = tid / nc;
+          if (t0 < tpc) {
+            const int c = cq, j = c / dc, ee = c - j * dc, x = ee / ncol, z = ee - x * ncol;
+            const double *tb = B.tab + ist[j].taboff + x * d;
+            const double *gc = T + j * dc + z, *gtc = X + j * dc + z;
+            for (int l = t0; l < r; l += tpc) {
+              const double *fl = tb + l * dd, *ftl = tb + (long)r * dd + l * dd;
+              const double *gl = gc + l * NC, *gtl = gtc + l * NC;
+              double a = 0.0;
+              for (int y = 0; y < d; ++y) a = fmad(ftl[y], gl[y * ncol], fmad(fl[y], gtl[y * ncol], a));
+              Y[l * NC + c] = a;
+            }
           }
-          __syncthreads();
+          group_sync<NG>(g);
           // (c) h1 = (beta K) Q (into X; Gt is no longer needed)
-          panel_gemm<RP, false>(sBK, Y, X, r, nc, nullptr, nullptr);
-          __syncthreads();
+          panel_gemm<RP, NG, false>(sBK, Y, X, r, nc, nullptr, nullptr, tid);
+          group_sync<NG>(g);
           // (d) P'_l = K(0, om_l) (fc_l gc_l) (into Y)
-          for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
-            const int l = idx / nc, c = idx - l * nc;
-            const int j = c / dc, ee = c - j * dc, x = ee / ncol, z = ee - x * ncol;
-            const double *fl = B.tab + ist[j].taboff + l * dd;
-            const double *gl = T + l * NC + j * dc;
-            double a = 0.0;
-            for (int y = 0; y < d; ++y) a = fmad(fl[x * d + y], gl[y * ncol + z], a);
-            Y[l * NC + c] = mul(B.k0[l], a);
+          if (t0 < tpc) {
+            const int c = cq, j = c / dc, ee = c - j * dc, x = ee / ncol, z = ee - x * ncol;
+            const double *tb = B.tab + ist[j].taboff + x * d;
+            const double *gc = T + j * dc + z;
+            for (int l = t0; l < r; l += tpc) {
+              const double *fl = tb + l * dd, *gl = gc + l * NC;
+              double a = 0.0;
+              for (int y = 0; y < d; ++y) a = fmad(fl[y], gl[y * ncol], a);
+              Y[l * NC + c] = mul(B.k0[l], a);
+            }
           }
-          __syncthreads();
+          group_sync<NG>(g);
           // (e) h = fma(t_i, (beta K) P', h1) (into T)
-          panel_gemm<RP, true>(sBK, Y, T, r, nc, B.tabs, X);
-          __syncthreads();
+          panel_gemm<RP, NG, true>(sBK, Y, T, r, nc, B.tabs, X, tid);
+          group_sync<NG>(g);
         } else {
           // ---- zero vertex (multiply_left_vertex_and_right_zero_vertex)
           const int b_mu = C.ind_path[v - 1];
@@ -367,54 +396,63 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
             if (B.set_to_orb[pk * n + i] >= 0) qs = i + 1;
           const int dci = dv * d1, dmid = dv * d0, dco = dvp * d0;
           const int ncm = nbi * dmid, nco = nbi * dco;
-          for (int idx = tid; idx < r * nco; idx += PANEL_THREADS) {
-            const int t = idx / nco, c = idx - t * nco;
-            X[t * NC + c] = 0.0;
-          }
-          __syncthreads();
+          const int tpo = NT / nco, co = tid % nco, to0 = tid / nco;
+          const int tpm = NT / ncm, cm = tid % ncm, tm0 = tid / ncm;
+          if (to0 < tpo)
+            for (int t = to0; t < r; t += tpo) X[t * NC + co] = 0.0;
+          group_sync<NG>(g);
           for (int mu = 0; mu < qs; ++mu) {
             const int om = B.set_to_orb[pk * n + mu];
-            for (int idx = tid; idx < r * ncm; idx += PANEL_THREADS) {
-              const int t = idx / ncm, c = idx - t * ncm;
-              const int j = c / dmid, ee = c - j * dmid, x = ee / d0, z = ee - x * d0;
-              const double *Tt = T + t * NC + j * dci;
-              double a = 0.0;
-              for (int kap = 0; kap < qs; ++kap) {
-                const int ok = B.set_to_orb[pk * n + kap];
-                const double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
-                if (h == 0.0) continue;
-                const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0;
-                double tf = 0.0;
-                for (int y = 0; y < d1; ++y) tf = fmad(Tt[x * d1 + y], Fk[y * d0 + z], tf);
-                a = fmad(mul(hs, h), tf, a);
+            if (tm0 < tpm) {
+              const int c = cm, j = c / dmid, ee = c - j * dmid, x = ee / d0, z = ee - x * d0;
+              const double *Tc = T + j * dci + x * d1;
+              for (int t = tm0; t < r; t += tpm) {
+                const double *Tt = Tc + t * NC;
+                double a = 0.0;
+                for (int kap = 0; kap < qs; ++kap) {
+                  const int ok = B.set_to_orb[pk * n + kap];
+                  const double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
+                  if (h == 0.0) continue;
+                  const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0 + z;
+                  double tf = 0.0;
+                  for (int y = 0; y < d1; ++y) tf = fmad(Tt[y], Fk[y * d0], tf);
+                  a = fmad(mul(hs, h), tf, a);
+                }
+                Y[t * NC + c] = a;
               }
-              Y[t * NC + c] = a;
             }
-            __syncthreads();
+            group_sync<NG>(g);
             const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
-            for (int idx = tid; idx < r * nco; idx += PANEL_THREADS) {
-              const int t = idx / nco, c = idx - t * nco;
-              const int j = c / dco, ee = c - j * dco, x = ee / d0, z = ee - x * d0;
-              const double *Yt = Y + t * NC + j * dmid;
-              double a = 0.0;
-              for (int y = 0; y < dv; ++y) a = fmad(Fm[x * dv + y], Yt[y * d0 + z], a);
-              X[t * NC + c] = add(X[t * NC + c], a);
+            if (to0 < tpo) {
+              const int c = co, j = c / dco, ee = c - j * dco, x = ee / d0, z = ee - x * d0;
+              const double *Fx = Fm + x * dv, *Yc = Y + j * dmid + z;
+              for (int t = to0; t < r; t += tpo) {
+                const double *Yt = Yc + t * NC;
+                double a = 0.0;
+                for (int y = 0; y < dv; ++y) a = fmad(Fx[y], Yt[y * d0], a);
+                X[t * NC + c] = add(X[t * NC + c], a);
+              }
             }
-            __syncthreads();
+            group_sync<NG>(g);
           }
           double *tmp = T; T = X; X = tmp;
         }
       }
       // ---- prefactor and signs, the |T| > 1e-16 guard, accumulation
       const int dco = dout * d0, nc = nbi * dco;
-      for (int idx = tid; idx < r * nc; idx += PANEL_THREADS) {
-        const int t = idx / nc, c = idx - t * nc, j = c / dco;
-        const double v = fabs(mul(T[t * NC + c], ist[j].scale));
-        atomicMax(&s_max[j], (unsigned long long)__double_as_longlong(v));  // non-negative doubles order as integers
+      {
+        const int tpc = NT / nc, c = tid % nc, t0 = tid / nc;
+        if (t0 < tpc) {
+          const int j = c / dco;
+          const double sc = ist[j].scale;
+          double mx = 0.0;
+          for (int t = t0; t < r; t += tpc) mx = fmax(mx, fabs(mul(T[t * NC + c], sc)));
+          atomicMax(&s_max[j], (unsigned long long)__double_as_longlong(mx));  // non-negative doubles order as integers
+        }
       }
-      __syncthreads();
+      group_sync<NG>(g);
       double *dst = Sigma + B.goff[C.b_out];
-      for (int idx = tid; idx < r * dco; idx += PANEL_THREADS) {
+      for (int idx = tid; idx < r * dco; idx += NT) {
         const int t = idx / dco, ee = idx - t * dco;
         double a = 0.0;
         bool keep_any = false;
@@ -425,7 +463,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           }
         if (keep_any) atomicAdd(dst + idx, mul(scale, a));
       }
-      __syncthreads();
+      group_sync<NG>(g);
     }
   }
 }
