@@ -34,6 +34,7 @@ struct DevBasis {
   const double *LUp;    // RP x RP padded LU of K(t_i, om_l), column-major: unit L below the diagonal, U on and above
                         // (pad: U_kk = 1), followed by the RP reciprocals 1 / U_kk
   const int *perm;      // RP: row gathered into position i by the pivoting (-1 beyond r)
+  const int *pinv;      // RP: position of row t after the pivoting (-1 beyond r)
   const double *Wp;     // RP x RP column-major: W[l][k] = K(0, om_k) / (om_k - om_l), 0 on the diagonal and in the pad
   const double *BKp;    // RP x RP column-major: beta * K(t_i, om_l), 0 in the pad
   const double *tabs;   // r: absolute t_i

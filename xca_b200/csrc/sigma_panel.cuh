@@ -4,7 +4,8 @@
 // `batch` of them together.  The T slabs of the batch's items sit side by side as the columns of a
 // shared-memory panel (RP rows = tau nodes, NC columns = item x matrix entry), so every r x r DLR
 // operator of an edge acts on all of them at once:
-//   K^-1 T     one thread per column, the column in registers, substitution in dtrsm order;
+//   K^-1 T     blocked substitution by the whole CTA (8-row blocks: register-tiled rectangular updates,
+//              then the in-block solve), every element in dtrsm order;
 //   W gc, (beta K) Q, (beta K) P'   register-tiled products (TR x TC outputs per thread, operand pairs
 //                                   loaded as double2 from shared memory), each output one chain of
 //                                   fused multiply-adds over k ascending from zero;
@@ -35,7 +36,7 @@ __host__ __device__ constexpr int panel_nc() { return PanelCfg<RP>::NC; }
 // Dynamic shared memory of the panel kernels, in doubles.
 template <int RP>
 __host__ __device__ constexpr size_t panel_smem_doubles() {
-  return 3 * (size_t)RP * RP + RP + 3 * (size_t)RP * PanelCfg<RP>::NC + (sizeof(ItemState) * PANEL_BMAX + 7) / 8 + (RP + 1) / 2;
+  return 3 * (size_t)RP * RP + RP + 3 * (size_t)RP * PanelCfg<RP>::NC + (sizeof(ItemState) * PANEL_BMAX + 7) / 8 + RP;
 }
 
 // A thread group of NT threads working on a panel of NCG columns (row stride NCG).
@@ -106,25 +107,99 @@ __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const 
   }
 }
 
-// P[:, c] <- K^-1 P[:, c] for c < ncols (row stride NCG), one column per thread of the group (gathered
-// through the pivots, LU substitution in registers, written back in place).
-template <int RP, int NCG, int NT>
-__device__ __forceinline__ void panel_lu_solve(const double *__restrict__ sLU, const int *__restrict__ sPerm, double *P, int r, int ncols,
-                                               int t) {
-  for (int c = t; c < ncols; c += NT) {
-    double x[RP];
-#pragma unroll
-    for (int i = 0; i < RP; ++i) {
-      const int s = sPerm[i];
-      x[i] = s >= 0 ? P[s * NCG + c] : 0.0;
+// P[:, c] <- K^-1 P[:, c] for c < nc on a panel whose rows are already in pivot order (row i holds the
+// original row perm[i]), by the whole thread group: 8-row blocks, each a rectangular update (every thread
+// a 2 x 2 tile, operand pairs as double2) followed by the in-block substitution (one thread per column).
+// Every element receives exactly the fused multiply-adds of lu_solve_reg in the same order — forward
+// k ascending, backward k descending with the reciprocal diagonal applied at k = i — so the result is
+// bit-identical to it; rows r .. RP-1 (padding) are neither read nor written.
+template <int RP, int NCG, int NT, int NG>
+__device__ __forceinline__ void panel_trsm(const double *__restrict__ sLU, double *P, int r, int nc, int t, int g) {
+  const int nblk = (r + 7) >> 3, ncp = (nc + 1) >> 1;
+  for (int J = 0; J < nblk; ++J) {
+    const int j0 = J << 3, j1 = min(r, j0 + 8);
+    if (J > 0) {
+      const int nrp = (j1 - j0 + 1) >> 1;
+      for (int w = t; w < nrp * ncp; w += NT) {
+        const int rp = w / ncp, c = 2 * (w - rp * ncp), i = j0 + 2 * rp;
+        const bool two = i + 1 < j1;
+        double2 a0 = *reinterpret_cast<const double2 *>(P + i * NCG + c);
+        double2 a1 = two ? *reinterpret_cast<const double2 *>(P + (i + 1) * NCG + c) : make_double2(0.0, 0.0);
+#pragma unroll 4
+        for (int k = 0; k < j0; ++k) {
+          const double2 l = *reinterpret_cast<const double2 *>(sLU + k * RP + i);  // L[i][k], L[i+1][k]
+          const double2 x = *reinterpret_cast<const double2 *>(P + k * NCG + c);
+          a0.x = fmad(-l.x, x.x, a0.x);
+          a0.y = fmad(-l.x, x.y, a0.y);
+          a1.x = fmad(-l.y, x.x, a1.x);
+          a1.y = fmad(-l.y, x.y, a1.y);
+        }
+        *reinterpret_cast<double2 *>(P + i * NCG + c) = a0;
+        if (two) *reinterpret_cast<double2 *>(P + (i + 1) * NCG + c) = a1;
+      }
+      group_sync<NG>(g);
     }
-    lu_solve_reg<RP>(sLU, x);
+    for (int c = t; c < nc; c += NT) {
+      double xb[8];
 #pragma unroll
-    for (int i = 0; i < RP; ++i)
-      if (i < r) P[i * NCG + c] = x[i];
+      for (int q = 0; q < 8; ++q) xb[q] = (j0 + q < j1) ? P[(j0 + q) * NCG + c] : 0.0;
+#pragma unroll
+      for (int kk = 0; kk < 7; ++kk)
+#pragma unroll
+        for (int q = kk + 1; q < 8; ++q)
+          if (j0 + q < j1) xb[q] = fmad(-sLU[(j0 + kk) * RP + j0 + q], xb[kk], xb[q]);
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (j0 + q < j1) P[(j0 + q) * NCG + c] = xb[q];
+    }
+    group_sync<NG>(g);
+  }
+  const double *dinv = sLU + RP * RP;
+  for (int J = nblk - 1; J >= 0; --J) {
+    const int j0 = J << 3, j1 = min(r, j0 + 8);
+    if (j1 < r) {
+      const int nrp = (j1 - j0 + 1) >> 1;
+      for (int w = t; w < nrp * ncp; w += NT) {
+        const int rp = w / ncp, c = 2 * (w - rp * ncp), i = j0 + 2 * rp;
+        const bool two = i + 1 < j1;
+        double2 a0 = *reinterpret_cast<const double2 *>(P + i * NCG + c);
+        double2 a1 = two ? *reinterpret_cast<const double2 *>(P + (i + 1) * NCG + c) : make_double2(0.0, 0.0);
+#pragma unroll 4
+        for (int k = r - 1; k >= j1; --k) {
+          const double2 u = *reinterpret_cast<const double2 *>(sLU + k * RP + i);  // U[i][k], U[i+1][k]
+          const double2 x = *reinterpret_cast<const double2 *>(P + k * NCG + c);
+          a0.x = fmad(-u.x, x.x, a0.x);
+          a0.y = fmad(-u.x, x.y, a0.y);
+          a1.x = fmad(-u.y, x.x, a1.x);
+          a1.y = fmad(-u.y, x.y, a1.y);
+        }
+        *reinterpret_cast<double2 *>(P + i * NCG + c) = a0;
+        if (two) *reinterpret_cast<double2 *>(P + (i + 1) * NCG + c) = a1;
+      }
+      group_sync<NG>(g);
+    }
+    for (int c = t; c < nc; c += NT) {
+      double xb[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) xb[q] = (j0 + q < j1) ? P[(j0 + q) * NCG + c] : 0.0;
+#pragma unroll
+      for (int kk = 7; kk >= 0; --kk) {
+        if (j0 + kk < j1) {
+          xb[kk] = mul(xb[kk], dinv[j0 + kk]);
+#pragma unroll
+          for (int q = 0; q < kk; ++q) xb[q] = fmad(-sLU[(j0 + kk) * RP + j0 + q], xb[kk], xb[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (j0 + q < j1) P[(j0 + q) * NCG + c] = xb[q];
+    }
+    group_sync<NG>(g);
   }
 }
 
+// Stage the DLR matrices; sPerm receives the pivot gather (RP ints) followed by its inverse (RP ints: the
+// pivot-order position of tau node t, -1 in the pad).
 template <int RP>
 __device__ __forceinline__ void stage_basis(const DevBasis &B, double *sLU, double *sW, double *sBK, int *sPerm) {
   for (int i = threadIdx.x; i < RP * RP + RP; i += blockDim.x) sLU[i] = B.LUp[i];
@@ -132,7 +207,10 @@ __device__ __forceinline__ void stage_basis(const DevBasis &B, double *sLU, doub
     sW[i] = B.Wp[i];
     sBK[i] = B.BKp[i];
   }
-  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
+  for (int i = threadIdx.x; i < RP; i += blockDim.x) {
+    sPerm[i] = B.perm[i];
+    sPerm[RP + i] = B.pinv[i];
+  }
   __syncthreads();
 }
 
@@ -175,11 +253,10 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(Dev
       double v = g[t * dd + e];
       if (nf >= 1) v = mul(v, (s1 ? B.kitm : B.kitp)[(size_t)t * p + l1]);
       if (nf >= 2) v = mul(v, (s2 ? B.kitm : B.kitp)[(size_t)t * p + l2]);
-      PA[t * NC + c] = v;
+      PA[sPerm[RP + t] * NC + c] = v;
     }
     __syncthreads();
-    panel_lu_solve<RP, NC, PANEL_THREADS>(sLU, sPerm, PA, r, ncols, threadIdx.x);
-    __syncthreads();
+    panel_trsm<RP, NC, PANEL_THREADS, 1>(sLU, PA, r, ncols, threadIdx.x, 0);
     panel_gemm<RP, 1, false>(sW, PA, PB, r, ncols, nullptr, nullptr, threadIdx.x);
     __syncthreads();
     double *out = const_cast<double *>(B.tab) + B.tab_off[b];
@@ -272,13 +349,22 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
       }
       group_sync<NG>(g);
 
+      // op order: for v < vct0: vertex v, edge v; zero vertex; for v > vct0: edge v - 1, vertex v
+      const int pre = 2 * (vct0 - 1);
+      auto op_kind = [&](int o) -> int {
+        if (o < pre) return (o & 1) ? 1 : 0;
+        if (o == pre) return 2;
+        return ((o - pre - 1) & 1) ? 0 : 1;
+      };
       for (int op = 0; op < nops; ++op) {
-        int kind, v;
-        const int pre = 2 * (vct0 - 1);
-        if (op < pre) { v = 1 + op / 2; kind = (op & 1) ? 1 : 0; }
-        else if (op == pre) { v = vct0; kind = 2; }
-        else { const int q = op - pre - 1; v = vct0 + 1 + q / 2; kind = (q & 1) ? 0 : 1; }
+        int v;
+        const int kind = op_kind(op);
+        if (op < pre) v = 1 + op / 2;
+        else if (op == pre) v = vct0;
+        else v = vct0 + 1 + (op - pre - 1) / 2;
         const int ncol = v < vct0 ? d1 : d0;
+        // a vertex feeding an edge writes its rows in pivot order (the order the substitution works in)
+        const int *rowpos = (op + 1 < nops && op_kind(op + 1) == 1) ? sPerm + RP : nullptr;
 
         if (kind == 0) {
           // ---- vertex v: T(t) <- k(t) F T(t)  (multiply_left_vertex)
@@ -318,7 +404,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
               double a = 0.0;
               for (int y = 0; y < dv; ++y) a = fmad(F[y], Tt[y * ncol], a);
               if (kt) a = mul(a, kt[(size_t)t * p]);
-              X[t * NC + c] = a;
+              X[(rowpos ? rowpos[t] : t) * NC + c] = a;
             }
           }
           group_sync<NG>(g);
@@ -344,8 +430,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
             S.taboff = B.tab_off[b] + sig * 2 * r * dd;
           }
           // (a) gc = K^-1 T (in place), then Gt = W gc (into X)
-          panel_lu_solve<RP, NC, NT>(sLU, sPerm, T, r, nc, tid);
-          group_sync<NG>(g);
+          panel_trsm<RP, NC, NT, NG>(sLU, T, r, nc, tid, g);
           panel_gemm<RP, NG, false>(sW, T, X, r, nc, nullptr, nullptr, tid);
           group_sync<NG>(g);
           // (b) Q_l = Ft_l gc_l + fc_l Gt_l (into Y)
@@ -399,7 +484,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           const int tpo = NT / nco, co = tid % nco, to0 = tid / nco;
           const int tpm = NT / ncm, cm = tid % ncm, tm0 = tid / ncm;
           if (to0 < tpo)
-            for (int t = to0; t < r; t += tpo) X[t * NC + co] = 0.0;
+            for (int t = to0; t < r; t += tpo) X[(rowpos ? rowpos[t] : t) * NC + co] = 0.0;
           group_sync<NG>(g);
           for (int mu = 0; mu < qs; ++mu) {
             const int om = B.set_to_orb[pk * n + mu];
@@ -430,7 +515,8 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
                 const double *Yt = Yc + t * NC;
                 double a = 0.0;
                 for (int y = 0; y < dv; ++y) a = fmad(Fx[y], Yt[y * d0], a);
-                X[t * NC + c] = add(X[t * NC + c], a);
+                const int row = rowpos ? rowpos[t] : t;
+                X[row * NC + c] = add(X[row * NC + c], a);
               }
             }
             group_sync<NG>(g);

@@ -152,7 +152,7 @@ struct Ctx {
   int region = 0;
   // device copies
   DevBuf<double> d_tabs, d_k0, d_kitp, d_kitm, d_kpow, d_polesb, d_hval, d_hrefl, d_ops;
-  DevBuf<int> d_dims, d_set_to_orb, d_perm;
+  DevBuf<int> d_dims, d_set_to_orb, d_perm, d_pinv;
   DevBuf<double> d_LUp, d_Wp, d_BKp, d_tab;
   DevBuf<long> d_tab_off;
   DevBuf<long> d_goff, d_F_off, d_Fd_off, d_Fb_off, d_Fdb_off;
@@ -184,7 +184,7 @@ struct Ctx {
   DevBasis basis(int nsig) const {
     DevBasis B;
     B.r = r; B.p = p; B.n = n; B.nb = nb; B.nq = nq; B.region = region; B.beta = beta;
-    B.LUp = d_LUp.ptr; B.perm = d_perm.ptr; B.Wp = d_Wp.ptr; B.BKp = d_BKp.ptr; B.tabs = d_tabs.ptr; B.k0 = d_k0.ptr;
+    B.LUp = d_LUp.ptr; B.perm = d_perm.ptr; B.pinv = d_pinv.ptr; B.Wp = d_Wp.ptr; B.BKp = d_BKp.ptr; B.tabs = d_tabs.ptr; B.k0 = d_k0.ptr;
     B.tab = d_tab.ptr; B.tab_off = d_tab_off.ptr; B.nsig = nsig;
     B.kitp = d_kitp.ptr; B.kitm = d_kitm.ptr; B.kpow = d_kpow.ptr; B.polesb = d_polesb.ptr;
     B.hval = d_hval.ptr; B.hrefl = d_hrefl.ptr; B.goff = d_goff.ptr; B.dims = d_dims.ptr; B.ops = d_ops.ptr;
@@ -267,12 +267,15 @@ static void setup_basis(Ctx *c, double beta, double lambda, double eps, int r, c
     for (int k = 0; k < r; ++k) std::swap(idx[k], idx[c->piv[k]]);
     for (int i = 0; i < r; ++i) c->perm[i] = idx[i];
   }
+  std::vector<int> pinv(RP, -1);
+  for (int i = 0; i < r; ++i) pinv[c->perm[i]] = i;
   c->RFp.assign((size_t)RP * RP, 0.0);
   for (int i = 0; i < r; ++i)
     for (int l = 0; l < r; ++l) c->RFp[(size_t)l * RP + i] = k_it(it[i], -rf[l]);
   cudaStream_t s = c->stream;
   c->d_LUp.upload(c->LUp, s); c->d_Wp.upload(c->Wp, s); c->d_BKp.upload(c->BKp, s); c->d_perm.upload(c->perm, s);
   c->d_RFp.upload(c->RFp, s);
+  c->d_pinv.upload(pinv, s);
   c->corr_cache.clear();
   c->d_tabs.upload(c->tabs, s); c->d_k0.upload(c->k0, s); c->d_k1.upload(c->k1, s); c->d_rf.upload(c->rf, s);
   c->d_dims.upload(c->dims, s); c->d_goff.upload(c->goff, s);
