@@ -6,9 +6,9 @@
 // operator of an edge acts on all of them at once:
 //   K^-1 T     blocked substitution by the whole CTA (8-row blocks: register-tiled rectangular updates,
 //              then the in-block solve), every element in dtrsm order;
-//   W gc, (beta K) Q, (beta K) P'   register-tiled products (TR x TC outputs per thread, operand pairs
-//                                   loaded as double2 from shared memory), each output one chain of
-//                                   fused multiply-adds over k ascending from zero;
+//   W gc, (beta K) Q and (beta K) P'   register-tiled products (TR x TC outputs per thread, operand pairs
+//                                   loaded as double2 from shared memory; the last two in one pass),
+//                                   each output one chain of fused multiply-adds over k ascending from zero;
 // and the per-item steps (vertex products with the item's operator and K factor, Q and P' with the
 // item's edge table, the zero vertex) run with the threads striding over panel entries.  Every element
 // sees exactly the operations, in the same order, as in the CPU restatement, so each item's contribution
@@ -103,6 +103,64 @@ __device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const 
     for (int b = 0; b < TC; ++b) {
       const int c = 2 * (ct + (b / 2) * CT) + (b & 1);
       if (c < ncols) Y[i * NCG + c] = EPI ? fmad(tabs[i], acc[a][b], H1[i * NCG + c]) : acc[a][b];
+    }
+  }
+}
+
+// Y[i][c] = fma(t_i, (M X2)[i][c], (M X1)[i][c]) for i < r, c < ncols: the two products of one operand M
+// in one pass (each accumulator one fused multiply-add chain over k ascending from zero), tiled as
+// panel_gemm.
+template <int RP, int G>
+__device__ __forceinline__ void panel_gemm2(const double *__restrict__ sM, const double *__restrict__ X1, const double *__restrict__ X2,
+                                            double *__restrict__ Y, int r, int ncols, const double *__restrict__ tabs, int t) {
+  using P = PanelGrp<RP, G>;
+  constexpr int NCG = P::NCG, TR = P::TR, TC = P::TC, CT = P::CT;
+  const int rt = t / CT, ct = t - rt * CT;
+  const int i0 = rt * TR;
+  if (i0 >= r || 2 * ct >= ncols) return;
+  double a1[TR][TC], a2[TR][TC];
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b) {
+      a1[a][b] = 0.0;
+      a2[a][b] = 0.0;
+    }
+#pragma unroll 1
+  for (int k = 0; k < r; ++k) {
+    double mv[TR], xv[TC], yv[TC];
+    const double2 *mp = reinterpret_cast<const double2 *>(sM + k * RP + i0);
+#pragma unroll
+    for (int a = 0; a < TR / 2; ++a) {
+      const double2 v = mp[a];
+      mv[2 * a] = v.x;
+      mv[2 * a + 1] = v.y;
+    }
+#pragma unroll
+    for (int q = 0; q < TC / 2; ++q) {
+      const double2 v = *reinterpret_cast<const double2 *>(X1 + k * NCG + 2 * (ct + q * CT));
+      const double2 w = *reinterpret_cast<const double2 *>(X2 + k * NCG + 2 * (ct + q * CT));
+      xv[2 * q] = v.x;
+      xv[2 * q + 1] = v.y;
+      yv[2 * q] = w.x;
+      yv[2 * q + 1] = w.y;
+    }
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) {
+        a1[a][b] = fmad(mv[a], xv[b], a1[a][b]);
+        a2[a][b] = fmad(mv[a], yv[b], a2[a][b]);
+      }
+  }
+#pragma unroll
+  for (int a = 0; a < TR; ++a) {
+    const int i = i0 + a;
+    if (i >= r) break;
+#pragma unroll
+    for (int b = 0; b < TC; ++b) {
+      const int c = 2 * (ct + (b / 2) * CT) + (b & 1);
+      if (c < ncols) Y[i * NCG + c] = fmad(tabs[i], a2[a][b], a1[a][b]);
     }
   }
 }
@@ -433,39 +491,52 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           panel_trsm<RP, NC, NT, NG>(sLU, T, r, nc, tid, g);
           panel_gemm<RP, NG, false>(sW, T, X, r, nc, nullptr, nullptr, tid);
           group_sync<NG>(g);
-          // (b) Q_l = Ft_l gc_l + fc_l Gt_l (into Y)
-          const int tpc = NT / nc, cq = tid % nc, t0 = tid / nc;
-          if (t0 < tpc) {
-            const int c = cq, j = c / dc, ee = c - j * dc, x = ee / ncol, z = ee - x * ncol;
-            const double *tb = B.tab + ist[j].taboff + x * d;
-            const double *gc = T + j * dc + z, *gtc = X + j * dc + z;
-            for (int l = t0; l < r; l += tpc) {
-              const double *fl = tb + l * dd, *ftl = tb + (long)r * dd + l * dd;
-              const double *gl = gc + l * NC, *gtl = gtc + l * NC;
-              double a = 0.0;
-              for (int y = 0; y < d; ++y) a = fmad(ftl[y], gl[y * ncol], fmad(fl[y], gtl[y * ncol], a));
-              Y[l * NC + c] = a;
+          // (b) per row l (one warp per row; Q and P' of row l read only row l of gc and Gt):
+          //     Q_l = Ft_l gc_l + fc_l Gt_l (into Y) and P'_l = K(0, om_l) (fc_l gc_l) (over Gt, into X)
+          {
+            constexpr int CPL = (NC + 31) / 32;
+            const int lane = tid & 31, warp = tid >> 5;
+            const double *tbq[CPL];
+            int coff[CPL];
+            bool cval[CPL];
+#pragma unroll
+            for (int q = 0; q < CPL; ++q) {
+              const int c = lane + 32 * q;
+              cval[q] = c < nc;
+              const int cc = cval[q] ? c : 0;
+              const int j = cc / dc, ee = cc - j * dc, x = ee / ncol, z = ee - x * ncol;
+              tbq[q] = B.tab + ist[j].taboff + x * d;
+              coff[q] = j * dc + z;
+            }
+            for (int l = warp; l < r; l += NT / 32) {
+              double qv[CPL], pv[CPL];
+#pragma unroll
+              for (int q = 0; q < CPL; ++q) {
+                double aq = 0.0, ap = 0.0;
+                if (cval[q]) {
+                  const double *fl = tbq[q] + l * dd, *ftl = tbq[q] + (long)r * dd + l * dd;
+                  const double *gl = T + l * NC + coff[q], *gtl = X + l * NC + coff[q];
+                  for (int y = 0; y < d; ++y) {
+                    aq = fmad(ftl[y], gl[y * ncol], fmad(fl[y], gtl[y * ncol], aq));
+                    ap = fmad(fl[y], gl[y * ncol], ap);
+                  }
+                }
+                qv[q] = aq;
+                pv[q] = mul(B.k0[l], ap);
+              }
+              __syncwarp();
+#pragma unroll
+              for (int q = 0; q < CPL; ++q)
+                if (cval[q]) {
+                  const int c = lane + 32 * q;
+                  Y[l * NC + c] = qv[q];
+                  X[l * NC + c] = pv[q];
+                }
             }
           }
           group_sync<NG>(g);
-          // (c) h1 = (beta K) Q (into X; Gt is no longer needed)
-          panel_gemm<RP, NG, false>(sBK, Y, X, r, nc, nullptr, nullptr, tid);
-          group_sync<NG>(g);
-          // (d) P'_l = K(0, om_l) (fc_l gc_l) (into Y)
-          if (t0 < tpc) {
-            const int c = cq, j = c / dc, ee = c - j * dc, x = ee / ncol, z = ee - x * ncol;
-            const double *tb = B.tab + ist[j].taboff + x * d;
-            const double *gc = T + j * dc + z;
-            for (int l = t0; l < r; l += tpc) {
-              const double *fl = tb + l * dd, *gl = gc + l * NC;
-              double a = 0.0;
-              for (int y = 0; y < d; ++y) a = fmad(fl[y], gl[y * ncol], a);
-              Y[l * NC + c] = mul(B.k0[l], a);
-            }
-          }
-          group_sync<NG>(g);
-          // (e) h = fma(t_i, (beta K) P', h1) (into T)
-          panel_gemm<RP, NG, true>(sBK, Y, T, r, nc, B.tabs, X, tid);
+          // (c) h = fma(t_i, (beta K) P', (beta K) Q) (into T; gc is no longer needed)
+          panel_gemm2<RP, NG>(sBK, Y, X, T, r, nc, B.tabs, tid);
           group_sync<NG>(g);
         } else {
           // ---- zero vertex (multiply_left_vertex_and_right_zero_vertex)
