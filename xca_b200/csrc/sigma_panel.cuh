@@ -3,299 +3,276 @@
 // A CTA of PANEL_THREADS threads takes a run of pole tuples of one path class (work unit) and evaluates
 // `batch` of them together.  The T slabs of the batch's items sit side by side as the columns of a
 // shared-memory panel (RP rows = tau nodes, NC columns = item x matrix entry), so every r x r DLR
-// operator of an edge acts on all of them at once:
-//   K^-1 T     blocked substitution by the whole CTA (8-row blocks: register-tiled rectangular updates,
-//              then the in-block solve), every element in dtrsm order;
-//   W gc, (beta K) Q and (beta K) P'   register-tiled products (TR x TC outputs per thread, operand pairs
-//                                   loaded as double2 from shared memory; the last two in one pass),
-//                                   each output one chain of fused multiply-adds over k ascending from zero;
-// and the per-item steps (vertex products with the item's operator and K factor, Q and P' with the
-// item's edge table, the zero vertex) run with the threads striding over panel entries.  Every element
-// sees exactly the operations, in the same order, as in the CPU restatement, so each item's contribution
-// is bit-identical to it (sigma_kernel.cuh documents the item arithmetic and its reference lines).
+// operator of an edge acts on all of them at once, on the FP64 tensor cores (mma.sync m8n8k4 f64):
+//   K^-1 T     blocked substitution by the whole CTA: per 8-row block an MMA rectangular update, then the
+//              in-block solve (one thread per column);
+//   W gc, and (beta K) Q with (beta K) P' in one pass   warp-tiled MMA products.
+// One FP64 MMA computes every element of its 8 x 8 tile as four fused multiply-adds in ascending k,
+// each correctly rounded — the same values as the scalar chain fma(a3, b3, fma(a2, b2, fma(a1, b1,
+// fma(a0, b0, c)))), which this build checks on the device bit for bit.  So each output element is
+// still one chain of fused multiply-adds over k ascending from zero (descending in the backward
+// substitution, fed as reversed k inside each group of four), exactly as in the CPU restatement, and
+// each item's contribution stays bit-identical to it.  The per-item steps (vertex products with the
+// item's operator and K factor, Q and P' with the item's edge table, the zero vertex) run on the CUDA
+// cores with threads owning panel columns.  sigma_kernel.cuh documents the item arithmetic and its
+// reference lines.
 #pragma once
 #include "sigma_kernel.cuh"
 
 namespace xca {
 
 constexpr int PANEL_THREADS = 256;
+constexpr int PANEL_WARPS = PANEL_THREADS / 32;
 constexpr int PANEL_BMAX = 128;  // items per batch at most
 
+// NC usable panel columns; rows are stored with stride LDP = NC + 8 and the DLR matrices' columns with
+// stride RP + 8 (both 8 mod 16 doubles), so that the four k rows of an MMA fragment fall on distinct
+// shared-memory banks.
 template <int RP>
 struct PanelCfg;
 template <>
-struct PanelCfg<32> { static constexpr int NC = 192, TR = 4, TC = 6; };
+struct PanelCfg<32> { static constexpr int NC = 192, LDP = 200; };
 template <>
-struct PanelCfg<48> { static constexpr int NC = 128, TR = 6, TC = 4; };
+struct PanelCfg<48> { static constexpr int NC = 128, LDP = 136; };
 template <>
-struct PanelCfg<64> { static constexpr int NC = 64, TR = 4, TC = 4; };
+struct PanelCfg<64> { static constexpr int NC = 64, LDP = 72; };
+
+template <int RP>
+__host__ __device__ constexpr int mat_stride() { return RP + 8; }
 
 template <int RP>
 __host__ __device__ constexpr int panel_nc() { return PanelCfg<RP>::NC; }
 
-// Dynamic shared memory of the panel kernels, in doubles.
+// Dynamic shared memory of the panel kernels, in doubles: LU (stride RP + 8) + reciprocal diagonal | W | BK
+// | panels A, B, C (RP x LDP each) | item states | pivot gather and its inverse (2 RP ints).
 template <int RP>
 __host__ __device__ constexpr size_t panel_smem_doubles() {
-  return 3 * (size_t)RP * RP + RP + 3 * (size_t)RP * PanelCfg<RP>::NC + (sizeof(ItemState) * PANEL_BMAX + 7) / 8 + RP;
+  return 3 * (size_t)mat_stride<RP>() * RP + RP + 3 * (size_t)RP * PanelCfg<RP>::LDP + (sizeof(ItemState) * PANEL_BMAX + 7) / 8 + RP;
 }
 
-// A thread group of NT threads working on a panel of NCG columns (row stride NCG).
-template <int RP, int G>
-struct PanelGrp {
-  static constexpr int NT = PANEL_THREADS / G, NCG = PanelCfg<RP>::NC / G;
-  static constexpr int TR = PanelCfg<RP>::TR, TC = PanelCfg<RP>::TC, CT = NCG / TC;
-  static_assert((RP / TR) * CT == NT, "panel tiling must cover the thread group");
-};
-
-// Barrier of thread group g (named barrier 1 + g of NT threads; the whole CTA when G == 1).
-template <int G>
-__device__ __forceinline__ void group_sync(int g) {
-  if (G == 1)
-    __syncthreads();
-  else
-    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(PANEL_THREADS / G) : "memory");
+template <int RP>
+__device__ __forceinline__ void panel_layout(double *smem, double *&sLU, double *&sW, double *&sBK, double *&PA, ItemState *&ist,
+                                             int *&sPerm) {
+  constexpr int S = mat_stride<RP>();
+  sLU = smem;
+  sW = sLU + S * RP + RP;
+  sBK = sW + S * RP;
+  PA = sBK + S * RP;
+  ist = reinterpret_cast<ItemState *>(PA + 3 * RP * PanelCfg<RP>::LDP);
+  sPerm = reinterpret_cast<int *>(reinterpret_cast<double *>(ist) + (sizeof(ItemState) * PANEL_BMAX + 7) / 8);
 }
 
-// Y[i][c] = sum_{k < r} M[i][k] X[k][c] for i < r, c < ncols (M column-major RP x RP; X, Y panels with row
-// stride NCG); t is the thread's index in its group.  EPI: Y[i][c] = fma(t_i, (M X)[i][c], H1[i][c]).
-// Each thread owns TR rows x TC columns: the column pairs 2 (ct + q CT) .. + 1 (q < TC / 2), so that
-// neighbouring lanes read consecutive 16-byte pairs of a panel row (no bank conflict); lanes that share
-// a row tile read the same M operands (broadcasts).
-template <int RP, int G, bool EPI>
-__device__ __forceinline__ void panel_gemm(const double *__restrict__ sM, const double *__restrict__ X, double *__restrict__ Y, int r,
-                                           int ncols, const double *__restrict__ tabs, const double *__restrict__ H1, int t) {
-  using P = PanelGrp<RP, G>;
-  constexpr int NCG = P::NCG, TR = P::TR, TC = P::TC, CT = P::CT;
-  const int rt = t / CT, ct = t - rt * CT;
-  const int i0 = rt * TR;
-  if (i0 >= r || 2 * ct >= ncols) return;
-  double acc[TR][TC];
-#pragma unroll
-  for (int a = 0; a < TR; ++a)
-#pragma unroll
-    for (int b = 0; b < TC; ++b) acc[a][b] = 0.0;
-#pragma unroll 2
-  for (int k = 0; k < r; ++k) {
-    double mv[TR], xv[TC];
-    const double2 *mp = reinterpret_cast<const double2 *>(sM + k * RP + i0);
-#pragma unroll
-    for (int a = 0; a < TR / 2; ++a) {
-      const double2 v = mp[a];
-      mv[2 * a] = v.x;
-      mv[2 * a + 1] = v.y;
-    }
-#pragma unroll
-    for (int q = 0; q < TC / 2; ++q) {
-      const double2 v = *reinterpret_cast<const double2 *>(X + k * NCG + 2 * (ct + q * CT));
-      xv[2 * q] = v.x;
-      xv[2 * q + 1] = v.y;
-    }
-#pragma unroll
-    for (int a = 0; a < TR; ++a)
-#pragma unroll
-      for (int b = 0; b < TC; ++b) acc[a][b] = fmad(mv[a], xv[b], acc[a][b]);
-  }
-#pragma unroll
-  for (int a = 0; a < TR; ++a) {
-    const int i = i0 + a;
-    if (i >= r) break;
-#pragma unroll
-    for (int b = 0; b < TC; ++b) {
-      const int c = 2 * (ct + (b / 2) * CT) + (b & 1);
-      if (c < ncols) Y[i * NCG + c] = EPI ? fmad(tabs[i], acc[a][b], H1[i * NCG + c]) : acc[a][b];
-    }
-  }
-}
-
-// Y[i][c] = fma(t_i, (M X2)[i][c], (M X1)[i][c]) for i < r, c < ncols: the two products of one operand M
-// in one pass (each accumulator one fused multiply-add chain over k ascending from zero), tiled as
-// panel_gemm.
-template <int RP, int G>
-__device__ __forceinline__ void panel_gemm2(const double *__restrict__ sM, const double *__restrict__ X1, const double *__restrict__ X2,
-                                            double *__restrict__ Y, int r, int ncols, const double *__restrict__ tabs, int t) {
-  using P = PanelGrp<RP, G>;
-  constexpr int NCG = P::NCG, TR = P::TR, TC = P::TC, CT = P::CT;
-  const int rt = t / CT, ct = t - rt * CT;
-  const int i0 = rt * TR;
-  if (i0 >= r || 2 * ct >= ncols) return;
-  double a1[TR][TC], a2[TR][TC];
-#pragma unroll
-  for (int a = 0; a < TR; ++a)
-#pragma unroll
-    for (int b = 0; b < TC; ++b) {
-      a1[a][b] = 0.0;
-      a2[a][b] = 0.0;
-    }
-#pragma unroll 1
-  for (int k = 0; k < r; ++k) {
-    double mv[TR], xv[TC], yv[TC];
-    const double2 *mp = reinterpret_cast<const double2 *>(sM + k * RP + i0);
-#pragma unroll
-    for (int a = 0; a < TR / 2; ++a) {
-      const double2 v = mp[a];
-      mv[2 * a] = v.x;
-      mv[2 * a + 1] = v.y;
-    }
-#pragma unroll
-    for (int q = 0; q < TC / 2; ++q) {
-      const double2 v = *reinterpret_cast<const double2 *>(X1 + k * NCG + 2 * (ct + q * CT));
-      const double2 w = *reinterpret_cast<const double2 *>(X2 + k * NCG + 2 * (ct + q * CT));
-      xv[2 * q] = v.x;
-      xv[2 * q + 1] = v.y;
-      yv[2 * q] = w.x;
-      yv[2 * q + 1] = w.y;
-    }
-#pragma unroll
-    for (int a = 0; a < TR; ++a)
-#pragma unroll
-      for (int b = 0; b < TC; ++b) {
-        a1[a][b] = fmad(mv[a], xv[b], a1[a][b]);
-        a2[a][b] = fmad(mv[a], yv[b], a2[a][b]);
-      }
-  }
-#pragma unroll
-  for (int a = 0; a < TR; ++a) {
-    const int i = i0 + a;
-    if (i >= r) break;
-#pragma unroll
-    for (int b = 0; b < TC; ++b) {
-      const int c = 2 * (ct + (b / 2) * CT) + (b & 1);
-      if (c < ncols) Y[i * NCG + c] = fmad(tabs[i], a2[a][b], a1[a][b]);
-    }
-  }
-}
-
-// P[:, c] <- K^-1 P[:, c] for c < nc on a panel whose rows are already in pivot order (row i holds the
-// original row perm[i]), by the whole thread group: 8-row blocks, each a rectangular update (every thread
-// a 2 x 2 tile, operand pairs as double2) followed by the in-block substitution (one thread per column).
-// Every element receives exactly the fused multiply-adds of lu_solve_reg in the same order — forward
-// k ascending, backward k descending with the reciprocal diagonal applied at k = i — so the result is
-// bit-identical to it; rows r .. RP-1 (padding) are neither read nor written.
-template <int RP, int NCG, int NT, int NG>
-__device__ __forceinline__ void panel_trsm(const double *__restrict__ sLU, double *P, int r, int nc, int t, int g) {
-  const int nblk = (r + 7) >> 3, ncp = (nc + 1) >> 1;
-  for (int J = 0; J < nblk; ++J) {
-    const int j0 = J << 3, j1 = min(r, j0 + 8);
-    if (J > 0) {
-      const int nrp = (j1 - j0 + 1) >> 1;
-      for (int w = t; w < nrp * ncp; w += NT) {
-        const int rp = w / ncp, c = 2 * (w - rp * ncp), i = j0 + 2 * rp;
-        const bool two = i + 1 < j1;
-        double2 a0 = *reinterpret_cast<const double2 *>(P + i * NCG + c);
-        double2 a1 = two ? *reinterpret_cast<const double2 *>(P + (i + 1) * NCG + c) : make_double2(0.0, 0.0);
-#pragma unroll 4
-        for (int k = 0; k < j0; ++k) {
-          const double2 l = *reinterpret_cast<const double2 *>(sLU + k * RP + i);  // L[i][k], L[i+1][k]
-          const double2 x = *reinterpret_cast<const double2 *>(P + k * NCG + c);
-          a0.x = fmad(-l.x, x.x, a0.x);
-          a0.y = fmad(-l.x, x.y, a0.y);
-          a1.x = fmad(-l.y, x.x, a1.x);
-          a1.y = fmad(-l.y, x.y, a1.y);
-        }
-        *reinterpret_cast<double2 *>(P + i * NCG + c) = a0;
-        if (two) *reinterpret_cast<double2 *>(P + (i + 1) * NCG + c) = a1;
-      }
-      group_sync<NG>(g);
-    }
-    for (int c = t; c < nc; c += NT) {
-      double xb[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) xb[q] = (j0 + q < j1) ? P[(j0 + q) * NCG + c] : 0.0;
-#pragma unroll
-      for (int kk = 0; kk < 7; ++kk)
-#pragma unroll
-        for (int q = kk + 1; q < 8; ++q)
-          if (j0 + q < j1) xb[q] = fmad(-sLU[(j0 + kk) * RP + j0 + q], xb[kk], xb[q]);
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-        if (j0 + q < j1) P[(j0 + q) * NCG + c] = xb[q];
-    }
-    group_sync<NG>(g);
-  }
-  const double *dinv = sLU + RP * RP;
-  for (int J = nblk - 1; J >= 0; --J) {
-    const int j0 = J << 3, j1 = min(r, j0 + 8);
-    if (j1 < r) {
-      const int nrp = (j1 - j0 + 1) >> 1;
-      for (int w = t; w < nrp * ncp; w += NT) {
-        const int rp = w / ncp, c = 2 * (w - rp * ncp), i = j0 + 2 * rp;
-        const bool two = i + 1 < j1;
-        double2 a0 = *reinterpret_cast<const double2 *>(P + i * NCG + c);
-        double2 a1 = two ? *reinterpret_cast<const double2 *>(P + (i + 1) * NCG + c) : make_double2(0.0, 0.0);
-#pragma unroll 4
-        for (int k = r - 1; k >= j1; --k) {
-          const double2 u = *reinterpret_cast<const double2 *>(sLU + k * RP + i);  // U[i][k], U[i+1][k]
-          const double2 x = *reinterpret_cast<const double2 *>(P + k * NCG + c);
-          a0.x = fmad(-u.x, x.x, a0.x);
-          a0.y = fmad(-u.x, x.y, a0.y);
-          a1.x = fmad(-u.y, x.x, a1.x);
-          a1.y = fmad(-u.y, x.y, a1.y);
-        }
-        *reinterpret_cast<double2 *>(P + i * NCG + c) = a0;
-        if (two) *reinterpret_cast<double2 *>(P + (i + 1) * NCG + c) = a1;
-      }
-      group_sync<NG>(g);
-    }
-    for (int c = t; c < nc; c += NT) {
-      double xb[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) xb[q] = (j0 + q < j1) ? P[(j0 + q) * NCG + c] : 0.0;
-#pragma unroll
-      for (int kk = 7; kk >= 0; --kk) {
-        if (j0 + kk < j1) {
-          xb[kk] = mul(xb[kk], dinv[j0 + kk]);
-#pragma unroll
-          for (int q = 0; q < kk; ++q) xb[q] = fmad(-sLU[(j0 + kk) * RP + j0 + q], xb[kk], xb[q]);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < 8; ++q)
-        if (j0 + q < j1) P[(j0 + q) * NCG + c] = xb[q];
-    }
-    group_sync<NG>(g);
-  }
-}
-
-// Stage the DLR matrices; sPerm receives the pivot gather (RP ints) followed by its inverse (RP ints: the
-// pivot-order position of tau node t, -1 in the pad).
+// Stage the DLR matrices (global: column stride RP) into shared memory with column stride RP + 8; the
+// reciprocal diagonal follows the LU columns; sPerm receives the pivot gather (RP ints) followed by its
+// inverse (RP ints: the pivot-order position of tau node t, -1 in the pad).
 template <int RP>
 __device__ __forceinline__ void stage_basis(const DevBasis &B, double *sLU, double *sW, double *sBK, int *sPerm) {
-  for (int i = threadIdx.x; i < RP * RP + RP; i += blockDim.x) sLU[i] = B.LUp[i];
-  for (int i = threadIdx.x; i < RP * RP; i += blockDim.x) {
-    sW[i] = B.Wp[i];
-    sBK[i] = B.BKp[i];
+  constexpr int S = mat_stride<RP>();
+  for (int e = threadIdx.x; e < RP * RP; e += blockDim.x) {
+    const int k = e / RP, i = e - k * RP;
+    sLU[k * S + i] = B.LUp[e];
+    sW[k * S + i] = B.Wp[e];
+    sBK[k * S + i] = B.BKp[e];
   }
   for (int i = threadIdx.x; i < RP; i += blockDim.x) {
+    sLU[S * RP + i] = B.LUp[RP * RP + i];
     sPerm[i] = B.perm[i];
     sPerm[RP + i] = B.pinv[i];
   }
   __syncthreads();
 }
 
-// Edge tables (see edge_table_kernel): for block b and signature sig, fc = K^-1 (G_b prod K) and W fc.
-// A CTA takes NC consecutive (sig, entry) columns of one block: gather with the K factors, K^-1, write fc,
-// W fc, write.  `chunks` lists (block, first column) pairs.
+// D = A B + C on one 8 x 8 x 4 tile (a: A[g][q], b: B[q][g], c/d: C[g][2q], C[g][2q + 1], g = lane / 4, q = lane % 4).
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};" : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+// Y[i][c] = sum_{k < r} M[i][k] X1[k][c] (DUAL: Y[i][c] = fma(t_i, (M X2)[i][c], (M X1)[i][c])) for i < r,
+// c < nc.  M is column-major with stride RP + 8 (zero beyond column r); X rows k >= r are masked to zero.
+// Warp w owns the column tiles [w NPW, (w + 1) NPW) and all row tiles.
+template <int RP, bool DUAL>
+__device__ __forceinline__ void panel_mma(const double *__restrict__ sM, const double *__restrict__ X1, const double *__restrict__ X2,
+                                          double *__restrict__ Y, int r, int nc, const double *__restrict__ tabs, int warp, int lane) {
+  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP, MT = RP / 8, NPW = PanelCfg<RP>::NC / (8 * PANEL_WARPS);
+  const int g = lane >> 2, q = lane & 3;
+  const int n0 = warp * NPW;
+  if (n0 * 8 >= nc) return;
+  const int mt = (r + 7) >> 3;
+  double a1[MT][NPW][2], a2[MT][NPW][2];
+#pragma unroll
+  for (int m = 0; m < MT; ++m)
+#pragma unroll
+    for (int t = 0; t < NPW; ++t) {
+      a1[m][t][0] = a1[m][t][1] = 0.0;
+      a2[m][t][0] = a2[m][t][1] = 0.0;
+    }
+  for (int k0 = 0; k0 < r; k0 += 4) {
+    const int k = k0 + q;
+    const bool kv = k < r;
+    double b1[NPW], b2[NPW];
+#pragma unroll
+    for (int t = 0; t < NPW; ++t) {
+      const int c = (n0 + t) * 8 + g;
+      b1[t] = kv ? X1[k * LDP + c] : 0.0;
+      if (DUAL) b2[t] = kv ? X2[k * LDP + c] : 0.0;
+    }
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+      if (m < mt) {
+        const double a = sM[k * S + m * 8 + g];
+#pragma unroll
+        for (int t = 0; t < NPW; ++t) {
+          dmma(a1[m][t][0], a1[m][t][1], a, b1[t]);
+          if (DUAL) dmma(a2[m][t][0], a2[m][t][1], a, b2[t]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < MT; ++m) {
+    const int i = m * 8 + g;
+    if (m < mt && i < r) {
+#pragma unroll
+      for (int t = 0; t < NPW; ++t)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int c = (n0 + t) * 8 + 2 * q + e;
+          if (c < nc) Y[i * LDP + c] = DUAL ? fmad(tabs[i], a2[m][t][e], a1[m][t][e]) : a1[m][t][e];
+        }
+    }
+  }
+}
+
+// P[:, c] <- K^-1 P[:, c] for c < nc on a panel whose rows are already in pivot order (row i holds the
+// original row perm[i]), by the whole CTA, 8-row blocks: the rectangular update of a block by the rows
+// already solved is one MMA row tile per warp column range (A = -L or -U), then the in-block
+// substitution runs one thread per column.  Every element receives exactly the fused multiply-adds of
+// lu_solve_reg in the same order — forward k ascending, backward k descending with the reciprocal
+// diagonal applied at k = i — so the result is bit-identical to it; padding rows are not written.
+template <int RP>
+__device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, double *P, int r, int nc, int tid, int warp, int lane) {
+  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP, NPW = PanelCfg<RP>::NC / (8 * PANEL_WARPS);
+  const int g = lane >> 2, q = lane & 3, n0 = warp * NPW;
+  const bool wact = n0 * 8 < nc;
+  const int nblk = (r + 7) >> 3;
+  for (int J = 0; J < nblk; ++J) {
+    const int j0 = J << 3, j1 = min(r, j0 + 8);
+    if (J > 0) {
+      if (wact) {
+        double acc[NPW][2];
+#pragma unroll
+        for (int t = 0; t < NPW; ++t)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) acc[t][e] = P[(j0 + g) * LDP + (n0 + t) * 8 + 2 * q + e];
+        for (int k0 = 0; k0 < j0; k0 += 4) {
+          const int k = k0 + q;
+          const double a = -sLU[k * S + j0 + g];  // -L[j0 + g][k]
+#pragma unroll
+          for (int t = 0; t < NPW; ++t) dmma(acc[t][0], acc[t][1], a, P[k * LDP + (n0 + t) * 8 + g]);
+        }
+        if (j0 + g < j1)
+#pragma unroll
+          for (int t = 0; t < NPW; ++t)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int c = (n0 + t) * 8 + 2 * q + e;
+              if (c < nc) P[(j0 + g) * LDP + c] = acc[t][e];
+            }
+      }
+      __syncthreads();
+    }
+    for (int c = tid; c < nc; c += PANEL_THREADS) {
+      double xb[8];
+#pragma unroll
+      for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + c] : 0.0;
+#pragma unroll
+      for (int kk = 0; kk < 7; ++kk)
+#pragma unroll
+        for (int qq = kk + 1; qq < 8; ++qq)
+          if (j0 + qq < j1) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+#pragma unroll
+      for (int qq = 0; qq < 8; ++qq)
+        if (j0 + qq < j1) P[(j0 + qq) * LDP + c] = xb[qq];
+    }
+    __syncthreads();
+  }
+  const double *dinv = sLU + S * RP;
+  for (int J = nblk - 1; J >= 0; --J) {
+    const int j0 = J << 3, j1 = min(r, j0 + 8);
+    if (j1 < r) {
+      if (wact) {
+        double acc[NPW][2];
+#pragma unroll
+        for (int t = 0; t < NPW; ++t)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) acc[t][e] = P[(j0 + g) * LDP + (n0 + t) * 8 + 2 * q + e];
+        // k runs from r - 1 down to j1: group kk feeds k = r - 1 - 4 kk - q, so that the MMA's ascending
+        // order inside the group is the descending order of the substitution
+        for (int kh = r - 1; kh >= j1; kh -= 4) {
+          const int k = kh - q;
+          const bool kv = k >= j1;
+          const double a = kv ? -sLU[k * S + j0 + g] : 0.0;  // -U[j0 + g][k]
+#pragma unroll
+          for (int t = 0; t < NPW; ++t) dmma(acc[t][0], acc[t][1], a, kv ? P[k * LDP + (n0 + t) * 8 + g] : 0.0);
+        }
+        if (j0 + g < j1)
+#pragma unroll
+          for (int t = 0; t < NPW; ++t)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int c = (n0 + t) * 8 + 2 * q + e;
+              if (c < nc) P[(j0 + g) * LDP + c] = acc[t][e];
+            }
+      }
+      __syncthreads();
+    }
+    for (int c = tid; c < nc; c += PANEL_THREADS) {
+      double xb[8];
+#pragma unroll
+      for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + c] : 0.0;
+#pragma unroll
+      for (int kk = 7; kk >= 0; --kk) {
+        if (j0 + kk < j1) {
+          xb[kk] = mul(xb[kk], dinv[j0 + kk]);
+#pragma unroll
+          for (int qq = 0; qq < kk; ++qq) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+        }
+      }
+#pragma unroll
+      for (int qq = 0; qq < 8; ++qq)
+        if (j0 + qq < j1) P[(j0 + qq) * LDP + c] = xb[qq];
+    }
+    __syncthreads();
+  }
+}
+
+// Edge tables: for block b and signature sig, fc = K^-1 (G_b prod K) and W fc (sig 0: no factor;
+// 1 + s p + l: one factor, s = 0: K(t, +beta w_l), 1: K(t, -beta w_l); 1 + 2p + (s1 p + l1) 2p + s2 p + l2:
+// two factors, the lower line's first).  A CTA takes NC consecutive (sig, entry) columns of one block:
+// gather with the K factors (rows in pivot order), K^-1, write fc, W fc, write.  `chunks` lists
+// (block, first column) pairs.
 template <int RP>
 __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(DevBasis B, const double *__restrict__ G,
                                                                               const int2 *__restrict__ chunks, int n_chunks) {
-  constexpr int NC = PanelCfg<RP>::NC;
+  constexpr int NCU = PanelCfg<RP>::NC, LDP = PanelCfg<RP>::LDP;
   extern __shared__ double smem[];
-  double *sLU = smem, *sW = sLU + RP * RP + RP, *sBK = sW + RP * RP;
-  double *PA = sBK + RP * RP, *PB = PA + RP * NC;
-  int *sPerm = reinterpret_cast<int *>(PB + RP * NC);
+  double *sLU, *sW, *sBK, *PA;
+  ItemState *ist;
+  int *sPerm;
+  panel_layout<RP>(smem, sLU, sW, sBK, PA, ist, sPerm);
+  double *PB = PA + RP * LDP;
   stage_basis<RP>(B, sLU, sW, sBK, sPerm);
-  const int r = B.r, p = B.p;
+  const int r = B.r, p = B.p, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   for (int ch = blockIdx.x; ch < n_chunks; ch += gridDim.x) {
     const int b = chunks[ch].x, col0 = chunks[ch].y;
     const int d = B.dims[b], dd = d * d;
     const long total = (long)B.nsig * dd;
-    const int ncols = (int)min((long)NC, total - col0);
+    const int ncols = (int)min((long)NCU, total - col0);
     const double *g = G + B.goff[b];
-    // gather: column c is (sig, e) = divmod(col0 + c, dd); rows are the tau nodes
-    for (int idx = threadIdx.x; idx < r * ncols; idx += PANEL_THREADS) {
+    for (int idx = tid; idx < r * ncols; idx += PANEL_THREADS) {
       const int t = idx / ncols, c = idx - t * ncols;
-      const long q = col0 + c;
-      const int sig = (int)(q / dd), e = (int)(q - (long)sig * dd);
+      const long qc = col0 + c;
+      const int sig = (int)(qc / dd), e = (int)(qc - (long)sig * dd);
       int nf = 0, s1 = 0, l1 = 0, s2 = 0, l2 = 0;
       if (sig >= 1 && sig < 1 + 2 * p) {
         nf = 1;
@@ -311,54 +288,48 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(Dev
       double v = g[t * dd + e];
       if (nf >= 1) v = mul(v, (s1 ? B.kitm : B.kitp)[(size_t)t * p + l1]);
       if (nf >= 2) v = mul(v, (s2 ? B.kitm : B.kitp)[(size_t)t * p + l2]);
-      PA[sPerm[RP + t] * NC + c] = v;
+      PA[sPerm[RP + t] * LDP + c] = v;
     }
     __syncthreads();
-    panel_trsm<RP, NC, PANEL_THREADS, 1>(sLU, PA, r, ncols, threadIdx.x, 0);
-    panel_gemm<RP, 1, false>(sW, PA, PB, r, ncols, nullptr, nullptr, threadIdx.x);
+    panel_trsm_mma<RP>(sLU, PA, r, ncols, tid, warp, lane);
+    panel_mma<RP, false>(sW, PA, nullptr, PB, r, ncols, nullptr, warp, lane);
     __syncthreads();
     double *out = const_cast<double *>(B.tab) + B.tab_off[b];
-    for (int idx = threadIdx.x; idx < r * ncols; idx += PANEL_THREADS) {
+    for (int idx = tid; idx < r * ncols; idx += PANEL_THREADS) {
       const int t = idx / ncols, c = idx - t * ncols;
-      const long q = col0 + c;
-      const long sig = q / dd, e = q - sig * dd;
+      const long qc = col0 + c;
+      const long sig = qc / dd, e = qc - sig * dd;
       double *o = out + sig * 2 * r * dd;
-      o[t * dd + e] = PA[t * NC + c];
-      o[(long)r * dd + t * dd + e] = PB[t * NC + c];
+      o[t * dd + e] = PA[t * LDP + c];
+      o[(long)r * dd + t * dd + e] = PB[t * LDP + c];
     }
     __syncthreads();
   }
 }
 
-// Dynamic shared memory: LU (+ reciprocal diagonal) | W | BK (column-major) | per thread group: panels A, B,
-// C (RP x NC / NG each) | per thread group: item states (PANEL_BMAX / NG) | perm (RP ints).  The NG thread
-// groups of the CTA run independent work loops (own units, batches and barriers) over the shared DLR
-// matrices, so that one group's substitution phase overlaps another group's products.
-template <int RP, int NG>
+// Dynamic shared memory: see panel_smem_doubles.
+template <int RP>
 __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis B, const ClassRec *__restrict__ classes,
                                                                         const WorkUnit *__restrict__ units, int n_units,
                                                                         int *__restrict__ unit_counter, const double *__restrict__ G,
                                                                         double *__restrict__ Sigma, double scale) {
-  using GP = PanelGrp<RP, NG>;
-  constexpr int NC = GP::NCG, NT = GP::NT, BG = PANEL_BMAX / NG;
+  constexpr int NC = PanelCfg<RP>::LDP, NCU = PanelCfg<RP>::NC, NT = PANEL_THREADS;  // NC: panel row stride
   extern __shared__ double smem[];
-  double *sLU = smem, *sW = sLU + RP * RP + RP, *sBK = sW + RP * RP;
-  const int g = threadIdx.x / NT, tid = threadIdx.x - g * NT;
-  double *PA = sBK + RP * RP + (size_t)g * 3 * RP * NC, *PB = PA + RP * NC, *PC = PB + RP * NC;
-  ItemState *ist = reinterpret_cast<ItemState *>(sBK + RP * RP + (size_t)3 * RP * NC * NG) + g * BG;
-  int *sPerm = reinterpret_cast<int *>(sBK + RP * RP + (size_t)3 * RP * NC * NG + (sizeof(ItemState) * PANEL_BMAX + 7) / 8);
-  __shared__ int s_unit_all[NG];
-  __shared__ unsigned long long s_max_all[PANEL_BMAX];
-  int &s_unit = s_unit_all[g];
-  unsigned long long *s_max = s_max_all + g * BG;
+  double *sLU, *sW, *sBK, *PA;
+  ItemState *ist;
+  int *sPerm;
+  panel_layout<RP>(smem, sLU, sW, sBK, PA, ist, sPerm);
+  double *PB = PA + RP * NC, *PC = PB + RP * NC;
+  __shared__ int s_unit;
+  __shared__ unsigned long long s_max[PANEL_BMAX];
   stage_basis<RP>(B, sLU, sW, sBK, sPerm);
-  const int r = B.r, p = B.p, n = B.n;
+  const int r = B.r, p = B.p, n = B.n, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   while (true) {
     if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
-    group_sync<NG>(g);
+    __syncthreads();
     const int u = s_unit;
-    group_sync<NG>(g);
+    __syncthreads();
     if (u >= n_units) break;
     const WorkUnit wu = units[u];
     const ClassRec &C = classes[wu.cls];
@@ -405,7 +376,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           for (int t = t0; t < r; t += tpc) T[t * NC + c] = g[t * dc + e];
         }
       }
-      group_sync<NG>(g);
+      __syncthreads();
 
       // op order: for v < vct0: vertex v, edge v; zero vertex; for v > vct0: edge v - 1, vertex v
       const int pre = 2 * (vct0 - 1);
@@ -449,7 +420,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
               S.kneg = ks < 0;
             }
           }
-          group_sync<NG>(g);
+          __syncthreads();
           const int dci = dv * ncol, dco = dvp * ncol, nc = nbi * dco, tpc = NT / nc, c = tid % nc, t0 = tid / nc;
           if (t0 < tpc) {
             const int j = c / dco, e = c - j * dco, x = e / ncol, z = e - x * ncol;
@@ -465,7 +436,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
               X[(rowpos ? rowpos[t] : t) * NC + c] = a;
             }
           }
-          group_sync<NG>(g);
+          __syncthreads();
           double *tmp = T; T = X; X = tmp;
         } else if (kind == 1) {
           // ---- edge e: T <- conv(G_b prod K, T)  (integrate_left_edge, time-ordered convolution)
@@ -488,14 +459,13 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
             S.taboff = B.tab_off[b] + sig * 2 * r * dd;
           }
           // (a) gc = K^-1 T (in place), then Gt = W gc (into X)
-          panel_trsm<RP, NC, NT, NG>(sLU, T, r, nc, tid, g);
-          panel_gemm<RP, NG, false>(sW, T, X, r, nc, nullptr, nullptr, tid);
-          group_sync<NG>(g);
+          panel_trsm_mma<RP>(sLU, T, r, nc, tid, warp, lane);
+          panel_mma<RP, false>(sW, T, nullptr, X, r, nc, nullptr, warp, lane);
+          __syncthreads();
           // (b) per row l (one warp per row; Q and P' of row l read only row l of gc and Gt):
           //     Q_l = Ft_l gc_l + fc_l Gt_l (into Y) and P'_l = K(0, om_l) (fc_l gc_l) (over Gt, into X)
           {
-            constexpr int CPL = (NC + 31) / 32;
-            const int lane = tid & 31, warp = tid >> 5;
+            constexpr int CPL = (NCU + 31) / 32;
             const double *tbq[CPL];
             int coff[CPL];
             bool cval[CPL];
@@ -534,10 +504,10 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
                 }
             }
           }
-          group_sync<NG>(g);
+          __syncthreads();
           // (c) h = fma(t_i, (beta K) P', (beta K) Q) (into T; gc is no longer needed)
-          panel_gemm2<RP, NG>(sBK, Y, X, T, r, nc, B.tabs, tid);
-          group_sync<NG>(g);
+          panel_mma<RP, true>(sBK, Y, X, T, r, nc, B.tabs, warp, lane);
+          __syncthreads();
         } else {
           // ---- zero vertex (multiply_left_vertex_and_right_zero_vertex)
           const int b_mu = C.ind_path[v - 1];
@@ -556,7 +526,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           const int tpm = NT / ncm, cm = tid % ncm, tm0 = tid / ncm;
           if (to0 < tpo)
             for (int t = to0; t < r; t += tpo) X[(rowpos ? rowpos[t] : t) * NC + co] = 0.0;
-          group_sync<NG>(g);
+          __syncthreads();
           for (int mu = 0; mu < qs; ++mu) {
             const int om = B.set_to_orb[pk * n + mu];
             if (tm0 < tpm) {
@@ -577,7 +547,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
                 Y[t * NC + c] = a;
               }
             }
-            group_sync<NG>(g);
+            __syncthreads();
             const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
             if (to0 < tpo) {
               const int c = co, j = c / dco, ee = c - j * dco, x = ee / d0, z = ee - x * d0;
@@ -590,7 +560,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
                 X[row * NC + c] = add(X[row * NC + c], a);
               }
             }
-            group_sync<NG>(g);
+            __syncthreads();
           }
           double *tmp = T; T = X; X = tmp;
         }
@@ -607,7 +577,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           atomicMax(&s_max[j], (unsigned long long)__double_as_longlong(mx));  // non-negative doubles order as integers
         }
       }
-      group_sync<NG>(g);
+      __syncthreads();
       double *dst = Sigma + B.goff[C.b_out];
       for (int idx = tid; idx < r * dco; idx += NT) {
         const int t = idx / dco, ee = idx - t * dco;
@@ -620,7 +590,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           }
         if (keep_any) atomicAdd(dst + idx, mul(scale, a));
       }
-      group_sync<NG>(g);
+      __syncthreads();
     }
   }
 }

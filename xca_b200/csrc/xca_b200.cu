@@ -292,8 +292,6 @@ static long ipow(long a, int e) {
 // Validity of a block path depends on the directions, the orbital tuple, the output block, the
 // symmetry set and the zero-block flags of G, never on the pole tuple, so it is enumerated once per
 // (topology, zero pattern) and every valid path class stands for p^(m-1) items.
-// Independent thread groups per Sigma CTA (each with its own panel slice and work loop).
-constexpr int SIGMA_GROUPS = 1;
 
 static int panel_nc_host(int RP) { return RP == 32 ? panel_nc<32>() : (RP == 48 ? panel_nc<48>() : panel_nc<64>()); }
 
@@ -395,11 +393,11 @@ static std::unique_ptr<ClassSet> build_classes(Ctx *c, const Topology &T, const 
             int mxb = 0;
             for (int i = 1; i <= nv; ++i) mxb = std::max(mxb, bd[i]);
             R.dcmax = mxb * std::max(bd[0], bd[1]);
-            const int nc = panel_nc_host(c->RP) / SIGMA_GROUPS;
+            const int nc = panel_nc_host(c->RP);
             if (R.dcmax > nc)
               throw Error(XCA_ERR_UNSUPPORTED, "block chain too wide for the panel kernel (" + std::to_string(R.dcmax) +
                                                    " entries per item, panel width " + std::to_string(nc) + ")");
-            R.batch = std::min(PANEL_BMAX / SIGMA_GROUPS, nc / R.dcmax);
+            R.batch = std::min(PANEL_BMAX, nc / R.dcmax);
           }
           for (int v = 0; v < nv; ++v) {
             R.vline[v] = vline[v];
@@ -476,12 +474,12 @@ template <int RP>
 static void launch_sigma_rp(Ctx *c, const DevBasis &B, const ClassRec *d_classes, const WorkUnit *d_units, int n_units, int *counter,
                             const double *G_dev, double *Sig_dev, double scale) {
   const size_t smem = panel_smem_doubles<RP>() * sizeof(double);
-  CUDA_CHECK(cudaFuncSetAttribute(sigma_panel_kernel<RP, SIGMA_GROUPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUDA_CHECK(cudaFuncSetAttribute(sigma_panel_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  const int grid = std::max(1, std::min(nsm, (n_units + SIGMA_GROUPS - 1) / SIGMA_GROUPS));
-  sigma_panel_kernel<RP, SIGMA_GROUPS><<<grid, PANEL_THREADS, smem, c->stream>>>(B, d_classes, d_units, n_units, counter, G_dev,
+  const int grid = std::max(1, std::min(nsm, n_units));
+  sigma_panel_kernel<RP><<<grid, PANEL_THREADS, smem, c->stream>>>(B, d_classes, d_units, n_units, counter, G_dev,
                                                                                  Sig_dev, scale);
   c->launches++;
   CUDA_CHECK(cudaGetLastError());
