@@ -102,7 +102,7 @@ class ClockSampler:
 
 def profiled_traffic():
     """DRAM bytes (read + write) per Sigma-kernel launch of this workload from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "sigma_items_kernel_kanamori_2orb_tca.md")
+    path = os.path.join(ROOT, "profiles", "sigma_panel_kernel_kanamori_2orb_tca.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -254,7 +254,9 @@ def main():
         e2e = {"value": 1.0 / te, "unit": UNIT, "h2d_bytes_per_step": int(len(topos) * ev.slab * 8),
                "d2h_bytes_per_step": int(len(topos) * ev.slab * 8)}
 
-    peak = ev.fp64_fma_peak()
+    peak_fma = ev.fp64_fma_peak()
+    peak_mma = ev.fp64_mma_peak()
+    peak = max(peak_fma, peak_mma)
     kernel_s = sigma_ms * 1e-3 / max(args.steps, 1)
     achieved = alg_flops / world / kernel_s / 1e12 if kernel_s > 0 else None
     traffic = profiled_traffic()
@@ -270,8 +272,10 @@ def main():
                           "alg_gflop_per_step": alg_flops / 1e9, "l2": "flushed (256 MiB write) before every timed step"},
                "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                            "kernel": "sigma_items_kernel",
-                            "peak_source": "FP64 FMA throughput measured by xca_fp64_fma_probe on this GPU",
+                            "kernel": "sigma_panel_kernel",
+                            "peak_source": "max of the FP64 FMA (xca_fp64_fma_probe) and FP64 tensor-core MMA "
+                                           "(xca_fp64_mma_probe) throughputs measured on this GPU",
+                            "peak_fp64_fma": peak_fma, "peak_fp64_mma": peak_mma,
                             "kernel_ms_per_step": sigma_ms / max(args.steps, 1), "launches_per_step": sigma_launches / max(args.steps, 1)},
                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
         print(json.dumps(out), flush=True)

@@ -188,6 +188,16 @@ int xca_flush_l2(xca_ctx *ctx, long bytes);
 /* Measurement support: FP64 fused-multiply-add throughput of this device in TFLOP/s (2 flops per FMA). */
 int xca_fp64_fma_probe(xca_ctx *ctx, double *tflops);
 
+/* Measurement support (no counterpart in the reference): FP64 tensor-core (mma.sync m8n8k4 f64)
+ * throughput of this device in TFLOP/s (2 flops per multiply-add). */
+int xca_fp64_mma_probe(xca_ctx *ctx, double *tflops);
+
+/* Validation support (no counterpart in the reference): the panel kernels' products run on the FP64
+ * tensor cores and rely on one MMA computing each element as four correctly rounded fused multiply-adds
+ * in ascending k.  This checks that on the device over n_tiles random 8 x 8 x 4 tiles (every fourth one
+ * cancelling) and returns the number of elements whose bits differ from the scalar chain (expected 0). */
+int xca_fp64_mma_selftest(xca_ctx *ctx, long n_tiles, unsigned long long seed, long *mismatches);
+
 /* Size in bytes of the packed real slab of the evaluator's blocks, and its rank r. */
 int xca_slab_info(xca_ctx *ctx, long *n_doubles, int *r);
 

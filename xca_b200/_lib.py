@@ -61,6 +61,8 @@ SIGNATURES = {
     "xca_event_elapsed": [P, I, I, dp],
     "xca_flush_l2": [P, L],
     "xca_fp64_fma_probe": [P, dp],
+    "xca_fp64_mma_probe": [P, dp],
+    "xca_fp64_mma_selftest": [P, L, ctypes.c_ulonglong, lp],
     "xca_slab_info": [P, lp, ip],
     "xca_device_buffer": [P, I, L, dpp],
     "xca_copy_to_device": [P, P, dp, L],

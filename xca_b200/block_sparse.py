@@ -308,6 +308,12 @@ class DiagramEvaluator:
         _lib.check(_lib.lib().xca_fp64_fma_probe(self._ctx, ctypes.byref(out)))
         return out.value
 
+    def fp64_mma_peak(self):
+        """Measured FP64 tensor-core (mma.sync m8n8k4 f64) throughput of the device in TFLOP/s."""
+        out = ctypes.c_double()
+        _lib.check(_lib.lib().xca_fp64_mma_probe(self._ctx, ctypes.byref(out)))
+        return out.value
+
     def flush_l2(self, nbytes=256 << 20):
         _lib.check(_lib.lib().xca_flush_l2(self._ctx, int(nbytes)))
 

@@ -91,6 +91,66 @@ __global__ void fp64_fma_probe_kernel(double *out, int iters, double x, double y
   if (s == 1.2345678e300) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// FP64 MMA throughput probe (measurement support): 8 independent 8 x 8 x 4 accumulations per warp.
+__global__ void fp64_mma_probe_kernel(double *out, int iters, double x, double y) {
+  const double a = x + 1e-3 * (threadIdx.x & 31), b = y;
+  double c[8][2];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) c[j][0] = c[j][1] = 0.0;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dmma(c[j][0], c[j][1], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += c[j][0] + c[j][1];
+  if (s == 1.2345678e300) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// Deterministic test value of (tile, array, index): a splitmix64 hash mapped to +-[0, 1) * 2^[-7, 8].
+__device__ __forceinline__ double selftest_value(unsigned long long seed, long tile, int arr, int idx) {
+  unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(tile * 4 + arr + 1) + 0xD1B54A32D192ED03ull * (unsigned long long)(idx + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  const double u = (double)(z >> 11) * 0x1.0p-53 * 2.0 - 1.0;
+  return scalbn(u, (int)((z >> 3) & 15) - 7);
+}
+
+// Check that one FP64 MMA computes every element as four fused multiply-adds in ascending k, each
+// correctly rounded (the operation order the panel kernels rely on): per 8 x 8 x 4 tile, random A, B, C
+// (every fourth tile with C cancelling A B), mma.sync against the scalar chain, mismatching bit patterns
+// counted.
+__global__ void fp64_mma_selftest_kernel(long n_tiles, unsigned long long seed, unsigned long long *mismatches) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+  unsigned long long bad = 0;
+  for (long tile = warp; tile < n_tiles; tile += nwarps) {
+    double c[2];
+    for (int e = 0; e < 2; ++e) {
+      const int j = 2 * q + e;
+      if ((tile & 3) == 0) {
+        double sp = 0.0;
+        for (int k = 0; k < 4; ++k)
+          sp = __dadd_rn(sp, __dmul_rn(selftest_value(seed, tile, 0, g * 4 + k), selftest_value(seed, tile, 1, k * 8 + j)));
+        c[e] = -sp * (1.0 + 1e-9 * selftest_value(seed, tile, 2, g * 8 + j));
+      } else {
+        c[e] = (g + j) % 3 == 0 ? 0.0 : selftest_value(seed, tile, 2, g * 8 + j);
+      }
+    }
+    double d0 = c[0], d1 = c[1];
+    dmma(d0, d1, selftest_value(seed, tile, 0, g * 4 + q), selftest_value(seed, tile, 1, q * 8 + g));
+    const double d[2] = {d0, d1};
+    for (int e = 0; e < 2; ++e) {
+      const int j = 2 * q + e;
+      double ref = c[e];
+      for (int k = 0; k < 4; ++k) ref = __fma_rn(selftest_value(seed, tile, 0, g * 4 + k), selftest_value(seed, tile, 1, k * 8 + j), ref);
+      if (__double_as_longlong(ref) != __double_as_longlong(d[e])) ++bad;
+    }
+  }
+  if (bad) atomicAdd(mismatches, bad);
+}
+
 __global__ void zero_kernel(double *x, long n) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) x[i] = 0.0;
 }
@@ -1614,6 +1674,51 @@ int xca_fp64_fma_probe(xca_ctx *ctx, double *tflops) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *tflops = 5.0 * 2.0 * 8.0 * iters * (double)blocks * threads / (ms * 1e-3) / 1e12;
+  API_END
+}
+
+int xca_fp64_mma_probe(xca_ctx *ctx, double *tflops) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  set_device(c);
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  const int blocks = nsm * 4, threads = 256, iters = 4096;
+  c->d_flush.resize((size_t)blocks * threads);
+  cudaEvent_t e0, e1;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  fp64_mma_probe_kernel<<<blocks, threads, 0, c->stream>>>(c->d_flush.ptr, iters, 0.999999, 1e-7);
+  CUDA_CHECK(cudaEventRecord(e0, c->stream));
+  for (int rep = 0; rep < 5; ++rep) fp64_mma_probe_kernel<<<blocks, threads, 0, c->stream>>>(c->d_flush.ptr, iters, 0.999999, 1e-7);
+  CUDA_CHECK(cudaEventRecord(e1, c->stream));
+  CUDA_CHECK(cudaEventSynchronize(e1));
+  float ms = 0;
+  CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // 8 MMAs of 8 x 8 x 4 (512 flops) per warp and iteration
+  *tflops = 5.0 * 8.0 * 512.0 * iters * ((double)blocks * threads / 32) / (ms * 1e-3) / 1e12;
+  API_END
+}
+
+int xca_fp64_mma_selftest(xca_ctx *ctx, long n_tiles, unsigned long long seed, long *mismatches) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  set_device(c);
+  if (n_tiles < 1) throw Error(XCA_ERR_INVALID, "n_tiles must be positive");
+  DevBuf<unsigned long long> cnt;
+  cnt.resize(1);
+  CUDA_CHECK(cudaMemsetAsync(cnt.ptr, 0, sizeof(unsigned long long), c->stream));
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  fp64_mma_selftest_kernel<<<nsm * 4, 256, 0, c->stream>>>(n_tiles, seed, cnt.ptr);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+  unsigned long long h = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&h, cnt.ptr, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  *mismatches = (long)h;
   API_END
 }
 
