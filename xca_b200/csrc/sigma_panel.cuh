@@ -21,7 +21,7 @@
 
 namespace xca {
 
-constexpr int PANEL_THREADS = 256;
+constexpr int PANEL_THREADS = 512;
 constexpr int PANEL_WARPS = PANEL_THREADS / 32;
 constexpr int PANEL_BMAX = 128;  // items per batch at most
 
@@ -31,7 +31,7 @@ constexpr int PANEL_BMAX = 128;  // items per batch at most
 template <int RP>
 struct PanelCfg;
 template <>
-struct PanelCfg<32> { static constexpr int NC = 192, LDP = 200; };
+struct PanelCfg<32> { static constexpr int NC = 128, LDP = 136; };
 template <>
 struct PanelCfg<48> { static constexpr int NC = 128, LDP = 136; };
 template <>
@@ -39,6 +39,19 @@ struct PanelCfg<64> { static constexpr int NC = 64, LDP = 72; };
 
 template <int RP>
 __host__ __device__ constexpr int mat_stride() { return RP + 8; }
+
+// Warp tiling of the MMA products: NTL column tiles and MT row tiles of 8; each warp owns NPW column tiles
+// and MPG row tiles (the row tiles are split into MG groups when there are fewer column tiles than warps).
+template <int RP>
+struct MmaMap {
+  static constexpr int NTL = PanelCfg<RP>::NC / 8, MT = RP / 8;
+  static constexpr int NPW = NTL >= PANEL_WARPS ? NTL / PANEL_WARPS : 1;
+  static constexpr int MG = NTL >= PANEL_WARPS ? 1 : PANEL_WARPS / NTL;
+  static constexpr int MPG = MT / MG;
+  static_assert(NTL >= PANEL_WARPS ? NTL % PANEL_WARPS == 0 : (PANEL_WARPS % NTL == 0 && MT % MG == 0), "MMA warp tiling");
+  __device__ static int n0(int warp) { return MG == 1 ? warp * NPW : warp % NTL; }
+  __device__ static int m0(int warp) { return MG == 1 ? 0 : (warp / NTL) * MPG; }
+};
 
 template <int RP>
 __host__ __device__ constexpr int panel_nc() { return PanelCfg<RP>::NC; }
@@ -89,15 +102,16 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 
 // Y[i][c] = sum_{k < r} M[i][k] X1[k][c] (DUAL: Y[i][c] = fma(t_i, (M X2)[i][c], (M X1)[i][c])) for i < r,
 // c < nc.  M is column-major with stride RP + 8 (zero beyond column r); X rows k >= r are masked to zero.
-// Warp w owns the column tiles [w NPW, (w + 1) NPW) and all row tiles.
+// Warps own column and row tiles as MmaMap lays them out.
 template <int RP, bool DUAL>
 __device__ __forceinline__ void panel_mma(const double *__restrict__ sM, const double *__restrict__ X1, const double *__restrict__ X2,
                                           double *__restrict__ Y, int r, int nc, const double *__restrict__ tabs, int warp, int lane) {
-  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP, MT = RP / 8, NPW = PanelCfg<RP>::NC / (8 * PANEL_WARPS);
+  using MM = MmaMap<RP>;
+  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP, MT = MM::MPG, NPW = MM::NPW;
   const int g = lane >> 2, q = lane & 3;
-  const int n0 = warp * NPW;
+  const int n0 = MM::n0(warp), mb = MM::m0(warp);
   if (n0 * 8 >= nc) return;
-  const int mt = (r + 7) >> 3;
+  const int mt = ((r + 7) >> 3) - mb;
   double a1[MT][NPW][2], a2[MT][NPW][2];
 #pragma unroll
   for (int m = 0; m < MT; ++m)
@@ -119,7 +133,7 @@ __device__ __forceinline__ void panel_mma(const double *__restrict__ sM, const d
 #pragma unroll
     for (int m = 0; m < MT; ++m) {
       if (m < mt) {
-        const double a = sM[k * S + m * 8 + g];
+        const double a = sM[k * S + (mb + m) * 8 + g];
 #pragma unroll
         for (int t = 0; t < NPW; ++t) {
           dmma(a1[m][t][0], a1[m][t][1], a, b1[t]);
@@ -130,7 +144,7 @@ __device__ __forceinline__ void panel_mma(const double *__restrict__ sM, const d
   }
 #pragma unroll
   for (int m = 0; m < MT; ++m) {
-    const int i = m * 8 + g;
+    const int i = (mb + m) * 8 + g;
     if (m < mt && i < r) {
 #pragma unroll
       for (int t = 0; t < NPW; ++t)
@@ -151,9 +165,10 @@ __device__ __forceinline__ void panel_mma(const double *__restrict__ sM, const d
 // diagonal applied at k = i — so the result is bit-identical to it; padding rows are not written.
 template <int RP>
 __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, double *P, int r, int nc, int tid, int warp, int lane) {
-  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP, NPW = PanelCfg<RP>::NC / (8 * PANEL_WARPS);
-  const int g = lane >> 2, q = lane & 3, n0 = warp * NPW;
-  const bool wact = n0 * 8 < nc;
+  using MM = MmaMap<RP>;
+  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP, NPW = MM::NPW;
+  const int g = lane >> 2, q = lane & 3, n0 = MM::n0(warp);
+  const bool wact = (MM::MG == 1 || warp < MM::NTL) && n0 * 8 < nc;  // one row tile: the first row group's warps
   const int nblk = (r + 7) >> 3;
   for (int J = 0; J < nblk; ++J) {
     const int j0 = J << 3, j1 = min(r, j0 + 8);
