@@ -150,3 +150,19 @@ def test_shards_partition_the_work(n_shards):
     a = dev.unpack(dev.to_host(part, dev.slab))
     b = dev.unpack(dev.to_host(full, dev.slab))
     assert _node_rel_err(a, b) <= 1.0
+
+
+def test_t2g_three_orbital_subset():
+    # three-orbital t2g Kanamori (U = 3, J = 0.3, beta = 50, Lambda = 500, eps = 1e-10; 16 blocks up to 9 x 9,
+    # orbital-off-diagonal hybridization) on a seeded subset of flat indices of every topology
+    d = O.Dlr(500.0, 1e-10)
+    m = models.t2g_3orb(d.rf, d.it)
+    G = models.seeded_G(m, 0)
+    dev, ora = _pair(m, d)
+    rng = np.random.default_rng(13)
+    for topo in TOPOS:
+        nmax = ora.num_self_energy_backbones(np.array(topo))
+        fix = np.sort(rng.choice(nmax, size=min(nmax, 300), replace=False))
+        a = dev.compute_self_energy(G, topo, f_ix=fix)
+        b = ora.compute_self_energy(G, topo, f_ix=fix)
+        assert _node_rel_err(a, b) <= 1.0, topo
