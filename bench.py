@@ -38,6 +38,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-API measurement (profiling runs)")
+    ap.add_argument("--serving", action="store_true",
+                    help="instead of the Sigma metric: a Poisson stream of whole self-consistent solves through the solve server")
+    ap.add_argument("--serving-requests", type=int, default=64)
     return ap.parse_args()
 
 
@@ -142,6 +145,48 @@ def cpu_sigma_rate(m, G, seconds, nthreads=0):
     return 1.0 / total_time, threads, f"{sampled} random flat indices over {len(topos)} topologies, extrapolated to {sum(nmax)}"
 
 
+def run_serving(args):
+    """Served solves/s and p50 / p99 time to converged solve for a mixed request stream: Poisson arrivals
+    (mean gap 5 ms, numpy default_rng(2)); each request draws a single-orbital Anderson (orders 1-3) or a
+    two-orbital Kanamori model (orders 1-2), beta in {10, 20, 50, 100}, Lambda = 10 beta, eps = 1e-10,
+    U ~ U(1, 6), tolerance 1e-8; up to 8 solves run concurrently, each with its own context and stream."""
+    from xca_b200.serving import SolveServer, synthetic_request
+    rng = np.random.default_rng(2)
+    n = args.serving_requests
+    gaps = rng.exponential(0.005, n)
+    reqs = []
+    for i in range(n):
+        kind = "anderson" if rng.random() < 0.5 else "kanamori"
+        beta = float(rng.choice([10.0, 20.0, 50.0, 100.0]))
+        U = float(rng.uniform(1.0, 6.0))
+        order = int(rng.integers(1, 4)) if kind == "anderson" else int(rng.integers(1, 3))
+        reqs.append(synthetic_request(kind, beta, U, order, tag=(kind, beta, order)))
+    srv = SolveServer(max_concurrent=8)
+    for kind, order in (("anderson", 3), ("kanamori", 2)):  # warm-up: module load and first-use set-up
+        srv.submit(synthetic_request(kind, 10.0, 2.0, order)).result()
+    t0 = time.perf_counter()
+    futs = []
+    t_next = t0
+    for req, gap in zip(reqs, gaps):
+        t_next += gap
+        wait = t_next - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        futs.append(srv.submit(req))
+    res = [f.result() for f in futs]
+    t1 = max(r.t_done for r in res)
+    srv.shutdown()
+    lat = np.array([r.latency for r in res])
+    out = {"metric": "served solves/s (FP64 plain, mixed stream)", "value": n / (t1 - t0), "unit": "solves/s", "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "poisson_stream", "requests": n, "mean_gap_ms": 5.0, "max_concurrent": 8,
+                      "models": "anderson orders 1-3, kanamori_2orb orders 1-2", "beta": [10, 20, 50, 100], "tol": 1e-8},
+           "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+           "mean_iterations": float(np.mean([r.n_iter for r in res])),
+           "converged": int(sum(r.diff_G < 1e-8 for r in res)), "wall_s": t1 - t0}
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args, rank):
     """--impl reference: the CPU restatement of the reference's path on the host cores."""
     if rank != 0:
@@ -170,6 +215,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.serving:
+        if rank == 0:
+            run_serving(args)
         return
     import torch
     dist = None
