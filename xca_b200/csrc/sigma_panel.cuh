@@ -158,11 +158,12 @@ __device__ __forceinline__ void panel_mma(const double *__restrict__ sM, const d
 }
 
 // P[:, c] <- K^-1 P[:, c] for c < nc on a panel whose rows are already in pivot order (row i holds the
-// original row perm[i]), by the whole CTA, 8-row blocks: the rectangular update of a block by the rows
-// already solved is one MMA row tile per warp column range (A = -L or -U), then the in-block
-// substitution runs one thread per column.  Every element receives exactly the fused multiply-adds of
-// lu_solve_reg in the same order — forward k ascending, backward k descending with the reciprocal
-// diagonal applied at k = i — so the result is bit-identical to it; padding rows are not written.
+// original row perm[i]).  Columns are independent, so each warp solves its own column tiles alone, with
+// no CTA barrier until the end: per 8-row block, the rectangular update by the rows already solved is an
+// MMA chain on the warp's tiles (A = -L or -U), then one lane per column runs the in-block
+// substitution.  Every element receives exactly the fused multiply-adds of lu_solve_reg in the same
+// order — forward k ascending, backward k descending with the reciprocal diagonal applied at k = i — so
+// the result is bit-identical to it; padding rows are not written.
 template <int RP>
 __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, double *P, int r, int nc, int tid, int warp, int lane) {
   using MM = MmaMap<RP>;
@@ -170,10 +171,13 @@ __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, d
   const int g = lane >> 2, q = lane & 3, n0 = MM::n0(warp);
   const bool wact = (MM::MG == 1 || warp < MM::NTL) && n0 * 8 < nc;  // one row tile: the first row group's warps
   const int nblk = (r + 7) >> 3;
-  for (int J = 0; J < nblk; ++J) {
-    const int j0 = J << 3, j1 = min(r, j0 + 8);
-    if (J > 0) {
-      if (wact) {
+  const double *dinv = sLU + S * RP;
+  const int cs = n0 * 8 + lane;  // the column this lane substitutes in-block (lanes < 8 NPW)
+  const bool sact = lane < 8 * NPW && cs < nc;
+  if (wact) {
+    for (int J = 0; J < nblk; ++J) {
+      const int j0 = J << 3, j1 = min(r, j0 + 8);
+      if (J > 0) {
         double acc[NPW][2];
 #pragma unroll
         for (int t = 0; t < NPW; ++t)
@@ -193,29 +197,26 @@ __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, d
               const int c = (n0 + t) * 8 + 2 * q + e;
               if (c < nc) P[(j0 + g) * LDP + c] = acc[t][e];
             }
+        __syncwarp();
       }
-      __syncthreads();
+      if (sact) {
+        double xb[8];
+#pragma unroll
+        for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + cs] : 0.0;
+#pragma unroll
+        for (int kk = 0; kk < 7; ++kk)
+#pragma unroll
+          for (int qq = kk + 1; qq < 8; ++qq)
+            if (j0 + qq < j1) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+#pragma unroll
+        for (int qq = 0; qq < 8; ++qq)
+          if (j0 + qq < j1) P[(j0 + qq) * LDP + cs] = xb[qq];
+      }
+      __syncwarp();
     }
-    for (int c = tid; c < nc; c += PANEL_THREADS) {
-      double xb[8];
-#pragma unroll
-      for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + c] : 0.0;
-#pragma unroll
-      for (int kk = 0; kk < 7; ++kk)
-#pragma unroll
-        for (int qq = kk + 1; qq < 8; ++qq)
-          if (j0 + qq < j1) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
-#pragma unroll
-      for (int qq = 0; qq < 8; ++qq)
-        if (j0 + qq < j1) P[(j0 + qq) * LDP + c] = xb[qq];
-    }
-    __syncthreads();
-  }
-  const double *dinv = sLU + S * RP;
-  for (int J = nblk - 1; J >= 0; --J) {
-    const int j0 = J << 3, j1 = min(r, j0 + 8);
-    if (j1 < r) {
-      if (wact) {
+    for (int J = nblk - 1; J >= 0; --J) {
+      const int j0 = J << 3, j1 = min(r, j0 + 8);
+      if (j1 < r) {
         double acc[NPW][2];
 #pragma unroll
         for (int t = 0; t < NPW; ++t)
@@ -238,27 +239,29 @@ __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, d
               const int c = (n0 + t) * 8 + 2 * q + e;
               if (c < nc) P[(j0 + g) * LDP + c] = acc[t][e];
             }
+        __syncwarp();
       }
-      __syncthreads();
-    }
-    for (int c = tid; c < nc; c += PANEL_THREADS) {
-      double xb[8];
+      if (sact) {
+        double xb[8];
 #pragma unroll
-      for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + c] : 0.0;
+        for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + cs] : 0.0;
 #pragma unroll
-      for (int kk = 7; kk >= 0; --kk) {
-        if (j0 + kk < j1) {
-          xb[kk] = mul(xb[kk], dinv[j0 + kk]);
+        for (int kk = 7; kk >= 0; --kk) {
+          if (j0 + kk < j1) {
+            xb[kk] = mul(xb[kk], dinv[j0 + kk]);
 #pragma unroll
-          for (int qq = 0; qq < kk; ++qq) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+            for (int qq = 0; qq < kk; ++qq) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+          }
         }
-      }
 #pragma unroll
-      for (int qq = 0; qq < 8; ++qq)
-        if (j0 + qq < j1) P[(j0 + qq) * LDP + c] = xb[qq];
+        for (int qq = 0; qq < 8; ++qq)
+          if (j0 + qq < j1) P[(j0 + qq) * LDP + cs] = xb[qq];
+      }
+      __syncwarp();
     }
-    __syncthreads();
   }
+  // a warp's column tiles in the products that follow are its own here unless the row tiles are split
+  if (MM::MG > 1) __syncthreads();
 }
 
 // Edge tables: for block b and signature sig, fc = K^-1 (G_b prod K) and W fc (sig 0: no factor;
