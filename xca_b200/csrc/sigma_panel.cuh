@@ -159,15 +159,17 @@ __device__ __forceinline__ void panel_mma(const double *__restrict__ sM, const d
 
 // P[:, c] <- K^-1 P[:, c] for c < nc on a panel whose rows are already in pivot order (row i holds the
 // original row perm[i]).  Columns are independent, so each warp solves its own column tiles alone, with
-// no CTA barrier until the end: per 8-row block, the rectangular update by the rows already solved is an
-// MMA chain on the warp's tiles (A = -L or -U), then one lane per column runs the in-block
-// substitution.  Every element receives exactly the fused multiply-adds of lu_solve_reg in the same
-// order — forward k ascending, backward k descending with the reciprocal diagonal applied at k = i — so
-// the result is bit-identical to it; padding rows are not written.
+// no CTA barrier until the end.  Right-looking over 8-row blocks: the warp keeps every block's rows of
+// its tiles in MMA accumulators; once block K is solved (one lane per column runs the in-block
+// substitution in shared memory), its rows, read back as MMA B fragments, update all later blocks'
+// accumulators at once (A = -L, or -U going backward) — independent MMA chains.  Every element still
+// receives exactly the fused multiply-adds of lu_solve_reg in the same order — forward k ascending,
+// backward k descending with the reciprocal diagonal applied at k = i — so the result is bit-identical
+// to it (a masked MMA term, k >= r, adds 0 * 0); padding rows are not written.
 template <int RP>
 __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, double *P, int r, int nc, int tid, int warp, int lane) {
   using MM = MmaMap<RP>;
-  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP, NPW = MM::NPW;
+  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP, NPW = MM::NPW, MT = RP / 8;
   const int g = lane >> 2, q = lane & 3, n0 = MM::n0(warp);
   const bool wact = (MM::MG == 1 || warp < MM::NTL) && n0 * 8 < nc;  // one row tile: the first row group's warps
   const int nblk = (r + 7) >> 3;
@@ -175,89 +177,114 @@ __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, d
   const int cs = n0 * 8 + lane;  // the column this lane substitutes in-block (lanes < 8 NPW)
   const bool sact = lane < 8 * NPW && cs < nc;
   if (wact) {
-    for (int J = 0; J < nblk; ++J) {
-      const int j0 = J << 3, j1 = min(r, j0 + 8);
-      if (J > 0) {
-        double acc[NPW][2];
+    double acc[MT][NPW][2];
+    // accumulators of row g of every block, columns 2q, 2q + 1 of each tile
+    auto load_acc = [&]() {
+#pragma unroll
+      for (int J = 0; J < MT; ++J)
 #pragma unroll
         for (int t = 0; t < NPW; ++t)
 #pragma unroll
-          for (int e = 0; e < 2; ++e) acc[t][e] = P[(j0 + g) * LDP + (n0 + t) * 8 + 2 * q + e];
-        for (int k0 = 0; k0 < j0; k0 += 4) {
-          const int k = k0 + q;
-          const double a = -sLU[k * S + j0 + g];  // -L[j0 + g][k]
-#pragma unroll
-          for (int t = 0; t < NPW; ++t) dmma(acc[t][0], acc[t][1], a, P[k * LDP + (n0 + t) * 8 + g]);
-        }
-        if (j0 + g < j1)
-#pragma unroll
-          for (int t = 0; t < NPW; ++t)
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int c = (n0 + t) * 8 + 2 * q + e;
-              if (c < nc) P[(j0 + g) * LDP + c] = acc[t][e];
-            }
-        __syncwarp();
-      }
-      if (sact) {
-        double xb[8];
-#pragma unroll
-        for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + cs] : 0.0;
-#pragma unroll
-        for (int kk = 0; kk < 7; ++kk)
-#pragma unroll
-          for (int qq = kk + 1; qq < 8; ++qq)
-            if (j0 + qq < j1) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
-#pragma unroll
-        for (int qq = 0; qq < 8; ++qq)
-          if (j0 + qq < j1) P[(j0 + qq) * LDP + cs] = xb[qq];
-      }
+          for (int e = 0; e < 2; ++e) acc[J][t][e] = J < nblk ? P[(J * 8 + g) * LDP + (n0 + t) * 8 + 2 * q + e] : 0.0;
       __syncwarp();
-    }
-    for (int J = nblk - 1; J >= 0; --J) {
-      const int j0 = J << 3, j1 = min(r, j0 + 8);
-      if (j1 < r) {
-        double acc[NPW][2];
+    };
+    auto store_acc = [&](int K) {
+      const int i = K * 8 + g;
+      if (i < r)
 #pragma unroll
         for (int t = 0; t < NPW; ++t)
 #pragma unroll
-          for (int e = 0; e < 2; ++e) acc[t][e] = P[(j0 + g) * LDP + (n0 + t) * 8 + 2 * q + e];
-        // k runs from r - 1 down to j1: group kk feeds k = r - 1 - 4 kk - q, so that the MMA's ascending
-        // order inside the group is the descending order of the substitution
-        for (int kh = r - 1; kh >= j1; kh -= 4) {
-          const int k = kh - q;
-          const bool kv = k >= j1;
-          const double a = kv ? -sLU[k * S + j0 + g] : 0.0;  // -U[j0 + g][k]
-#pragma unroll
-          for (int t = 0; t < NPW; ++t) dmma(acc[t][0], acc[t][1], a, kv ? P[k * LDP + (n0 + t) * 8 + g] : 0.0);
-        }
-        if (j0 + g < j1)
-#pragma unroll
-          for (int t = 0; t < NPW; ++t)
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int c = (n0 + t) * 8 + 2 * q + e;
-              if (c < nc) P[(j0 + g) * LDP + c] = acc[t][e];
-            }
-        __syncwarp();
-      }
-      if (sact) {
-        double xb[8];
-#pragma unroll
-        for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + cs] : 0.0;
-#pragma unroll
-        for (int kk = 7; kk >= 0; --kk) {
-          if (j0 + kk < j1) {
-            xb[kk] = mul(xb[kk], dinv[j0 + kk]);
-#pragma unroll
-            for (int qq = 0; qq < kk; ++qq) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+          for (int e = 0; e < 2; ++e) {
+            const int c = (n0 + t) * 8 + 2 * q + e;
+            if (c < nc) P[i * LDP + c] = acc[K][t][e];
           }
-        }
-#pragma unroll
-        for (int qq = 0; qq < 8; ++qq)
-          if (j0 + qq < j1) P[(j0 + qq) * LDP + cs] = xb[qq];
-      }
       __syncwarp();
+    };
+    load_acc();
+#pragma unroll
+    for (int K = 0; K < MT; ++K) {
+      if (K < nblk) {
+        const int j0 = K * 8, j1 = min(r, j0 + 8);
+        if (K > 0) store_acc(K);  // block 0's rows are P's rows
+        if (sact) {
+          double xb[8];
+#pragma unroll
+          for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + cs] : 0.0;
+#pragma unroll
+          for (int kk = 0; kk < 7; ++kk)
+#pragma unroll
+            for (int qq = kk + 1; qq < 8; ++qq)
+              if (j0 + qq < j1) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+#pragma unroll
+          for (int qq = 0; qq < 8; ++qq)
+            if (j0 + qq < j1) P[(j0 + qq) * LDP + cs] = xb[qq];
+        }
+        __syncwarp();
+        if (K + 1 < nblk) {  // block K is full here: rows j0 .. j0 + 7 < r
+          double bf[2][NPW];
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int t = 0; t < NPW; ++t) bf[h][t] = P[(j0 + 4 * h + q) * LDP + (n0 + t) * 8 + g];
+#pragma unroll
+          for (int J = K + 1; J < MT; ++J)
+            if (J < nblk)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const double a = -sLU[(j0 + 4 * h + q) * S + J * 8 + g];  // -L[8 J + g][k]
+#pragma unroll
+                for (int t = 0; t < NPW; ++t) dmma(acc[J][t][0], acc[J][t][1], a, bf[h][t]);
+              }
+        }
+      }
+    }
+    load_acc();
+#pragma unroll
+    for (int K = MT - 1; K >= 0; --K) {
+      if (K < nblk) {
+        const int j0 = K * 8, j1 = min(r, j0 + 8);
+        if (K + 1 < nblk) store_acc(K);  // the last block's rows are P's rows
+        if (sact) {
+          double xb[8];
+#pragma unroll
+          for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + cs] : 0.0;
+#pragma unroll
+          for (int kk = 7; kk >= 0; --kk) {
+            if (j0 + kk < j1) {
+              xb[kk] = mul(xb[kk], dinv[j0 + kk]);
+#pragma unroll
+              for (int qq = 0; qq < kk; ++qq) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+            }
+          }
+#pragma unroll
+          for (int qq = 0; qq < 8; ++qq)
+            if (j0 + qq < j1) P[(j0 + qq) * LDP + cs] = xb[qq];
+        }
+        __syncwarp();
+        if (K > 0) {
+          // group h feeds k = j0 + 7 - 4 h - q: the MMA's ascending order inside a group is the
+          // descending order of the substitution
+          double bf[2][NPW];
+          bool kv[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int k = j0 + 7 - 4 * h - q;
+            kv[h] = k < j1;
+#pragma unroll
+            for (int t = 0; t < NPW; ++t) bf[h][t] = kv[h] ? P[k * LDP + (n0 + t) * 8 + g] : 0.0;
+          }
+#pragma unroll
+          for (int J = 0; J < MT; ++J)
+            if (J < K)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int k = j0 + 7 - 4 * h - q;
+                const double a = kv[h] ? -sLU[k * S + J * 8 + g] : 0.0;  // -U[8 J + g][k]
+#pragma unroll
+                for (int t = 0; t < NPW; ++t) dmma(acc[J][t][0], acc[J][t][1], a, bf[h][t]);
+              }
+        }
+      }
     }
   }
   // a warp's column tiles in the products that follow are its own here unless the row tiles are split
