@@ -111,7 +111,7 @@ __device__ __forceinline__ void coefs_and_hilbert(const double *sLU, const doubl
 // [sigc | gt | Q | P' | f | ft], each r d^2 doubles.
 template <int RP>
 __global__ void __launch_bounds__(256) dyson_coef_kernel(DysonBasis B, const double *__restrict__ Sigma, double eta) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *sLU = smem;
   double *sW = sLU + RP * RP + RP;
   int *sPerm = reinterpret_cast<int *>(sW + RP * RP);
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(1024) dyson_lu_solve_kernel(DysonBasis B, doub
 // Per block: sum_x G_b(beta)[x][x] = sum_x sum_l K(1, om_l) (K^-1 G_b)_l[x][x], one lane per diagonal entry.
 template <int RP>
 __global__ void __launch_bounds__(128) trace_beta_kernel(DysonBasis B, const double *__restrict__ G, double *__restrict__ out) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *sLU = smem;
   int *sPerm = reinterpret_cast<int *>(sLU + RP * RP + RP);
   __shared__ double part[128];

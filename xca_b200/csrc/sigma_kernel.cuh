@@ -29,7 +29,7 @@ constexpr int NSLAB = 3;            // per-item slabs: T, X, Y
 constexpr int WARPS_MAX = 8;
 
 struct DevBasis {
-  int r, p, n, nb, nq, region;  // region: doubles per slab region of a warp, r * max(32, largest dcmax)
+  int r, p, n, nb, nq;
   double beta;
   const double *LUp;    // RP x RP padded LU of K(t_i, om_l), column-major: unit L below the diagonal, U on and above
                         // (pad: U_kk = 1), followed by the RP reciprocals 1 / U_kk
@@ -58,8 +58,8 @@ struct DevBasis {
 struct ClassRec {
   int m, vct0, fbmask, b_out, pk;
   int npt;                 // pole tuples p^(m-1)
-  int batch;               // items a warp evaluates in lockstep: batch * dcmax <= 32 (1 when dcmax > 32)
-  int dcmax;               // largest (rows x columns) of the chain's T slabs
+  int batch;               // items a CTA evaluates together as panel columns: batch * dcmax <= panel width
+  int dcmax;               // panel columns of one item at the widest point of the chain
   int la[MAXM], lb[MAXM];  // line endpoints
   int ind_path[2 * MAXM - 1];
   int bdims[2 * MAXM + 1];

@@ -157,15 +157,104 @@ __device__ __forceinline__ void panel_mma(const double *__restrict__ sM, const d
   }
 }
 
+// In-block substitution of panel column c over rows j0 .. j1 - 1 of one 8-row block, one thread: forward
+// with the unit lower L, backward with U and the reciprocal diagonal, in the operation order of
+// lu_solve_reg.  A full block (j1 = j0 + 8) loads every operand before the first operation, the L / U
+// columns and the diagonal as 16-byte pairs; the last, partial block keeps each step behind its row guard.
+template <int RP>
+__device__ __forceinline__ void inblock_forward(const double *__restrict__ sLU, double *P, int j0, int j1, int c) {
+  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP;
+  double xb[8];
+  if (j1 == j0 + 8) {
+    double L[8][8];  // L[qq][kk] = L[j0 + qq][j0 + kk] for qq > kk
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) xb[qq] = P[(j0 + qq) * LDP + c];
+#pragma unroll
+    for (int kk = 0; kk < 7; ++kk)
+#pragma unroll
+      for (int pr = (kk + 1) & ~1; pr < 8; pr += 2) {
+        const double2 v = *reinterpret_cast<const double2 *>(sLU + (j0 + kk) * S + j0 + pr);
+        L[pr][kk] = v.x;
+        L[pr + 1][kk] = v.y;
+      }
+#pragma unroll
+    for (int kk = 0; kk < 7; ++kk)
+#pragma unroll
+      for (int qq = kk + 1; qq < 8; ++qq) xb[qq] = fmad(-L[qq][kk], xb[kk], xb[qq]);
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) P[(j0 + qq) * LDP + c] = xb[qq];
+  } else {
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + c] : 0.0;
+#pragma unroll
+    for (int kk = 0; kk < 7; ++kk)
+#pragma unroll
+      for (int qq = kk + 1; qq < 8; ++qq)
+        if (j0 + qq < j1) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq)
+      if (j0 + qq < j1) P[(j0 + qq) * LDP + c] = xb[qq];
+  }
+}
+
+template <int RP>
+__device__ __forceinline__ void inblock_backward(const double *__restrict__ sLU, double *P, int j0, int j1, int c) {
+  constexpr int S = mat_stride<RP>(), LDP = PanelCfg<RP>::LDP;
+  const double *dinv = sLU + S * RP;
+  double xb[8];
+  if (j1 == j0 + 8) {
+    double U[8][8], dv[8];  // U[qq][kk] = U[j0 + qq][j0 + kk] for qq < kk
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) xb[qq] = P[(j0 + qq) * LDP + c];
+#pragma unroll
+    for (int pr = 0; pr < 8; pr += 2) {
+      const double2 v = *reinterpret_cast<const double2 *>(dinv + j0 + pr);
+      dv[pr] = v.x;
+      dv[pr + 1] = v.y;
+    }
+#pragma unroll
+    for (int kk = 1; kk < 8; ++kk)
+#pragma unroll
+      for (int pr = 0; pr < kk; pr += 2) {
+        const double2 v = *reinterpret_cast<const double2 *>(sLU + (j0 + kk) * S + j0 + pr);
+        U[pr][kk] = v.x;
+        U[pr + 1][kk] = v.y;
+      }
+#pragma unroll
+    for (int kk = 7; kk >= 0; --kk) {
+      xb[kk] = mul(xb[kk], dv[kk]);
+#pragma unroll
+      for (int qq = 0; qq < kk; ++qq) xb[qq] = fmad(-U[qq][kk], xb[kk], xb[qq]);
+    }
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) P[(j0 + qq) * LDP + c] = xb[qq];
+  } else {
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + c] : 0.0;
+#pragma unroll
+    for (int kk = 7; kk >= 0; --kk) {
+      if (j0 + kk < j1) {
+        xb[kk] = mul(xb[kk], dinv[j0 + kk]);
+#pragma unroll
+        for (int qq = 0; qq < kk; ++qq) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
+      }
+    }
+#pragma unroll
+    for (int qq = 0; qq < 8; ++qq)
+      if (j0 + qq < j1) P[(j0 + qq) * LDP + c] = xb[qq];
+  }
+}
+
 // P[:, c] <- K^-1 P[:, c] for c < nc on a panel whose rows are already in pivot order (row i holds the
 // original row perm[i]).  Columns are independent, so each warp solves its own column tiles alone, with
 // no CTA barrier until the end.  Right-looking over 8-row blocks: the warp keeps every block's rows of
 // its tiles in MMA accumulators; once block K is solved (one lane per column runs the in-block
 // substitution in shared memory), its rows, read back as MMA B fragments, update all later blocks'
-// accumulators at once (A = -L, or -U going backward) — independent MMA chains.  Every element still
-// receives exactly the fused multiply-adds of lu_solve_reg in the same order — forward k ascending,
-// backward k descending with the reciprocal diagonal applied at k = i — so the result is bit-identical
-// to it (a masked MMA term, k >= r, adds 0 * 0); padding rows are not written.
+// accumulators at once (A = -L, or -U going backward) — independent MMA chains whose fragments are all
+// loaded before the first MMA of the step (every address lies inside the LU and the panel).  Every
+// element still receives exactly the fused multiply-adds of lu_solve_reg in the same order — forward k
+// ascending, backward k descending with the reciprocal diagonal applied at k = i — so the result is
+// bit-identical to it (a masked MMA term, k >= r, adds 0 * 0); padding rows are not written.
 template <int RP>
 __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, double *P, int r, int nc, int tid, int warp, int lane) {
   using MM = MmaMap<RP>;
@@ -173,19 +262,18 @@ __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, d
   const int g = lane >> 2, q = lane & 3, n0 = MM::n0(warp);
   const bool wact = (MM::MG == 1 || warp < MM::NTL) && n0 * 8 < nc;  // one row tile: the first row group's warps
   const int nblk = (r + 7) >> 3;
-  const double *dinv = sLU + S * RP;
   const int cs = n0 * 8 + lane;  // the column this lane substitutes in-block (lanes < 8 NPW)
   const bool sact = lane < 8 * NPW && cs < nc;
   if (wact) {
     double acc[MT][NPW][2];
-    // accumulators of row g of every block, columns 2q, 2q + 1 of each tile
+    // accumulators of row g of every block, columns 2q, 2q + 1 of each tile (rows past r: unused)
     auto load_acc = [&]() {
 #pragma unroll
       for (int J = 0; J < MT; ++J)
 #pragma unroll
         for (int t = 0; t < NPW; ++t)
 #pragma unroll
-          for (int e = 0; e < 2; ++e) acc[J][t][e] = J < nblk ? P[(J * 8 + g) * LDP + (n0 + t) * 8 + 2 * q + e] : 0.0;
+          for (int e = 0; e < 2; ++e) acc[J][t][e] = P[(J * 8 + g) * LDP + (n0 + t) * 8 + 2 * q + e];
       __syncwarp();
     };
     auto store_acc = [&](int K) {
@@ -206,35 +294,24 @@ __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, d
       if (K < nblk) {
         const int j0 = K * 8, j1 = min(r, j0 + 8);
         if (K > 0) store_acc(K);  // block 0's rows are P's rows
-        if (sact) {
-          double xb[8];
-#pragma unroll
-          for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + cs] : 0.0;
-#pragma unroll
-          for (int kk = 0; kk < 7; ++kk)
-#pragma unroll
-            for (int qq = kk + 1; qq < 8; ++qq)
-              if (j0 + qq < j1) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
-#pragma unroll
-          for (int qq = 0; qq < 8; ++qq)
-            if (j0 + qq < j1) P[(j0 + qq) * LDP + cs] = xb[qq];
-        }
+        if (sact) inblock_forward<RP>(sLU, P, j0, j1, cs);
         __syncwarp();
         if (K + 1 < nblk) {  // block K is full here: rows j0 .. j0 + 7 < r
-          double bf[2][NPW];
+          double bf[2][NPW], af[MT][2];
 #pragma unroll
-          for (int h = 0; h < 2; ++h)
+          for (int h = 0; h < 2; ++h) {
 #pragma unroll
             for (int t = 0; t < NPW; ++t) bf[h][t] = P[(j0 + 4 * h + q) * LDP + (n0 + t) * 8 + g];
+#pragma unroll
+            for (int J = K + 1; J < MT; ++J) af[J][h] = -sLU[(j0 + 4 * h + q) * S + J * 8 + g];  // -L[8 J + g][k]
+          }
 #pragma unroll
           for (int J = K + 1; J < MT; ++J)
             if (J < nblk)
 #pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                const double a = -sLU[(j0 + 4 * h + q) * S + J * 8 + g];  // -L[8 J + g][k]
+              for (int h = 0; h < 2; ++h)
 #pragma unroll
-                for (int t = 0; t < NPW; ++t) dmma(acc[J][t][0], acc[J][t][1], a, bf[h][t]);
-              }
+                for (int t = 0; t < NPW; ++t) dmma(acc[J][t][0], acc[J][t][1], af[J][h], bf[h][t]);
         }
       }
     }
@@ -244,45 +321,33 @@ __device__ __forceinline__ void panel_trsm_mma(const double *__restrict__ sLU, d
       if (K < nblk) {
         const int j0 = K * 8, j1 = min(r, j0 + 8);
         if (K + 1 < nblk) store_acc(K);  // the last block's rows are P's rows
-        if (sact) {
-          double xb[8];
-#pragma unroll
-          for (int qq = 0; qq < 8; ++qq) xb[qq] = (j0 + qq < j1) ? P[(j0 + qq) * LDP + cs] : 0.0;
-#pragma unroll
-          for (int kk = 7; kk >= 0; --kk) {
-            if (j0 + kk < j1) {
-              xb[kk] = mul(xb[kk], dinv[j0 + kk]);
-#pragma unroll
-              for (int qq = 0; qq < kk; ++qq) xb[qq] = fmad(-sLU[(j0 + kk) * S + j0 + qq], xb[kk], xb[qq]);
-            }
-          }
-#pragma unroll
-          for (int qq = 0; qq < 8; ++qq)
-            if (j0 + qq < j1) P[(j0 + qq) * LDP + cs] = xb[qq];
-        }
+        if (sact) inblock_backward<RP>(sLU, P, j0, j1, cs);
         __syncwarp();
         if (K > 0) {
           // group h feeds k = j0 + 7 - 4 h - q: the MMA's ascending order inside a group is the
           // descending order of the substitution
-          double bf[2][NPW];
-          bool kv[2];
+          double bf[2][NPW], af[MT][2];
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int k = j0 + 7 - 4 * h - q;
-            kv[h] = k < j1;
+            const bool kv = k < j1;
 #pragma unroll
-            for (int t = 0; t < NPW; ++t) bf[h][t] = kv[h] ? P[k * LDP + (n0 + t) * 8 + g] : 0.0;
+            for (int t = 0; t < NPW; ++t) {
+              const double pv = P[k * LDP + (n0 + t) * 8 + g];
+              bf[h][t] = kv ? pv : 0.0;
+            }
+#pragma unroll
+            for (int J = 0; J < K; ++J) {
+              const double u = sLU[k * S + J * 8 + g];  // U[8 J + g][k]
+              af[J][h] = kv ? -u : 0.0;
+            }
           }
 #pragma unroll
-          for (int J = 0; J < MT; ++J)
-            if (J < K)
+          for (int J = 0; J < K; ++J)
 #pragma unroll
-              for (int h = 0; h < 2; ++h) {
-                const int k = j0 + 7 - 4 * h - q;
-                const double a = kv[h] ? -sLU[k * S + J * 8 + g] : 0.0;  // -U[8 J + g][k]
+            for (int h = 0; h < 2; ++h)
 #pragma unroll
-                for (int t = 0; t < NPW; ++t) dmma(acc[J][t][0], acc[J][t][1], a, bf[h][t]);
-              }
+              for (int t = 0; t < NPW; ++t) dmma(acc[J][t][0], acc[J][t][1], af[J][h], bf[h][t]);
         }
       }
     }
@@ -300,7 +365,7 @@ template <int RP>
 __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(DevBasis B, const double *__restrict__ G,
                                                                               const int2 *__restrict__ chunks, int n_chunks) {
   constexpr int NCU = PanelCfg<RP>::NC, LDP = PanelCfg<RP>::LDP;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *sLU, *sW, *sBK, *PA;
   ItemState *ist;
   int *sPerm;
@@ -359,7 +424,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
                                                                         int *__restrict__ unit_counter, const double *__restrict__ G,
                                                                         double *__restrict__ Sigma, double scale) {
   constexpr int NC = PanelCfg<RP>::LDP, NCU = PanelCfg<RP>::NC, NT = PANEL_THREADS;  // NC: panel row stride
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *sLU, *sW, *sBK, *PA;
   ItemState *ist;
   int *sPerm;

@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis C
                                                          const WorkUnit *__restrict__ units, int n_units, int *__restrict__ unit_counter,
                                                          const double *__restrict__ G, double *__restrict__ gout, double scale,
                                                          int nmax, double *__restrict__ scratch, long warp_doubles) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   double *sLU = smem, *sW = sLU + RP * RP + RP, *sBK = sW + RP * RP, *sRF = sBK + RP * RP;
   int *sPerm = reinterpret_cast<int *>(sRF + RP * RP);
   for (int i = threadIdx.x; i < RP * RP + RP; i += blockDim.x) sLU[i] = B.LUp[i];

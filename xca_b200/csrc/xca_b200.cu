@@ -209,7 +209,6 @@ struct Ctx {
   std::vector<int> perm;                        // RP
   std::vector<long> tab_off;                    // per block offset into the edge tables
   long nsig_alloc = 0;
-  int region = 0;
   // device copies
   DevBuf<double> d_tabs, d_k0, d_kitp, d_kitm, d_kpow, d_polesb, d_hval, d_hrefl, d_ops;
   DevBuf<int> d_dims, d_set_to_orb, d_perm, d_pinv;
@@ -243,7 +242,7 @@ struct Ctx {
 
   DevBasis basis(int nsig) const {
     DevBasis B;
-    B.r = r; B.p = p; B.n = n; B.nb = nb; B.nq = nq; B.region = region; B.beta = beta;
+    B.r = r; B.p = p; B.n = n; B.nb = nb; B.nq = nq; B.beta = beta;
     B.LUp = d_LUp.ptr; B.perm = d_perm.ptr; B.pinv = d_pinv.ptr; B.Wp = d_Wp.ptr; B.BKp = d_BKp.ptr; B.tabs = d_tabs.ptr; B.k0 = d_k0.ptr;
     B.tab = d_tab.ptr; B.tab_off = d_tab_off.ptr; B.nsig = nsig;
     B.kitp = d_kitp.ptr; B.kitm = d_kitm.ptr; B.kpow = d_kpow.ptr; B.polesb = d_polesb.ptr;
@@ -450,9 +449,12 @@ static std::unique_ptr<ClassSet> build_classes(Ctx *c, const Topology &T, const 
           for (int i = 0; i < nv - 1; ++i) R.ind_path[i] = path[i];
           for (int i = 0; i <= nv; ++i) R.bdims[i] = bd[i];
           {
-            int mxb = 0;
-            for (int i = 1; i <= nv; ++i) mxb = std::max(mxb, bd[i]);
-            R.dcmax = mxb * std::max(bd[0], bd[1]);
+            // widest panel state along the chain: blocks up to the zero vertex carry d1 columns per
+            // entry, the zero vertex's intermediate and everything after it d0
+            int w = 0;
+            for (int i = 1; i <= vct0; ++i) w = std::max(w, bd[i] * bd[1]);
+            for (int i = vct0; i <= nv; ++i) w = std::max(w, bd[i] * bd[0]);
+            R.dcmax = w;
             const int nc = panel_nc_host(c->RP);
             if (R.dcmax > nc)
               throw Error(XCA_ERR_UNSUPPORTED, "block chain too wide for the panel kernel (" + std::to_string(R.dcmax) +
@@ -1133,11 +1135,6 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
   }
   if ((double)toff * 8.0 > 24e9) throw Error(XCA_ERR_UNSUPPORTED, "edge tables would exceed 24 GB");
   c->d_tab.resize(toff);
-  {
-    int mxb = 0;
-    for (int b = 0; b < n_blocks; ++b) mxb = std::max(mxb, block_dims[b]);
-    c->region = r * std::max(32, mxb * mxb);
-  }
   // upload
   cudaStream_t s = c->stream;
   c->d_tab_off.upload(c->tab_off, s);
