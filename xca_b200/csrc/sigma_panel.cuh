@@ -417,6 +417,108 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(Dev
   }
 }
 
+// Vertex pass: X(t) <- k(t) F T(t) for every item of the batch (multiply_left_vertex), thread per output
+// column over a stride of tau rows.  DV > 0 is the input block dimension known at compile time (the
+// operator row is held in registers across the rows and every load of a row is issued before its
+// fused multiply-adds); DV = 0 takes dv at run time.  The operation order is the same either way.
+template <int RP, int DV>
+__device__ __forceinline__ void vertex_pass(const DevBasis &B, const ItemState *ist, const double *T, double *X, const int *rowpos,
+                                            int r, int dv, int dvp, int ncol, int nbi, int tid) {
+  constexpr int NC = PanelCfg<RP>::LDP, NT = PANEL_THREADS;
+  const int dci = dv * ncol, dco = dvp * ncol, nc = nbi * dco, tpc = NT / nc, c = tid % nc, t0 = tid / nc;
+  if (t0 >= tpc) return;
+  const int j = c / dco, e = c - j * dco, x = e / ncol, z = e - x * ncol;
+  const ItemState &S = ist[j];
+  const double *F = B.ops + S.opoff + x * dv;
+  const double *kt = S.kcol >= 0 ? (S.kneg ? B.kitm : B.kitp) + S.kcol : nullptr;
+  const double *Tc = T + j * dci + z;
+  const int p = B.p;
+  double f[DV > 0 ? DV : 1];
+#pragma unroll
+  for (int y = 0; y < DV; ++y) f[y] = F[y];
+  for (int t = t0; t < r; t += tpc) {
+    const double *Tt = Tc + t * NC;
+    double a = 0.0;
+    if (DV > 0) {
+      double tv[DV > 0 ? DV : 1];
+#pragma unroll
+      for (int y = 0; y < DV; ++y) tv[y] = Tt[y * ncol];
+#pragma unroll
+      for (int y = 0; y < DV; ++y) a = fmad(f[y], tv[y], a);
+    } else {
+      for (int y = 0; y < dv; ++y) a = fmad(F[y], Tt[y * ncol], a);
+    }
+    if (kt) a = mul(a, kt[(size_t)t * p]);
+    X[(rowpos ? rowpos[t] : t) * NC + c] = a;
+  }
+}
+
+// Q / P' pass of an edge, one warp per tau row l (Q and P' of row l read only row l of gc and Gt):
+// Q_l = Ft_l gc_l + fc_l Gt_l (into Y) and P'_l = K(0, om_l) (fc_l gc_l) (over Gt, into X).  D > 0 is the
+// edge's block dimension known at compile time (all loads of an entry are issued before its fused
+// multiply-adds); D = 0 takes d at run time.  The operation order is the same either way.
+template <int RP, int D>
+__device__ __forceinline__ void qp_pass(const DevBasis &B, const ItemState *ist, const double *T, double *X, double *Y, int r, int d,
+                                        int ncol, int nc, int warp, int lane) {
+  constexpr int NC = PanelCfg<RP>::LDP, NCU = PanelCfg<RP>::NC, NT = PANEL_THREADS;
+  constexpr int CPL = (NCU + 31) / 32;
+  const int dd = d * d, dc = d * ncol;
+  const double *tbq[CPL];
+  int coff[CPL];
+  bool cval[CPL];
+#pragma unroll
+  for (int q = 0; q < CPL; ++q) {
+    const int c = lane + 32 * q;
+    cval[q] = c < nc;
+    const int cc = cval[q] ? c : 0;
+    const int j = cc / dc, ee = cc - j * dc, x = ee / ncol, z = ee - x * ncol;
+    tbq[q] = B.tab + ist[j].taboff + x * d;
+    coff[q] = j * dc + z;
+  }
+  for (int l = warp; l < r; l += NT / 32) {
+    double qv[CPL], pv[CPL];
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) {
+      double aq = 0.0, ap = 0.0;
+      if (cval[q]) {
+        const double *fl = tbq[q] + l * dd, *ftl = tbq[q] + (long)r * dd + l * dd;
+        const double *gl = T + l * NC + coff[q], *gtl = X + l * NC + coff[q];
+        if (D > 0) {
+          constexpr int DD = D > 0 ? D : 1;
+          double f[DD], ft[DD], gv[DD], gtv[DD];
+#pragma unroll
+          for (int y = 0; y < D; ++y) {
+            f[y] = fl[y];
+            ft[y] = ftl[y];
+            gv[y] = gl[y * ncol];
+            gtv[y] = gtl[y * ncol];
+          }
+#pragma unroll
+          for (int y = 0; y < D; ++y) {
+            aq = fmad(ft[y], gv[y], fmad(f[y], gtv[y], aq));
+            ap = fmad(f[y], gv[y], ap);
+          }
+        } else {
+          for (int y = 0; y < d; ++y) {
+            aq = fmad(ftl[y], gl[y * ncol], fmad(fl[y], gtl[y * ncol], aq));
+            ap = fmad(fl[y], gl[y * ncol], ap);
+          }
+        }
+      }
+      qv[q] = aq;
+      pv[q] = mul(B.k0[l], ap);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < CPL; ++q)
+      if (cval[q]) {
+        const int c = lane + 32 * q;
+        Y[l * NC + c] = qv[q];
+        X[l * NC + c] = pv[q];
+      }
+  }
+}
+
 // Dynamic shared memory: see panel_smem_doubles.
 template <int RP>
 __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis B, const ClassRec *__restrict__ classes,
@@ -531,20 +633,12 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
             }
           }
           __syncthreads();
-          const int dci = dv * ncol, dco = dvp * ncol, nc = nbi * dco, tpc = NT / nc, c = tid % nc, t0 = tid / nc;
-          if (t0 < tpc) {
-            const int j = c / dco, e = c - j * dco, x = e / ncol, z = e - x * ncol;
-            const ItemState &S = ist[j];
-            const double *F = B.ops + S.opoff + x * dv;
-            const double *kt = S.kcol >= 0 ? (S.kneg ? B.kitm : B.kitp) + S.kcol : nullptr;
-            const double *Tc = T + j * dci + z;
-            for (int t = t0; t < r; t += tpc) {
-              const double *Tt = Tc + t * NC;
-              double a = 0.0;
-              for (int y = 0; y < dv; ++y) a = fmad(F[y], Tt[y * ncol], a);
-              if (kt) a = mul(a, kt[(size_t)t * p]);
-              X[(rowpos ? rowpos[t] : t) * NC + c] = a;
-            }
+          switch (dv) {
+            case 1: vertex_pass<RP, 1>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+            case 2: vertex_pass<RP, 2>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+            case 3: vertex_pass<RP, 3>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+            case 4: vertex_pass<RP, 4>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+            default: vertex_pass<RP, 0>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
           }
           __syncthreads();
           double *tmp = T; T = X; X = tmp;
@@ -574,45 +668,12 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           __syncthreads();
           // (b) per row l (one warp per row; Q and P' of row l read only row l of gc and Gt):
           //     Q_l = Ft_l gc_l + fc_l Gt_l (into Y) and P'_l = K(0, om_l) (fc_l gc_l) (over Gt, into X)
-          {
-            constexpr int CPL = (NCU + 31) / 32;
-            const double *tbq[CPL];
-            int coff[CPL];
-            bool cval[CPL];
-#pragma unroll
-            for (int q = 0; q < CPL; ++q) {
-              const int c = lane + 32 * q;
-              cval[q] = c < nc;
-              const int cc = cval[q] ? c : 0;
-              const int j = cc / dc, ee = cc - j * dc, x = ee / ncol, z = ee - x * ncol;
-              tbq[q] = B.tab + ist[j].taboff + x * d;
-              coff[q] = j * dc + z;
-            }
-            for (int l = warp; l < r; l += NT / 32) {
-              double qv[CPL], pv[CPL];
-#pragma unroll
-              for (int q = 0; q < CPL; ++q) {
-                double aq = 0.0, ap = 0.0;
-                if (cval[q]) {
-                  const double *fl = tbq[q] + l * dd, *ftl = tbq[q] + (long)r * dd + l * dd;
-                  const double *gl = T + l * NC + coff[q], *gtl = X + l * NC + coff[q];
-                  for (int y = 0; y < d; ++y) {
-                    aq = fmad(ftl[y], gl[y * ncol], fmad(fl[y], gtl[y * ncol], aq));
-                    ap = fmad(fl[y], gl[y * ncol], ap);
-                  }
-                }
-                qv[q] = aq;
-                pv[q] = mul(B.k0[l], ap);
-              }
-              __syncwarp();
-#pragma unroll
-              for (int q = 0; q < CPL; ++q)
-                if (cval[q]) {
-                  const int c = lane + 32 * q;
-                  Y[l * NC + c] = qv[q];
-                  X[l * NC + c] = pv[q];
-                }
-            }
+          switch (d) {
+            case 1: qp_pass<RP, 1>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
+            case 2: qp_pass<RP, 2>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
+            case 3: qp_pass<RP, 3>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
+            case 4: qp_pass<RP, 4>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
+            default: qp_pass<RP, 0>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
           }
           __syncthreads();
           // (c) h = fma(t_i, (beta K) P', (beta K) Q) (into T; gc is no longer needed)
