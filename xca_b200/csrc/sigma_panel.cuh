@@ -519,13 +519,83 @@ __device__ __forceinline__ void qp_pass(const DevBasis &B, const ItemState *ist,
   }
 }
 
+// Zero vertex, inner pass for operator mu (multiply_left_vertex_and_right_zero_vertex): Y(t) =
+// sum_kappa (+-h(t)[om, ok]) (T(t) F_kappa), thread per Y column over a stride of tau rows.  D1 > 0 is
+// the first block's dimension known at compile time (the row of T is loaded once for every kappa);
+// D1 = 0 takes d1 at run time.  The operation order is the same either way.
+template <int RP, int D1>
+__device__ __forceinline__ void zv_inner_pass(const DevBasis &B, const double *T, double *Y, int r, int pk, int qs, int om, bool fwd,
+                                              double hs, long ok_off, int d0, int d1, int dv, int nbi, int tid) {
+  constexpr int NC = PanelCfg<RP>::LDP, NT = PANEL_THREADS;
+  const int n = B.n, dci = dv * d1, dmid = dv * d0, ncm = nbi * dmid, tpm = NT / ncm, c = tid % ncm, tm0 = tid / ncm;
+  if (tm0 >= tpm) return;
+  const int j = c / dmid, ee = c - j * dmid, x = ee / d0, z = ee - x * d0;
+  const double *Tc = T + j * dci + x * d1;
+  for (int t = tm0; t < r; t += tpm) {
+    const double *Tt = Tc + t * NC;
+    double tv[D1 > 0 ? D1 : 1];
+#pragma unroll
+    for (int y = 0; y < D1; ++y) tv[y] = Tt[y];
+    double a = 0.0;
+    for (int kap = 0; kap < qs; ++kap) {
+      const int ok = B.set_to_orb[pk * n + kap];
+      const double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
+      if (h == 0.0) continue;
+      const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0 + z;
+      double tf = 0.0;
+      if (D1 > 0) {
+        double fv[D1 > 0 ? D1 : 1];
+#pragma unroll
+        for (int y = 0; y < D1; ++y) fv[y] = Fk[y * d0];
+#pragma unroll
+        for (int y = 0; y < D1; ++y) tf = fmad(tv[y], fv[y], tf);
+      } else {
+        for (int y = 0; y < d1; ++y) tf = fmad(Tt[y], Fk[y * d0], tf);
+      }
+      a = fmad(mul(hs, h), tf, a);
+    }
+    Y[t * NC + c] = a;
+  }
+}
+
+// Zero vertex, outer pass for operator mu: X(t) += F_mu Y(t) (first = true: X(t) = 0 + F_mu Y(t)), thread
+// per output column over a stride of tau rows; rows go to rowpos[t] when given.  DV > 0: the block
+// dimension known at compile time (the operator row is held in registers); DV = 0 takes dv at run time.
+template <int RP, int DV>
+__device__ __forceinline__ void zv_outer_pass(const double *Fm, const double *Y, double *X, const int *rowpos, int r, int d0, int dv,
+                                              int dvp, int nbi, int tid, bool first) {
+  constexpr int NC = PanelCfg<RP>::LDP, NT = PANEL_THREADS;
+  const int dmid = dv * d0, dco = dvp * d0, nco = nbi * dco, tpo = NT / nco, c = tid % nco, to0 = tid / nco;
+  if (to0 >= tpo) return;
+  const int j = c / dco, ee = c - j * dco, x = ee / d0, z = ee - x * d0;
+  const double *Fx = Fm + x * dv, *Yc = Y + j * dmid + z;
+  double f[DV > 0 ? DV : 1];
+#pragma unroll
+  for (int y = 0; y < DV; ++y) f[y] = Fx[y];
+  for (int t = to0; t < r; t += tpo) {
+    const double *Yt = Yc + t * NC;
+    double a = 0.0;
+    if (DV > 0) {
+      double yv[DV > 0 ? DV : 1];
+#pragma unroll
+      for (int y = 0; y < DV; ++y) yv[y] = Yt[y * d0];
+#pragma unroll
+      for (int y = 0; y < DV; ++y) a = fmad(f[y], yv[y], a);
+    } else {
+      for (int y = 0; y < dv; ++y) a = fmad(Fx[y], Yt[y * d0], a);
+    }
+    const int row = rowpos ? rowpos[t] : t;
+    X[row * NC + c] = add(first ? 0.0 : X[row * NC + c], a);
+  }
+}
+
 // Dynamic shared memory: see panel_smem_doubles.
 template <int RP>
 __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis B, const ClassRec *__restrict__ classes,
                                                                         const WorkUnit *__restrict__ units, int n_units,
                                                                         int *__restrict__ unit_counter, const double *__restrict__ G,
                                                                         double *__restrict__ Sigma, double scale) {
-  constexpr int NC = PanelCfg<RP>::LDP, NCU = PanelCfg<RP>::NC, NT = PANEL_THREADS;  // NC: panel row stride
+  constexpr int NC = PanelCfg<RP>::LDP, NT = PANEL_THREADS;  // NC: panel row stride
   extern __shared__ __align__(16) double smem[];
   double *sLU, *sW, *sBK, *PA;
   ItemState *ist;
@@ -691,45 +761,29 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           int qs = 0;
           for (int i = 0; i < n; ++i)
             if (B.set_to_orb[pk * n + i] >= 0) qs = i + 1;
-          const int dci = dv * d1, dmid = dv * d0, dco = dvp * d0;
-          const int ncm = nbi * dmid, nco = nbi * dco;
-          const int tpo = NT / nco, co = tid % nco, to0 = tid / nco;
-          const int tpm = NT / ncm, cm = tid % ncm, tm0 = tid / ncm;
-          if (to0 < tpo)
-            for (int t = to0; t < r; t += tpo) X[(rowpos ? rowpos[t] : t) * NC + co] = 0.0;
-          __syncthreads();
+          if (qs == 0) {  // no operator pair: the zero vertex is zero
+            const int nco = nbi * dvp * d0, tpo = NT / nco, co = tid % nco, to0 = tid / nco;
+            if (to0 < tpo)
+              for (int t = to0; t < r; t += tpo) X[(rowpos ? rowpos[t] : t) * NC + co] = 0.0;
+            __syncthreads();
+          }
           for (int mu = 0; mu < qs; ++mu) {
             const int om = B.set_to_orb[pk * n + mu];
-            if (tm0 < tpm) {
-              const int c = cm, j = c / dmid, ee = c - j * dmid, x = ee / d0, z = ee - x * d0;
-              const double *Tc = T + j * dci + x * d1;
-              for (int t = tm0; t < r; t += tpm) {
-                const double *Tt = Tc + t * NC;
-                double a = 0.0;
-                for (int kap = 0; kap < qs; ++kap) {
-                  const int ok = B.set_to_orb[pk * n + kap];
-                  const double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
-                  if (h == 0.0) continue;
-                  const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0 + z;
-                  double tf = 0.0;
-                  for (int y = 0; y < d1; ++y) tf = fmad(Tt[y], Fk[y * d0], tf);
-                  a = fmad(mul(hs, h), tf, a);
-                }
-                Y[t * NC + c] = a;
-              }
+            switch (d1) {
+              case 1: zv_inner_pass<RP, 1>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
+              case 2: zv_inner_pass<RP, 2>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
+              case 3: zv_inner_pass<RP, 3>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
+              case 4: zv_inner_pass<RP, 4>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
+              default: zv_inner_pass<RP, 0>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
             }
             __syncthreads();
             const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
-            if (to0 < tpo) {
-              const int c = co, j = c / dco, ee = c - j * dco, x = ee / d0, z = ee - x * d0;
-              const double *Fx = Fm + x * dv, *Yc = Y + j * dmid + z;
-              for (int t = to0; t < r; t += tpo) {
-                const double *Yt = Yc + t * NC;
-                double a = 0.0;
-                for (int y = 0; y < dv; ++y) a = fmad(Fx[y], Yt[y * d0], a);
-                const int row = rowpos ? rowpos[t] : t;
-                X[row * NC + c] = add(X[row * NC + c], a);
-              }
+            switch (dv) {
+              case 1: zv_outer_pass<RP, 1>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
+              case 2: zv_outer_pass<RP, 2>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
+              case 3: zv_outer_pass<RP, 3>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
+              case 4: zv_outer_pass<RP, 4>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
+              default: zv_outer_pass<RP, 0>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
             }
             __syncthreads();
           }
