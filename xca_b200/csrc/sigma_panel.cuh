@@ -603,6 +603,7 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
   panel_layout<RP>(smem, sLU, sW, sBK, PA, ist, sPerm);
   double *PB = PA + RP * NC, *PC = PB + RP * NC;
   __shared__ int s_unit;
+  __shared__ ClassRec s_cls;
   __shared__ unsigned long long s_max[PANEL_BMAX];
   stage_basis<RP>(B, sLU, sW, sBK, sPerm);
   const int r = B.r, p = B.p, n = B.n, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -614,7 +615,14 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
     __syncthreads();
     if (u >= n_units) break;
     const WorkUnit wu = units[u];
-    const ClassRec &C = classes[wu.cls];
+    // the unit's class record, read by every per-item set-up step, staged in shared memory
+    static_assert(sizeof(ClassRec) % sizeof(int) == 0, "ClassRec holds ints only");
+    {
+      const int *src = reinterpret_cast<const int *>(classes + wu.cls);
+      for (int i = tid; i < (int)(sizeof(ClassRec) / sizeof(int)); i += NT) reinterpret_cast<int *>(&s_cls)[i] = src[i];
+    }
+    __syncthreads();
+    const ClassRec &C = s_cls;
     const int m = C.m, vct0 = C.vct0;
     const int d0 = C.bdims[0], d1 = C.bdims[1];
     const int dout = C.bdims[2 * m];
