@@ -453,79 +453,6 @@ __device__ __forceinline__ void vertex_pass(const DevBasis &B, const ItemState *
   }
 }
 
-// Offset of an item's edge table for edge e on block b: the signature counts the K factors of the lines
-// that span the edge in their case-B form (integrate_left_edge's choice of table).
-__device__ __forceinline__ long edge_table_offset(const DevBasis &B, const ClassRec &C, const ItemState &S, int e, int b, int r, int dd) {
-  const int p = B.p;
-  int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
-  for (int i = 1; i < C.m; ++i)
-    if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
-      sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
-      lp[nf] = S.lpole[i];
-      nf++;
-    }
-  long sig = 0;
-  if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
-  if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
-  return B.tab_off[b] + sig * 2 * r * dd;
-}
-
-// Q / P' pass of an edge for one warp's own 8-column tile, used when every item's columns lie inside one
-// tile (d * ncol divides 8): lane & 7 picks the column, lane >> 3 the row of each group of four rows, and
-// each lane finds its item's edge table itself, so the pass needs no CTA barrier.  Same operations, in the
-// same order, as qp_pass.
-template <int RP, int D>
-__device__ __forceinline__ void qp_tile(const DevBasis &B, const ClassRec &C, const ItemState *ist, const double *T, double *X, double *Y,
-                                        int e, int b, int r, int d, int ncol, int nc, int warp, int lane) {
-  constexpr int NC = PanelCfg<RP>::LDP;
-  const int c0 = warp * 8;  // one column tile per warp (MmaMap<RP>::MG == 1, NPW == 1)
-  if (c0 >= nc) return;
-  const int dd = d * d, dc = d * ncol;
-  const int c = c0 + (lane & 7);
-  const bool cv = c < nc;
-  const int cc = cv ? c : c0;
-  const int j = cc / dc, ee = cc - j * dc, x = ee / ncol, z = ee - x * ncol;
-  const double *tb = B.tab + edge_table_offset(B, C, ist[j], e, b, r, dd) + x * d;
-  const int coff = j * dc + z;
-  const int nit = (r + 3) >> 2;
-  for (int it = 0; it < nit; ++it) {
-    const int l = (lane >> 3) + 4 * it;
-    const bool lv = cv && l < r;
-    double aq = 0.0, ap = 0.0;
-    if (lv) {
-      const double *fl = tb + l * dd, *ftl = tb + (long)r * dd + l * dd;
-      const double *gl = T + l * NC + coff, *gtl = X + l * NC + coff;
-      if (D > 0) {
-        constexpr int DD = D > 0 ? D : 1;
-        double f[DD], ft[DD], gv[DD], gtv[DD];
-#pragma unroll
-        for (int y = 0; y < D; ++y) {
-          f[y] = fl[y];
-          ft[y] = ftl[y];
-          gv[y] = gl[y * ncol];
-          gtv[y] = gtl[y * ncol];
-        }
-#pragma unroll
-        for (int y = 0; y < D; ++y) {
-          aq = fmad(ft[y], gv[y], fmad(f[y], gtv[y], aq));
-          ap = fmad(f[y], gv[y], ap);
-        }
-      } else {
-        for (int y = 0; y < d; ++y) {
-          aq = fmad(ftl[y], gl[y * ncol], fmad(fl[y], gtl[y * ncol], aq));
-          ap = fmad(fl[y], gl[y * ncol], ap);
-        }
-      }
-    }
-    __syncwarp();  // row l of Gt is read by this lane group before any of it is overwritten with P'
-    if (lv) {
-      Y[l * NC + c] = aq;
-      X[l * NC + c] = mul(B.k0[l], ap);
-    }
-  }
-  __syncwarp();
-}
-
 // Q / P' pass of an edge, one warp per tau row l (Q and P' of row l read only row l of gc and Gt):
 // Q_l = Ft_l gc_l + fc_l Gt_l (into Y) and P'_l = K(0, om_l) (fc_l gc_l) (over Gt, into X).  D > 0 is the
 // edge's block dimension known at compile time (all loads of an entry are issued before its fused
@@ -799,22 +726,20 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           const int b = C.ind_path[e];
           const int d = C.bdims[e + 1];
           const int dd = d * d, dc = d * ncol, nc = nbi * dc;
-          if (MmaMap<RP>::MG == 1 && 8 % dc == 0) {
-            // every item's columns lie inside one warp's 8-column tile: the whole edge is warp-local
-            panel_trsm_mma<RP>(sLU, T, r, nc, tid, warp, lane);
-            panel_mma<RP, false>(sW, T, nullptr, X, r, nc, nullptr, warp, lane);
-            __syncwarp();
-            switch (d) {
-              case 1: qp_tile<RP, 1>(B, C, ist, T, X, Y, e, b, r, d, ncol, nc, warp, lane); break;
-              case 2: qp_tile<RP, 2>(B, C, ist, T, X, Y, e, b, r, d, ncol, nc, warp, lane); break;
-              case 4: qp_tile<RP, 4>(B, C, ist, T, X, Y, e, b, r, d, ncol, nc, warp, lane); break;
-              default: qp_tile<RP, 0>(B, C, ist, T, X, Y, e, b, r, d, ncol, nc, warp, lane); break;
-            }
-            panel_mma<RP, true>(sBK, Y, X, T, r, nc, B.tabs, warp, lane);
-            __syncthreads();
-            continue;
+          if (tid < nbi) {
+            ItemState &S = ist[tid];
+            int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
+            for (int i = 1; i < m; ++i)
+              if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
+                sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
+                lp[nf] = S.lpole[i];
+                nf++;
+              }
+            long sig = 0;
+            if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
+            if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
+            S.taboff = B.tab_off[b] + sig * 2 * r * dd;
           }
-          if (tid < nbi) ist[tid].taboff = edge_table_offset(B, C, ist[tid], e, b, r, dd);
           // (a) gc = K^-1 T (in place), then Gt = W gc (into X)
           panel_trsm_mma<RP>(sLU, T, r, nc, tid, warp, lane);
           panel_mma<RP, false>(sW, T, nullptr, X, r, nc, nullptr, warp, lane);
