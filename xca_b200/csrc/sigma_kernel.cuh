@@ -78,10 +78,7 @@ struct ItemState {
   double scale;          // prefactor * prefactor sign * order / direction sign
   int lpole[MAXM];       // pole index of line i (i >= 1)
   int caseA[MAXM];       // line i in case 4(a): K on its end vertices; else 4(b): K on the edges it spans
-  long opoff;            // per-step: operator slab offset of this item
   long taboff;           // per-step: edge-table offset of this item
-  int kcol;              // per-step: K-table column of the vertex (-1: none), sign in kneg
-  int kneg;
   int keep;              // 1e-16 guard outcome
 };
 

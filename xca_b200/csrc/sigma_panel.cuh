@@ -417,22 +417,33 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) edge_tables_panel_kernel(Dev
   }
 }
 
+// One vertex of a class: operator table base (F, F^dag, or their pole-resolved reflected forms), the
+// operator's index within its set, the vertex's hybridization line and the sign of its K factor.
+struct VertexOp {
+  long base;
+  int qo, line, ks;
+  bool pole;
+};
+
 // Vertex pass: X(t) <- k(t) F T(t) for every item of the batch (multiply_left_vertex), thread per output
 // column over a stride of tau rows.  DV > 0 is the input block dimension known at compile time (the
 // operator row is held in registers across the rows and every load of a row is issued before its
 // fused multiply-adds); DV = 0 takes dv at run time.  The operation order is the same either way.
 template <int RP, int DV>
-__device__ __forceinline__ void vertex_pass(const DevBasis &B, const ItemState *ist, const double *T, double *X, const int *rowpos,
-                                            int r, int dv, int dvp, int ncol, int nbi, int tid) {
+__device__ __forceinline__ void vertex_pass(const DevBasis &B, const VertexOp &vo, const ItemState *ist, const double *T, double *X,
+                                            const int *rowpos, int r, int dv, int dvp, int ncol, int nbi, int tid) {
   constexpr int NC = PanelCfg<RP>::LDP, NT = PANEL_THREADS;
   const int dci = dv * ncol, dco = dvp * ncol, nc = nbi * dco, tpc = NT / nc, c = tid % nc, t0 = tid / nc;
   if (t0 >= tpc) return;
+  const int p = B.p;
   const int j = c / dco, e = c - j * dco, x = e / ncol, z = e - x * ncol;
   const ItemState &S = ist[j];
-  const double *F = B.ops + S.opoff + x * dv;
-  const double *kt = S.kcol >= 0 ? (S.kneg ? B.kitm : B.kitp) + S.kcol : nullptr;
+  const int l = S.lpole[vo.line];
+  const long opoff = vo.base + (vo.pole ? (long)vo.qo * p + l : (long)vo.qo) * dvp * dv;
+  const double *F = B.ops + opoff + x * dv;
+  // a line in its case-A form contributes its K factor at both of its vertices
+  const double *kt = (vo.line > 0 && S.caseA[vo.line]) ? (vo.ks < 0 ? B.kitm : B.kitp) + l : nullptr;
   const double *Tc = T + j * dci + z;
-  const int p = B.p;
   double f[DV > 0 ? DV : 1];
 #pragma unroll
   for (int y = 0; y < DV; ++y) f[y] = F[y];
@@ -691,32 +702,22 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
           const int b = C.ind_path[v - 1];
           const int dv = C.bdims[v], dvp = C.bdims[v + 1];
           const int s = C.vset[v], qo = C.vqo[v];
-          if (tid < nbi) {
-            ItemState &S = ist[tid];
-            const int l = S.lpole[line];
-            long off;
-            switch (C.vkind[v]) {
-              case 0: off = B.F_off[s * B.nb + b] + (long)qo * dvp * dv; break;
-              case 1: off = B.Fd_off[s * B.nb + b] + (long)qo * dvp * dv; break;
-              case 2: off = B.Fb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
-              default: off = B.Fdb_off[s * B.nb + b] + ((long)qo * p + l) * dvp * dv; break;
-            }
-            S.opoff = off;
-            S.kcol = -1;
-            if (line > 0 && S.caseA[line]) {
-              const int fwd = (C.fbmask >> line) & 1;
-              const int ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
-              S.kcol = l;
-              S.kneg = ks < 0;
-            }
+          // operator base of this vertex (uniform); the pole-dependent part and the K factor are per item
+          const int vk = C.vkind[v];
+          const long vbase = vk == 0 ? B.F_off[s * B.nb + b] : vk == 1 ? B.Fd_off[s * B.nb + b]
+                           : vk == 2 ? B.Fb_off[s * B.nb + b] : B.Fdb_off[s * B.nb + b];
+          int ks = 0;
+          if (line > 0) {
+            const int fwd = (C.fbmask >> line) & 1;
+            ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
           }
-          __syncthreads();
+          const VertexOp vo{vbase, qo, line, ks, vk >= 2};
           switch (dv) {
-            case 1: vertex_pass<RP, 1>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
-            case 2: vertex_pass<RP, 2>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
-            case 3: vertex_pass<RP, 3>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
-            case 4: vertex_pass<RP, 4>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
-            default: vertex_pass<RP, 0>(B, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+            case 1: vertex_pass<RP, 1>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+            case 2: vertex_pass<RP, 2>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+            case 3: vertex_pass<RP, 3>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+            case 4: vertex_pass<RP, 4>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+            default: vertex_pass<RP, 0>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
           }
           __syncthreads();
           double *tmp = T; T = X; X = tmp;
