@@ -17,6 +17,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -59,13 +60,33 @@ def build_model():
     return m, G
 
 
+MODEL_FIXTURE = os.path.join(ROOT, "oracle", "fixtures", "kanamori_2orb_beta20_L200_eps1e-12.npz")
+
+
+def cpu_model():
+    """(CPU model name, logical CPUs usable by this process) of the host."""
+    name = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                name = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except AttributeError:
+        usable = os.cpu_count()
+    return name, usable
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
 
     def __init__(self, index):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        fd, self.path = tempfile.mkstemp(prefix="xca_clocks_", suffix=".csv")
+        os.close(fd)
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
@@ -85,7 +106,9 @@ class ClockSampler:
         self.proc.wait()
         self.f.close()
         sm, smax, reasons = [], [], set()
-        for line in open(self.path):
+        lines = open(self.path).read().splitlines()
+        os.unlink(self.path)
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -103,46 +126,43 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def profiled_traffic():
-    """DRAM bytes (read + write) per Sigma-kernel launch of this workload from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "sigma_panel_kernel_kanamori_2orb_tca.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if "traffic_bytes_per_launch:" in line:
-            try:
-                return int(line.split("traffic_bytes_per_launch:")[1].split("*")[0].strip())
-            except ValueError:
-                return None
-    return None
-
-
-def cpu_sigma_rate(m, G, seconds, nthreads=0):
-    """Oracle (CPU restatement) timed on a bounded random sample of flat indices of every topology;
-    returns (evals/s extrapolated to the full evaluation, threads used, sample description)."""
+def cpu_sigma_sample(seconds, nthreads=0, seed=7):
+    """The oracle (CPU restatement of the reference's path) on a bounded random sample of flat indices of
+    every topology of the benchmark model, loaded from the oracle's model file (no product library is
+    mapped).  Returns (evals/s extrapolated to the full evaluation, wall seconds of the sample, threads,
+    sample description)."""
     from oracle import oracle as O
-    d = O.Dlr(m.lam, m.eps, rf=m.rf, it=m.it)
-    ev = O.Evaluator(d, m.beta, m.hyb_poles, m.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
-    topos = topologies()
-    rng = np.random.default_rng(7)
-    nmax = [ev.num_self_energy_backbones(t) for _, t, _ in topos]
+    _, ev, G = O.Evaluator.from_fixture(MODEL_FIXTURE)
+    topos = [np.array(t, np.int32) for order in (1, 2, 3) for _, t in O.connected_pairings(order)]
+    rng = np.random.default_rng(seed)
+    nmax = [ev.num_self_energy_backbones(t) for t in topos]
     per_topo = seconds / len(topos)
-    total_time = 0.0
-    sampled = 0
-    for (_, t, _), nm in zip(topos, nmax):
+    total_est, wall, sampled = 0.0, 0.0, 0
+    for t, nm in zip(topos, nmax):
         k = min(nm, 64)
         while True:
             fix = np.sort(rng.choice(nm, size=k, replace=False))
             t0 = time.perf_counter()
             ev.compute_self_energy(G, t, f_ix=fix, nthreads=nthreads)
             dt = time.perf_counter() - t0
+            wall += dt
             if dt > 0.2 * per_topo or k == nm:
                 break
             k = min(nm, max(k * 2, int(k * 0.5 * per_topo / max(dt, 1e-6))))
-        total_time += dt * nm / k
+        total_est += dt * nm / k
         sampled += k
-    threads = nthreads or int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
-    return 1.0 / total_time, threads, f"{sampled} random flat indices over {len(topos)} topologies, extrapolated to {sum(nmax)}"
+    threads = nthreads or int(os.environ.get("OMP_NUM_THREADS", cpu_model()[1]))
+    return (1.0 / total_est, wall, threads,
+            f"{sampled} random flat indices over {len(topos)} topologies, time extrapolated to all {sum(nmax)} flat indices")
+
+
+def cpu_baseline_object(seconds):
+    """cpu_baseline of the GPU arm: all host threads, plus a 1-thread figure on a shorter sample."""
+    v, wall, cores, sample = cpu_sigma_sample(seconds)
+    v1, _, _, _ = cpu_sigma_sample(max(seconds / 4, 2.0), nthreads=1, seed=8)
+    name, usable = cpu_model()
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample, "value_1thread": v1,
+            "cpu_model": name, "host_cpus": usable, "sample_wall_s": wall}
 
 
 def run_serving(args):
@@ -188,22 +208,30 @@ def run_serving(args):
 
 
 def run_reference(args, rank):
-    """--impl reference: the CPU restatement of the reference's path on the host cores."""
+    """--impl reference: the CPU restatement of the reference's path (oracle) on the host cores.  One step is
+    a bounded random sample of the benchmark evaluation; its time is extrapolated to the full evaluation."""
     if rank != 0:
         return
-    m, G = build_model()
-    vals = []
-    for _ in range(args.warmup):
-        cpu_sigma_rate(m, G, min(args.cpu_seconds, 5.0) / 2)
-    for _ in range(args.steps):
-        v, cores, sample = cpu_sigma_rate(m, G, args.cpu_seconds / max(args.steps, 1))
+    per_step = args.cpu_seconds / max(args.steps, 1)
+    for w in range(args.warmup):
+        cpu_sigma_sample(min(per_step, 2.0) / 2, seed=100 + w)
+    vals, walls = [], []
+    sample = ""
+    cores = 0
+    for k in range(args.steps):
+        v, wall, cores, sample = cpu_sigma_sample(per_step, seed=200 + k)
         vals.append(v)
+        walls.append(wall)
     v = float(np.median(vals))
+    v1, _, _, _ = cpu_sigma_sample(min(per_step, 4.0), nthreads=1, seed=300)
+    name, usable = cpu_model()
     out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "c128",
-           "data": "synthetic", "impl": "reference",
-           "config": {"workload": CONFIG_NAME, "l2": "inputs < L2; CPU run"},
-           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+           "ms_per_step": 1000.0 * float(np.mean(walls)), "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+           "dtype": "c128", "data": "synthetic", "impl": "reference",
+           "config": {"workload": CONFIG_NAME, "l2": "inputs < L2; CPU run",
+                      "step": "one bounded random sample of the evaluation; value = 1 / (sample time extrapolated to all flat indices)"},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample, "value_1thread": v1,
+                            "cpu_model": name, "host_cpus": usable},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -308,11 +336,9 @@ def main():
     peak = max(peak_fma, peak_mma)
     kernel_s = sigma_ms * 1e-3 / max(args.steps, 1)
     achieved = alg_flops / world / kernel_s / 1e12 if kernel_s > 0 else None
-    traffic = profiled_traffic()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, sample = cpu_sigma_rate(m, G, args.cpu_seconds)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        cpu = cpu_baseline_object(args.cpu_seconds)
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": t_step, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
@@ -320,7 +346,7 @@ def main():
                "config": {"workload": CONFIG_NAME, "r": int(ev.r), "poles": int(ev.p), "items_per_step": int(items),
                           "alg_gflop_per_step": alg_flops / 1e9, "l2": "flushed (256 MiB write) before every timed step"},
                "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                            "frac": (achieved / peak) if achieved else None, "traffic": None,
                             "kernel": "sigma_panel_kernel",
                             "peak_source": "max of the FP64 FMA (xca_fp64_fma_probe) and FP64 tensor-core MMA "
                                            "(xca_fp64_mma_probe) throughputs measured on this GPU",

@@ -31,6 +31,13 @@ extern "C" {
 #define XCA_ERR_CUDA 3
 #define XCA_ERR_UNSUPPORTED 4
 
+/* Precision / summation modes of the Sigma evaluation (xca_set_precision_mode). */
+#define XCA_PREC_FP64 0          /* FP64, items summed into Sigma with atomics (fastest; order varies run to run) */
+#define XCA_PREC_FP64_ORDERED 1  /* FP64, fixed summation order: reproducible bit for bit from run to run */
+
+/* Pole tuples per work unit in XCA_PREC_FP64_ORDERED (part of the definition of its summation order). */
+#define XCA_ORDERED_UNIT_TUPLES 64
+
 typedef struct xca_ctx xca_ctx;
 
 /* Message of the last failing call on this thread (empty string if none). */
@@ -210,6 +217,19 @@ int xca_copy_to_host(xca_ctx *ctx, double *host, const double *dev, long n_doubl
 
 /* Wait for the context's stream. */
 int xca_synchronize(xca_ctx *ctx);
+
+/* Precision / summation mode of the context's Sigma evaluations (the reference has one mode, FP64 with
+ * the sum order of its flat-index loop, c++/triqs_xca/block_sparse_backbone.cpp:407-435; this argument
+ * takes the place of the precision_mode of the evaluation call).  XCA_PREC_FP64 (default): items reach
+ * Sigma through atomic adds.  XCA_PREC_FP64_ORDERED: the same items summed in a fixed order — per output
+ * block, path classes in enumeration order (directions, orbital tuple, symmetry set), within a class runs
+ * of XCA_ORDERED_UNIT_TUPLES pole tuples in order, within a run the items in order, each partial sum
+ * starting from zero; for a flat-index list (xca_compute_self_energy with f_ix) the items in list order.
+ * Applies to xca_compute_self_energy, xca_compute_self_energy_device and the single-shard
+ * xca_compute_self_energy_device_shard (n_shards > 1 gives XCA_ERR_UNSUPPORTED); the allocation-free
+ * variant always uses XCA_PREC_FP64.  Unknown modes give XCA_ERR_UNSUPPORTED. */
+int xca_set_precision_mode(xca_ctx *ctx, int mode);
+int xca_get_precision_mode(xca_ctx *ctx, int *mode);
 
 /* Number of kernels this library launched on the context since creation. */
 int xca_kernel_launches(xca_ctx *ctx, long *out);

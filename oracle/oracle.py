@@ -12,6 +12,7 @@ Layout conventions (shared with the product's C-ABI):
 """
 
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -54,6 +55,7 @@ def lib():
         L.ora_num_spgf_backbones.restype = LG
         L.ora_num_spgf_backbones.argtypes = [P, I, ip]
         L.ora_sigma.argtypes = [P, dp, I, ip, lp, LG, I, dp, lp, dp]
+        L.ora_sigma_ordered.argtypes = [P, dp, I, ip, LG, I, dp, lp]
         L.ora_items.restype = LG
         L.ora_items.argtypes = [P, dp, I, ip, LG, LG, lp, LG]
         L.ora_spgf.argtypes = [P, dp, I, ip, lp, LG, I, dp]
@@ -186,6 +188,31 @@ class Evaluator:
             raise ValueError(lib().ora_last_error().decode())
         self.r = dlr.r
 
+    @classmethod
+    def from_fixture(cls, path):
+        """(Dlr, Evaluator, G) of a model written by ``oracle/make_model_fixture.py`` (packed operator arrays)."""
+        z = np.load(path)
+        dlr = Dlr(float(z["lam"]), float(z["eps"]), rf=z["rf"], it=z["it"])
+        self = cls.__new__(cls)
+        self.dlr = dlr
+        self.beta = float(z["beta"])
+        self.dims = np.ascontiguousarray(z["dims"], dtype=np.int32)
+        self.labels = np.ascontiguousarray(z["labels"], dtype=np.int64)
+        self.n = len(self.labels)
+        self.poles = np.ascontiguousarray(z["hyb_poles"], dtype=float)
+        self.coeffs = _c(z["hyb_coeffs"])
+        self.p = len(self.poles)
+        self._fi = np.ascontiguousarray(z["F_index"], dtype=np.int32)
+        self._fd = _c(z["F_data"])
+        self._gi = np.ascontiguousarray(z["Fd_index"], dtype=np.int32)
+        self._gd = _c(z["Fd_data"])
+        self._h = lib().ora_eval_new(dlr._h, self.beta, self.p, _dp(self.poles), _dp(self.coeffs), self.n, _lp(self.labels),
+                                     len(self.dims), _ip(self.dims), _ip(self._fi), _dp(self._fd), _ip(self._gi), _dp(self._gd))
+        if not self._h:
+            raise ValueError(lib().ora_last_error().decode())
+        self.r = dlr.r
+        return dlr, self, self.unpack(_c(z["G"]))
+
     def __del__(self):
         if getattr(self, "_h", None) and _LIB is not None:
             _LIB.ora_eval_free(self._h)
@@ -225,6 +252,16 @@ class Evaluator:
         if stats is not None:
             stats["items"] = stats.get("items", 0) + int(items[0])
             stats["flops"] = stats.get("flops", 0.0) + float(flops[0])
+        return self.unpack(out)
+
+    def compute_self_energy_ordered(self, G, topology, unit=64, nthreads=0):
+        """``compute_self_energy(G, topology)`` with the additions into Sigma in the fixed order of the
+        device's ordered mode (path classes in order, runs of ``unit`` pole tuples, items in order)."""
+        t = np.ascontiguousarray(topology, dtype=np.int32)
+        g = self.pack(G)
+        out = np.empty_like(g)
+        items = np.zeros(1, np.int64)
+        _check(lib().ora_sigma_ordered(self._h, _dp(g), t.shape[0], _ip(t), int(unit), int(nthreads), _dp(out), _lp(items)))
         return self.unpack(out)
 
     def item_list(self, G, topology, f0=0, f1=None):
@@ -286,13 +323,17 @@ def connected_pairings(order):
             yield parity, pairing
 
 
-def sigma_total(ev, G, max_order, nthreads=0, stats=None, orders=None):
+def sigma_total(ev, G, max_order, nthreads=0, stats=None, orders=None, ordered=False):
     """``BlockSparseSolver.eval_pseudo_particle_self_energy`` (``block_sparse_solver.py:597-640``):
-    Sigma = sum_order sum_topology (-1)^order * parity * (-1)^(order+1) * compute_self_energy."""
+    Sigma = sum_order sum_topology (-1)^order * parity * (-1)^(order+1) * compute_self_energy.
+    ``ordered``: each topology summed in the fixed order of the device's ordered mode."""
     Sig = [np.zeros_like(_c(g)) for g in G]
     for order in (orders if orders is not None else range(1, max_order + 1)):
         for sign, topo in connected_pairings(order):
-            part = ev.compute_self_energy(G, np.array(topo, np.int32), nthreads=nthreads, stats=stats)
+            if ordered:
+                part = ev.compute_self_energy_ordered(G, np.array(topo, np.int32), nthreads=nthreads)
+            else:
+                part = ev.compute_self_energy(G, np.array(topo, np.int32), nthreads=nthreads, stats=stats)
             fac = (-1) ** order * sign * (-1) ** (order + 1)
             for b in range(len(Sig)):
                 Sig[b] += fac * part[b]
@@ -309,11 +350,15 @@ def spgf_total(ev, G, max_order, nthreads=0):
 
 
 def trace_beta(dlr, G):
-    """``trace`` (``c++/triqs_xca/block_sparse.cpp:852-861``): sum_b Tr G_b(beta) by DLR evaluation."""
+    """``trace`` (``c++/triqs_xca/block_sparse.cpp:852-861``): sum_b Tr G_b(beta) by DLR evaluation, the
+    diagonal and the blocks summed one after another from zero (``nda::trace`` and ``trace +=``)."""
     tot = 0.0 + 0.0j
     for g in G:
-        gc = dlr.vals2coefs(g)
-        tot += np.trace(dlr.coefs2eval(gc, 1.0))
+        gb = dlr.coefs2eval(dlr.vals2coefs(g), 1.0)
+        tr = 0.0 + 0.0j
+        for x in range(gb.shape[0]):
+            tr += complex(gb[x, x])
+        tot += tr
     return tot
 
 
@@ -329,22 +374,26 @@ def solve_dyson(dlr, beta, G0, Sig, eta):
 def normalize(dlr, beta, G, eta):
     """``normalize_pseudo_particle_gf`` (``block_sparse_solver.py:427-449``)."""
     Z = -trace_beta(dlr, G).real
-    deta = np.log(np.abs(Z)) / beta
-    tau = dlr.tau(beta)
-    return [g * np.exp(-tau * deta)[:, None, None] for g in G], eta + deta
+    deta = math.log(abs(Z)) / beta
+    tabs = dlr_ref.rel2abs(dlr.it)
+    fac = np.array([math.exp(-((beta * float(t)) * deta)) for t in tabs])
+    return [g * fac[:, None, None] for g in G], eta + deta
 
 
-def solve(dlr, ev, beta, G0, max_order, tol, maxiter, mix=1.0, spgf_max_order=None, nthreads=0, verbose=False):
+def solve(dlr, ev, beta, G0, max_order, tol, maxiter, mix=1.0, spgf_max_order=None, nthreads=0, verbose=False, ordered=False,
+          G_init=None, eta_init=0.0):
     """``BlockSparseSolver.solve`` with 'classic' normalization (``block_sparse_solver.py:240-355``).
+    ``ordered``: Sigma summed in the fixed order of the device's ordered mode.  ``G_init``/``eta_init``:
+    start from a previous solution (the reference's solver keeps self.G and self.eta between solves).
 
     Returns (G, Sigma, eta, g_spgf, n_iter, diff_G)."""
-    G = [g.copy() for g in G0]
-    eta = 0.0
+    G = [g.copy() for g in (G0 if G_init is None else G_init)]
+    eta = eta_init
     it = 0
     diff = np.inf
     Sig = None
     for it in range(1, maxiter + 1):
-        Sig = sigma_total(ev, G, max_order, nthreads=nthreads)
+        Sig = sigma_total(ev, G, max_order, nthreads=nthreads, ordered=ordered)
         Gn = solve_dyson(dlr, beta, G0, Sig, eta)
         Gn, eta = normalize(dlr, beta, Gn, eta)
         diff = max(np.max(np.abs(a - b)) for a, b in zip(Gn, G))

@@ -1056,6 +1056,86 @@ int ora_sigma(void *ev, const double *G_, int m, const int *topo, const long *fi
   } catch (std::exception &e) { g_err = e.what(); return 1; }
 }
 
+// compute_self_energy(G, topology) summed in the fixed order of the device's ordered mode (the items are
+// the reference's; only the order of the additions into Sigma is fixed here, so two runs, and this
+// restatement and the device, agree bit for bit).  Per output block b: the path classes (fb_ix, o_ix,
+// p_kap) in that order, each class's value the sum over runs of `unit` consecutive pole tuples (p_ix
+// ascending), each run's value the sum of its items in p_ix order; every partial sum starts from zero.
+// The runs of one (fb_ix, o_ix) group are evaluated in parallel.
+int ora_sigma_ordered(void *ev, const double *G_, int m, const int *topo, long unit, int nthreads, double *Sig_out, long *n_items) {
+  try {
+    auto *E = (Evaluator *)ev;
+    if (unit < 1) throw std::invalid_argument("unit must be positive");
+    const cd *G = (const cd *)G_;
+    Backbone B0(m, topo, E->n, E->p, false);
+    BlockG g = make_G(*E, G);
+    std::vector<size_t> off(E->nb + 1, 0);
+    for (int b = 0; b < E->nb; ++b) off[b + 1] = off[b] + (size_t)E->r * E->dims[b] * E->dims[b];
+    std::vector<cd> Sig(off[E->nb], 0.0);
+    const long omax = B0.o_ix_max, npt = B0.p_ix_max, fbmax = B0.fb_ix_max;
+    const long nruns = (npt + unit - 1) / unit;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+    long items = 0;
+    for (long fb = 0; fb < fbmax; ++fb)
+      for (long o = 0; o < omax; ++o) {
+        // the valid (b, p_kap) classes of this group do not depend on the pole tuple
+        std::vector<std::pair<int, int>> cls;
+        {
+          Backbone B(m, topo, E->n, E->p, false);
+          Work w;
+          B.set_flat_index(o + omax * (npt * fb), E->poles_beta);
+          find_paths(*E, B, g, w, [&](int b, int pk, int) { cls.emplace_back(b, pk); });
+        }
+        if (cls.empty()) continue;
+        const size_t nc = cls.size();
+        std::vector<std::vector<cd>> part(nruns * nc);
+        long grp_items = 0;
+#pragma omp parallel num_threads(nthreads) reduction(+ : grp_items)
+        {
+          Backbone B(m, topo, E->n, E->p, false);
+          Work w;
+          alloc_work(*E, w);
+#pragma omp for schedule(dynamic, 1)
+          for (long run = 0; run < nruns; ++run) {
+            for (size_t k = 0; k < nc; ++k) part[run * nc + k].assign((size_t)E->r * E->dims[cls[k].first] * E->dims[cls[k].first], 0.0);
+            for (long pix = run * unit; pix < std::min(npt, (run + 1) * unit); ++pix) {
+              B.set_flat_index(o + omax * (pix + npt * fb), E->poles_beta);
+              size_t k = 0;
+              find_paths(*E, B, g, w, [&](int b, int pk, int pm) {
+                while (k < nc && !(cls[k].first == b && cls[k].second == pk)) ++k;
+                if (k == nc) throw std::logic_error("class set changed with the pole tuple");
+                eval_fixed(*E, B, g, w, b, pk, pm, part[run * nc + k]);
+              });
+            }
+            grp_items += w.items;
+            w.items = 0;
+          }
+        }
+        items += grp_items;
+        for (size_t k = 0; k < nc; ++k) {
+          const int b = cls[k].first;
+          std::vector<cd> cp((size_t)E->r * E->dims[b] * E->dims[b], 0.0);
+          for (long run = 0; run < nruns; ++run)
+            for (size_t x = 0; x < cp.size(); ++x) cp[x] += part[run * nc + k][x];
+          for (size_t x = 0; x < cp.size(); ++x) Sig[off[b] + x] += cp[x];
+        }
+      }
+    for (int b = 0; b < E->nb; ++b) {
+      double mx = 0;
+      for (size_t x = off[b]; x < off[b + 1]; ++x) mx = std::max(mx, std::abs(Sig[x]));
+      if (mx < 1e-16)
+        for (size_t x = off[b]; x < off[b + 1]; ++x) Sig[x] = 0;
+    }
+    std::copy(Sig.begin(), Sig.end(), (cd *)Sig_out);
+    if (n_items) *n_items = items;
+    return 0;
+  } catch (std::exception &e) { g_err = e.what(); return 1; }
+}
+
 // Valid item list of find_path_self_energy for flat indices [f0, f1): rows (f_ix, b_ix, p_kap, ind_path[0..2m-2]).
 long ora_items(void *ev, const double *G_, int m, const int *topo, long f0, long f1, long *out, long max_rows) {
   auto *E = (Evaluator *)ev;

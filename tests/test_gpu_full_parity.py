@@ -1,0 +1,200 @@
+"""Full-size GPU parity of the Sigma evaluation and of self-consistent solves against the oracle.
+
+Two summation modes are checked.  In the ordered mode (``precision_mode = 'fp64_ordered'``) the device
+adds the items into Sigma in a fixed order that the oracle's ``compute_self_energy_ordered`` restates;
+since every item is computed with the oracle's rounding, the whole evaluation must agree bit for bit
+(tolerance 0).  The fast mode (the one ``bench.py`` times) adds them with atomics in a varying order; it
+must agree with the same golden values to 1e-12 relative per tau node (the error at node t divided by
+the largest |Sigma| at that node over all blocks).
+
+Golden values come from ``tests/golden/make_sigma_golden.py`` (the oracle on all flat indices).
+Self-consistent solves run the oracle's restated solve loop live on the same DLR nodes as the device.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from xca_b200 import models
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL_FAST_PER_NODE = 1e-12
+
+
+def _load(name):
+    path = os.path.join(GOLDEN, f"sigma_{name}_ordered.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"golden file {path} not generated")
+    return np.load(path)
+
+
+def _device(fx, builder):
+    from xca_b200.block_sparse import BlockOpSymQuartet, DiagramEvaluator
+    beta, lam, eps = float(fx["beta"]), float(fx["lam"]), float(fx["eps"])
+    rf, it = fx["rf"], fx["it"]
+    m = builder(rf, it, beta, lam, eps)
+    assert np.array_equal(m.dims, fx["dims"])
+    Fq = BlockOpSymQuartet(m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks, m.dims)
+    ev = DiagramEvaluator.from_arrays(beta, lam, eps, rf, it, m.hyb_poles, m.hyb_coeffs, Fq)
+    G = ev.unpack(fx["G"].astype(np.complex128))
+    return ev, m, G
+
+
+def _per_node_rel(ev, a_flat, b_flat):
+    """max over tau nodes of max|a - b| / max|b| at that node (all blocks)."""
+    r = ev.r
+    num = np.zeros(r)
+    den = np.zeros(r)
+    off = 0
+    for d in ev.dims:
+        sz = r * d * d
+        a = a_flat[off:off + sz].reshape(r, -1)
+        b = b_flat[off:off + sz].reshape(r, -1)
+        num = np.maximum(num, np.max(np.abs(a - b), axis=1))
+        den = np.maximum(den, np.max(np.abs(b), axis=1))
+        off += sz
+    return float(np.max(num / np.maximum(den, 1e-300)))
+
+
+def _device_topology(ev, G, topo, scale=1.0):
+    buf_g = ev.device_buffer(30, ev.slab)
+    buf_s = ev.device_buffer(31, ev.slab)
+    ev.to_device(buf_g, ev.pack(G).real)
+    ev.zero_device(buf_s, ev.slab)
+    ev.compute_self_energy_device(buf_g, topo, scale, buf_s)
+    return ev.to_host(buf_s, ev.slab)
+
+
+@pytest.mark.parametrize("name,builder", [("kanamori_2orb", models.kanamori_2orb), ("t2g_oca", models.t2g_3orb),
+                                          ("t2g_tca", models.t2g_3orb)])
+def test_full_sigma_ordered_bit_identical(name, builder):
+    fx = _load(name)
+    ev, m, G = _device(fx, builder)
+    ev.precision_mode = "fp64_ordered"
+    for k in range(int(fx["n_topologies"])):
+        topo, gold = fx[f"topo_{k}"], fx[f"sigma_{k}"]
+        # host API (the reference's compute_self_energy(G, topology)) and the device-resident call
+        host = np.concatenate([s.real.ravel() for s in ev.compute_self_energy(G, topo)])
+        dev = _device_topology(ev, G, topo)
+        assert np.array_equal(host, gold), (name, topo.tolist(), float(np.max(np.abs(host - gold))))
+        nz = np.abs(gold) > 0
+        assert np.array_equal(dev[nz], gold[nz]), (name, topo.tolist())
+        # and again: the ordered mode is reproducible run to run
+        assert np.array_equal(_device_topology(ev, G, topo), dev)
+
+
+@pytest.mark.parametrize("name,builder", [("kanamori_2orb", models.kanamori_2orb), ("t2g_oca", models.t2g_3orb),
+                                          ("t2g_tca", models.t2g_3orb)])
+def test_full_sigma_fast_mode_per_node(name, builder):
+    # the batched, atomically accumulated path that bench.py times (RP = 48 for the Kanamori basis)
+    fx = _load(name)
+    ev, m, G = _device(fx, builder)
+    assert ev.precision_mode == "fp64"
+    worst = 0.0
+    for k in range(int(fx["n_topologies"])):
+        topo, gold = fx[f"topo_{k}"], fx[f"sigma_{k}"]
+        worst = max(worst, _per_node_rel(ev, _device_topology(ev, G, topo), gold))
+    print(f"{name}: fast mode vs golden, worst per-node relative error {worst:.3e}")
+    assert worst <= TOL_FAST_PER_NODE
+
+
+def test_full_sigma_total_kanamori_fast_mode():
+    # Sigma of orders 1..3 with the reference's signs, accumulated on the device as the bench step does
+    fx = _load("kanamori_2orb")
+    ev, m, G = _device(fx, models.kanamori_2orb)
+    buf_g = ev.device_buffer(30, ev.slab)
+    buf_s = ev.device_buffer(31, ev.slab)
+    ev.to_device(buf_g, ev.pack(G).real)
+    ev.zero_device(buf_s, ev.slab)
+    gold = np.zeros(ev.slab)
+    facs = [fac for order in (1, 2, 3) for fac, _ in
+            [((-1) ** order * sign * (-1) ** (order + 1), t) for sign, t in O.connected_pairings(order)]]
+    for k, fac in enumerate(facs):
+        ev.compute_self_energy_device(buf_g, fx[f"topo_{k}"], float(fac), buf_s)
+        gold = gold + fac * fx[f"sigma_{k}"]
+    got = ev.to_host(buf_s, ev.slab)
+    rel = _per_node_rel(ev, got, gold)
+    print(f"Sigma orders 1-3: worst per-node relative error {rel:.3e}")
+    assert rel <= TOL_FAST_PER_NODE
+
+
+def _anderson_solver(precision):
+    from xca_b200.block_sparse_solver import BlockSparseSolver
+    from xca_b200.pycppdlr import MeshDLRImTime
+    beta, lam, eps = 10.0, 100.0, 1e-10
+    mesh = MeshDLRImTime(beta=beta, statistic="Fermion", w_max=lam / beta, eps=eps)
+    m = models.anderson(mesh.dlr_rf, mesh.dlr_it.it, beta, lam, eps)
+    S = BlockSparseSolver(m.ad, beta, lam / beta, eps, precision=precision)
+    delta = np.zeros((S.r, 2, 2), np.complex128)
+    dv = models.bethe_delta(beta, S.it)
+    delta[:, 0, 0] = dv
+    delta[:, 1, 1] = dv
+    S.Delta_tau = delta
+    d = O.Dlr(lam, eps, rf=S.rf, it=S.it)
+    return S, m, d, beta
+
+
+def _oracle_eval(d, m, S, beta):
+    return O.Evaluator(d, beta, S.hyb_poles, S.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
+
+
+def _max_diff(A, B):
+    return max(float(np.max(np.abs(a - b))) for a, b in zip(A, B))
+
+
+def test_anderson_nca_then_oca_ordered_vs_oracle():
+    # the single-orbital Anderson solve as written: NCA to 1e-10, then OCA from the NCA solution
+    S, m, d, beta = _anderson_solver("fp64_ordered")
+    S.solve(max_order=1, tol=1e-10, maxiter=60)
+    n1 = S.n_ppsc_iter
+    S.solve(max_order=2, tol=1e-10, maxiter=60)
+    ev = _oracle_eval(d, m, S, beta)
+    G1, _, e1, _, it1, _ = O.solve(d, ev, beta, m.G0, 1, 1e-10, 60, spgf_max_order=0, ordered=True)
+    G, Sig, eta, g, it2, diff = O.solve(d, ev, beta, m.G0, 2, 1e-10, 60, spgf_max_order=2, ordered=True, G_init=G1, eta_init=e1)
+    print(f"NCA->OCA: iterations device {n1}+{S.n_ppsc_iter}, oracle {it1}+{it2}; |dG| {_max_diff(S.G, G):.2e}, "
+          f"|dSigma| {_max_diff(S.Sigma, Sig):.2e}, |deta| {abs(S.eta - eta):.2e}, |dg| {np.max(np.abs(S.G_tau - g)):.2e}")
+    assert (n1, S.n_ppsc_iter) == (it1, it2)
+    assert S.diff_G < 1e-10 and diff < 1e-10
+    assert _max_diff(S.G, G) <= 1e-14
+    assert _max_diff(S.Sigma, Sig) <= 1e-14 * max(1.0, max(float(np.max(np.abs(s))) for s in Sig))
+    assert abs(S.eta - eta) <= 1e-14
+    assert float(np.max(np.abs(S.G_tau - g))) <= 1e-13
+
+
+def test_anderson_tca_solve_ordered_vs_oracle():
+    S, m, d, beta = _anderson_solver("fp64_ordered")
+    S.solve(max_order=3, tol=1e-10, maxiter=60)
+    ev = _oracle_eval(d, m, S, beta)
+    G, Sig, eta, g, n_iter, diff = O.solve(d, ev, beta, m.G0, 3, 1e-10, 60, spgf_max_order=3, ordered=True)
+    print(f"TCA: iterations device {S.n_ppsc_iter}, oracle {n_iter}; |dG| {_max_diff(S.G, G):.2e}, "
+          f"|dSigma| {_max_diff(S.Sigma, Sig):.2e}, |deta| {abs(S.eta - eta):.2e}, |dg| {np.max(np.abs(S.G_tau - g)):.2e}")
+    assert S.n_ppsc_iter == n_iter
+    assert S.diff_G < 1e-10 and diff < 1e-10
+    assert _max_diff(S.G, G) <= 1e-14
+    assert abs(S.eta - eta) <= 1e-14
+    assert float(np.max(np.abs(S.G_tau - g))) <= 1e-13
+
+
+def test_t2g_nca_solve_ordered_vs_oracle():
+    from xca_b200.block_sparse_solver import BlockSparseSolver
+    from xca_b200.pycppdlr import MeshDLRImTime
+    beta, lam, eps = 50.0, 500.0, 1e-10
+    mesh = MeshDLRImTime(beta=beta, statistic="Fermion", w_max=lam / beta, eps=eps)
+    m = models.t2g_3orb(mesh.dlr_rf, mesh.dlr_it.it, beta, lam, eps)
+    S = BlockSparseSolver(m.ad, beta, lam / beta, eps, precision="fp64_ordered")
+    rf, it = S.rf, S.it
+    S.Delta_tau = np.asarray(models.kernel(it[:, None], rf[None, :]) @ m.hyb_coeffs.reshape(len(rf), -1)).reshape(S.Delta_tau.shape)
+    S.solve(max_order=1, tol=1e-8, maxiter=40)
+    d = O.Dlr(lam, eps, rf=rf, it=it)
+    ev = O.Evaluator(d, beta, S.hyb_poles, S.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
+    G, Sig, eta, g, n_iter, diff = O.solve(d, ev, beta, m.G0, 1, 1e-8, 40, spgf_max_order=1, ordered=True)
+    print(f"t2g NCA: iterations device {S.n_ppsc_iter}, oracle {n_iter}; |dG| {_max_diff(S.G, G):.2e}, "
+          f"|deta| {abs(S.eta - eta):.2e}, |dg| {np.max(np.abs(S.G_tau - g)):.2e}")
+    assert S.n_ppsc_iter == n_iter
+    assert _max_diff(S.G, G) <= 1e-10
+    assert abs(S.eta - eta) <= 1e-10
+    assert float(np.max(np.abs(S.G_tau - g))) <= 1e-10

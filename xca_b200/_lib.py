@@ -16,6 +16,12 @@ XCA_ERR_RUNTIME = 2
 XCA_ERR_CUDA = 3
 XCA_ERR_UNSUPPORTED = 4
 
+# precision / summation modes (xca_set_precision_mode)
+XCA_PREC_FP64 = 0
+XCA_PREC_FP64_ORDERED = 1
+XCA_ORDERED_UNIT_TUPLES = 64
+PRECISION_MODES = {"fp64": XCA_PREC_FP64, "fp64_ordered": XCA_PREC_FP64_ORDERED}
+
 _lib = None
 
 D = ctypes.c_double
@@ -69,6 +75,8 @@ SIGNATURES = {
     "xca_copy_to_host": [P, dp, P, L],
     "xca_synchronize": [P],
     "xca_kernel_launches": [P, lp],
+    "xca_set_precision_mode": [P, I],
+    "xca_get_precision_mode": [P, ip],
 }
 _RESTYPES = {"xca_last_error": ctypes.c_char_p}
 

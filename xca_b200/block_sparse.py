@@ -217,6 +217,19 @@ class DiagramEvaluator:
         _lib.check(_lib.lib().xca_trace(self._ctx, _lib.as_dp(g.view(np.float64)), _lib.as_dp(out)))
         return complex(out[0], out[1])
 
+    @property
+    def precision_mode(self):
+        """'fp64' (items summed with atomics) or 'fp64_ordered' (fixed summation order, reproducible bit for bit)."""
+        out = ctypes.c_int()
+        _lib.check(_lib.lib().xca_get_precision_mode(self._ctx, ctypes.byref(out)))
+        return {v: k for k, v in _lib.PRECISION_MODES.items()}[out.value]
+
+    @precision_mode.setter
+    def precision_mode(self, mode):
+        if mode not in _lib.PRECISION_MODES:
+            raise NotImplementedError(f"precision mode {mode!r} is not available ({sorted(_lib.PRECISION_MODES)})")
+        _lib.check(_lib.lib().xca_set_precision_mode(self._ctx, _lib.PRECISION_MODES[mode]))
+
     # ---------------------------------------------------------------- device-resident use
     def dyson_setup(self, G0):
         """Dyson solvers of every block for the atomic propagator G0 (``DysonItPPSC(beta, itops, G0_b)`` for each

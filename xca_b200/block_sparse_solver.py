@@ -28,8 +28,11 @@ _SLOTS = {"G": 10, "Gn": 11, "S": 12}
 
 
 class BlockSparseSolver:
-    def __init__(self, atom_diag, beta, w_max, eps, device=0, verbose=False):
+    def __init__(self, atom_diag, beta, w_max, eps, device=0, verbose=False, precision="fp64"):
+        """``precision``: the evaluator's precision mode, 'fp64' (items summed with atomics) or
+        'fp64_ordered' (fixed summation order: the solve is reproducible bit for bit)."""
         self.ad = atom_diag
+        self.precision = precision
         self.beta = float(beta)
         self.w_max = float(w_max)
         self.eps = float(eps)
@@ -60,6 +63,7 @@ class BlockSparseSolver:
     def init_diagram_evaluator(self):
         self.d = DiagramEvaluator.from_arrays(self.beta, self.beta * self.w_max, self.eps, self.rf, self.it, self.hyb_poles,
                                               self.hyb_coeffs, self.Fq, device=self.device)
+        self.d.precision_mode = self.precision
         self.d.dyson_setup(self.G0)
         self._buf = {k: self.d.device_buffer(slot, self.d.slab) for k, slot in _SLOTS.items()}
 

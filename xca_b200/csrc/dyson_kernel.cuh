@@ -16,21 +16,6 @@
 
 namespace xca {
 
-struct DysonBasis {
-  int r, nb;
-  double beta;
-  const double *LUp, *Wp, *BKp;  // RP x RP column-major (as DevBasis)
-  const int *perm;
-  const double *tabs, *k0, *k1;  // r: absolute t_i, K(0, om_l), K(1, om_l)
-  const double *rf;              // r: DLR frequencies om_l
-  const long *goff;              // nb: block offsets in a packed slab
-  const int *dims;               // nb
-  const long *woff;              // nb: per-block work offsets (6 r d^2 doubles each)
-  const long *moff;              // nb: per-block system matrix offsets ((r d)^2 doubles each)
-  const double *g0, *g0c, *g0t;  // packed slabs: G0 values, K^-1 G0, W K^-1 G0
-  double *work;
-  double *mats;
-};
 
 // K^T z = a for one register-resident row vector, with K = P L U (the factors of lu_factor): U^T y = a
 // row by row (i ascending: subtract U_ki y_k for k < i ascending, then divide by U_ii), L^T w = y
@@ -346,14 +331,17 @@ __global__ void __launch_bounds__(128) trace_beta_kernel(DysonBasis B, const dou
 }
 
 // G(tau_i) <- G(tau_i) exp(-tau_i deta), tau_i = beta t_i (energy_shift_ppgf, block_sparse_solver.py:436-441).
-__global__ void energy_shift_kernel(DysonBasis B, double *__restrict__ G, double deta) {
+// G_b(tau_t) <- G_b(tau_t) * fac[t] for every block, fac[t] = exp(-tau_t deta) (energy_shift_ppgf of
+// normalize_pseudo_particle_gf, python/triqs_xca/block_sparse_solver.py:436-442); the r factors are
+// computed by the caller.
+__global__ void energy_shift_kernel(DysonBasis B, double *__restrict__ G, const double *__restrict__ fac) {
   const int b = blockIdx.y;
   const int dd = B.dims[b] * B.dims[b];
   const long n = (long)B.r * dd;
   double *g = G + B.goff[b];
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
     const int t = (int)(e / dd);
-    g[e] = mul(g[e], exp(-mul(mul(B.beta, B.tabs[t]), deta)));
+    g[e] = mul(g[e], fac[t]);
   }
 }
 

@@ -1,0 +1,39 @@
+// Host-side launchers of the device kernels, one translation unit per kernel family and padded rank
+// (sigma_rp.cu and spgf_rp.cu are compiled once per RP in {32, 48, 64}; dyson.cu holds every rank).
+// The context code in xca_b200.cu calls these; each returns the number of kernels it launched.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "sigma_kernel.cuh"
+#include "spgf_kernel.cuh"
+
+namespace xca {
+
+template <int RP>
+int launch_edge_tables(cudaStream_t s, int nsm, const DevBasis &B, const double *G, const int2 *chunks, int n_chunks);
+
+template <int RP>
+int launch_sigma_panel(cudaStream_t s, int nsm, const DevBasis &B, const ClassRec *classes, const WorkUnit *units, int n_units,
+                       int *counter, const double *G, const SigmaOut &out);
+
+// Usable panel columns of the panel kernels of rank RP.
+template <int RP>
+int panel_width();
+
+template <int RP>
+int launch_correlator(cudaStream_t s, int grid, int warps_per_cta, const DevBasis &B, const CorrBasis &CB, const CorrClass *classes,
+                      const CorrChain *chains, const CorrTerm *terms, const WorkUnit *units, int n_units, int *counter,
+                      const double *G, double *g, double scale, int nmax, double *scratch, long warp_doubles);
+
+template <int RP>
+int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const double *Sigma, double eta, int hermitize, double *rhs,
+                 double *G, int *status);
+
+template <int RP>
+int launch_trace_beta(cudaStream_t s, const DysonBasis &B, const double *G, double *out);
+
+int launch_energy_shift(cudaStream_t s, const DysonBasis &B, double *G, const double *fac);
+int launch_max_abs_diff(cudaStream_t s, int blocks, const double *a, const double *b, long n, double *out);
+int launch_axpby(cudaStream_t s, double alpha, const double *x, double beta, double *y, long n);
+
+}  // namespace xca

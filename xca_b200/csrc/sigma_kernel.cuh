@@ -27,6 +27,7 @@ constexpr int MAXV = 2 * MAXM;      // vertices
 constexpr int MAXE = 2 * MAXM;      // largest K(0) exponent of a prefactor, plus one
 constexpr int NSLAB = 3;            // per-item slabs: T, X, Y
 constexpr int WARPS_MAX = 8;
+constexpr int PANEL_BMAX = 128;    // items per panel batch at most
 
 struct DevBasis {
   int r, p, n, nb, nq;
@@ -73,6 +74,17 @@ struct WorkUnit {
   int count;
 };
 
+// Where a Sigma launch puts its result.  Fast mode (slots == nullptr): every batch adds scale * (its sum)
+// into Sigma with atomics, so the order in which items reach Sigma varies from run to run.  Ordered
+// mode: work unit u keeps the running sum of its items, in pole-tuple order, in slots + slot_off[u]
+// (r d_out d_0 doubles); a reduction kernel then sums the units in a fixed order into Sigma.
+struct SigmaOut {
+  double *Sigma;
+  double scale;
+  double *slots;
+  const long *slot_off;
+};
+
 // Per-item state of a batch, kept in shared memory.
 struct ItemState {
   double scale;          // prefactor * prefactor sign * order / direction sign
@@ -81,6 +93,28 @@ struct ItemState {
   long taboff;           // per-step: edge-table offset of this item
   int keep;              // 1e-16 guard outcome
 };
+
+// Device state of the Dyson solve, trace and normalisation kernels (dyson_kernel.cuh).
+struct DysonBasis {
+  int r, nb;
+  double beta;
+  const double *LUp, *Wp, *BKp;  // RP x RP column-major (as DevBasis)
+  const int *perm;
+  const double *tabs, *k0, *k1;  // r: absolute t_i, K(0, om_l), K(1, om_l)
+  const double *rf;              // r: DLR frequencies om_l
+  const long *goff;              // nb: block offsets in a packed slab
+  const int *dims;               // nb
+  const long *woff;              // nb: per-block work offsets (6 r d^2 doubles each)
+  const long *moff;              // nb: per-block system matrix offsets ((r d)^2 doubles each)
+  const double *g0, *g0c, *g0t;  // packed slabs: G0 values, K^-1 G0, W K^-1 G0
+  double *work;
+  double *mats;
+};
+
+// D = A B + C on one 8 x 8 x 4 tile (a: A[g][q], b: B[q][g], c/d: C[g][2q], C[g][2q + 1], g = lane / 4, q = lane % 4).
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};" : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
 
 // Arithmetic of the plain FP64 path: the fused multiply-adds and the separately rounded products and
 // sums of the CPU restatement, at the same places and in the same order.

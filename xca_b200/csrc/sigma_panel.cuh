@@ -23,7 +23,6 @@ namespace xca {
 
 constexpr int PANEL_THREADS = 512;
 constexpr int PANEL_WARPS = PANEL_THREADS / 32;
-constexpr int PANEL_BMAX = 128;  // items per batch at most
 
 // NC usable panel columns; rows are stored with stride LDP = NC + 8 and the DLR matrices' columns with
 // stride RP + 8 (both 8 mod 16 doubles), so that the four k rows of an MMA fragment fall on distinct
@@ -95,10 +94,6 @@ __device__ __forceinline__ void stage_basis(const DevBasis &B, double *sLU, doub
   __syncthreads();
 }
 
-// D = A B + C on one 8 x 8 x 4 tile (a: A[g][q], b: B[q][g], c/d: C[g][2q], C[g][2q + 1], g = lane / 4, q = lane % 4).
-__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
-  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};" : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
-}
 
 // Y[i][c] = sum_{k < r} M[i][k] X1[k][c] (DUAL: Y[i][c] = fma(t_i, (M X2)[i][c], (M X1)[i][c])) for i < r,
 // c < nc.  M is column-major with stride RP + 8 (zero beyond column r); X rows k >= r are masked to zero.
@@ -605,7 +600,7 @@ template <int RP>
 __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis B, const ClassRec *__restrict__ classes,
                                                                         const WorkUnit *__restrict__ units, int n_units,
                                                                         int *__restrict__ unit_counter, const double *__restrict__ G,
-                                                                        double *__restrict__ Sigma, double scale) {
+                                                                        SigmaOut out) {
   constexpr int NC = PanelCfg<RP>::LDP, NT = PANEL_THREADS;  // NC: panel row stride
   extern __shared__ __align__(16) double smem[];
   double *sLU, *sW, *sBK, *PA;
@@ -812,17 +807,30 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
         }
       }
       __syncthreads();
-      double *dst = Sigma + B.goff[C.b_out];
-      for (int idx = tid; idx < r * dco; idx += NT) {
-        const int t = idx / dco, ee = idx - t * dco;
-        double a = 0.0;
-        bool keep_any = false;
-        for (int j = 0; j < nbi; ++j)
-          if (__longlong_as_double((long long)s_max[j]) > 1e-16) {
-            a = add(a, mul(T[t * NC + j * dco + ee], ist[j].scale));
-            keep_any = true;
-          }
-        if (keep_any) atomicAdd(dst + idx, mul(scale, a));
+      if (out.slots) {
+        // ordered mode: the unit's running sum continues over its batches (a thread keeps the same
+        // entries from batch to batch, so it reads back only what it wrote)
+        double *dst = out.slots + out.slot_off[u];
+        for (int idx = tid; idx < r * dco; idx += NT) {
+          const int t = idx / dco, ee = idx - t * dco;
+          double a = first == 0 ? 0.0 : dst[idx];
+          for (int j = 0; j < nbi; ++j)
+            if (__longlong_as_double((long long)s_max[j]) > 1e-16) a = add(a, mul(T[t * NC + j * dco + ee], ist[j].scale));
+          dst[idx] = a;
+        }
+      } else {
+        double *dst = out.Sigma + B.goff[C.b_out];
+        for (int idx = tid; idx < r * dco; idx += NT) {
+          const int t = idx / dco, ee = idx - t * dco;
+          double a = 0.0;
+          bool keep_any = false;
+          for (int j = 0; j < nbi; ++j)
+            if (__longlong_as_double((long long)s_max[j]) > 1e-16) {
+              a = add(a, mul(T[t * NC + j * dco + ee], ist[j].scale));
+              keep_any = true;
+            }
+          if (keep_any) atomicAdd(dst + idx, mul(out.scale, a));
+        }
       }
       __syncthreads();
     }

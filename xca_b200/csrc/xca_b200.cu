@@ -21,10 +21,7 @@
 
 #include "../../include/xca_b200.h"
 #include "dlr_host.hpp"
-#include "sigma_kernel.cuh"
-#include "sigma_panel.cuh"
-#include "dyson_kernel.cuh"
-#include "spgf_kernel.cuh"
+#include "launch.hpp"
 
 namespace xca {
 
@@ -161,6 +158,26 @@ struct Topology {
   int t[MAXM][2];
 };
 
+// Fixed summation order of the ordered mode.  Work unit u writes the running sum of its items (pole tuples
+// ascending) to slot_off[u]; groups are runs of consecutive units, listed block by block; block b's sum
+// is S_b = (((0 + g_0) + g_1) + ...) over its groups in list order, each group's value
+// (((0 + u_0) + u_1) + ...) over its units.  For a whole topology a group is one path class (its units
+// are runs of XCA_ORDERED_UNIT_TUPLES pole tuples) and the groups of a block follow the class order
+// (directions, orbital tuple, symmetry set); for a list of flat indices every (flat index, class) item is
+// its own unit and group, in list order.
+struct OrderedPlan {
+  std::vector<WorkUnit> units;
+  std::vector<long> slot_off;
+  long slot_doubles = 0;
+  std::vector<int2> groups;
+  std::vector<int> blk_group0;  // nb + 1
+  int max_block_elems = 0;
+  DevBuf<WorkUnit> d_units;
+  DevBuf<long> d_slot_off;
+  DevBuf<int2> d_groups;
+  DevBuf<int> d_blk_group0;
+};
+
 struct ClassSet {
   std::vector<ClassRec> classes;
   std::vector<WorkUnit> units;
@@ -170,6 +187,7 @@ struct ClassSet {
   std::vector<std::vector<int>> by_fbo;
   long long n_items = 0;
   std::map<std::pair<int, int>, std::unique_ptr<ClassSet>> shards;
+  std::unique_ptr<OrderedPlan> ordered;
 };
 
 struct CorrSet {
@@ -186,6 +204,7 @@ struct CorrSet {
 
 struct Ctx {
   int device = 0;
+  int nsm = 148;  // streaming multiprocessors of the device
   cudaStream_t stream = nullptr;
   long launches = 0;
   bool ready = false;
@@ -225,6 +244,8 @@ struct Ctx {
   DevBuf<long> d_mu_off, d_ka_off;
   std::map<std::string, std::unique_ptr<ClassSet>> noalloc_classes;  // host-only work lists of the allocation-free call
   int unit_batches = 4;  // panel batches per work unit
+  int precision = XCA_PREC_FP64;
+  DevBuf<double> d_slots;  // ordered mode: per-unit partial sums
   std::map<int, std::pair<int, std::unique_ptr<DevBuf<int2>>>> chunk_bufs;  // edge-table panel chunks per signature count
   // profiling: CUDA events around every Sigma launch (enabled on request), user events, L2 flush buffer
   bool profile = false;
@@ -236,7 +257,7 @@ struct Ctx {
   std::vector<double> k1;                 // K(1, om_l)
   std::vector<long> woff, moff;           // per-block work and system-matrix offsets
   long n_conv_rows = 0;                   // largest r d_b^2 (rows of the convolution-matrix kernel grid)
-  DevBuf<double> d_k1, d_rf, d_g0, d_g0c, d_g0t, d_dwork, d_mats, d_rhs, d_red;
+  DevBuf<double> d_k1, d_rf, d_g0, d_g0c, d_g0t, d_dwork, d_mats, d_rhs, d_red, d_efac;
   DevBuf<long> d_woff, d_moff;
   DevBuf<int> d_status;
 
@@ -352,11 +373,7 @@ static long ipow(long a, int e) {
 // symmetry set and the zero-block flags of G, never on the pole tuple, so it is enumerated once per
 // (topology, zero pattern) and every valid path class stands for p^(m-1) items.
 
-static int panel_nc_host(int RP) { return RP == 32 ? panel_nc<32>() : (RP == 48 ? panel_nc<48>() : panel_nc<64>()); }
-
-static size_t panel_smem_bytes(int RP) {
-  return (RP == 32 ? panel_smem_doubles<32>() : (RP == 48 ? panel_smem_doubles<48>() : panel_smem_doubles<64>())) * sizeof(double);
-}
+static int panel_nc_host(int RP) { return RP == 32 ? panel_width<32>() : (RP == 48 ? panel_width<48>() : panel_width<64>()); }
 
 // (block, first column) chunks of the edge-table panels for `nsig` signatures per block.
 static std::vector<int2> table_chunks(const Ctx *c, int nsig) {
@@ -498,23 +515,12 @@ static ClassSet *get_classes(Ctx *c, const Topology &T, const std::vector<int> &
   return ret;
 }
 
-template <int RP>
-static void launch_tables_rp(Ctx *c, const double *G_dev, int nsig, const int2 *d_chunks, int n_chunks, const DevBasis &B) {
-  const size_t smem = panel_smem_doubles<RP>() * sizeof(double);
-  CUDA_CHECK(cudaFuncSetAttribute(edge_tables_panel_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  const int grid = std::max(1, std::min(n_chunks, nsm));
-  edge_tables_panel_kernel<RP><<<grid, PANEL_THREADS, smem, c->stream>>>(B, G_dev, d_chunks, n_chunks);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
-}
-
 static void launch_tables(Ctx *c, const double *G_dev, int nsig, const int2 *d_chunks, int n_chunks, const DevBasis &B) {
+  (void)nsig;
   switch (c->RP) {
-    case 32: launch_tables_rp<32>(c, G_dev, nsig, d_chunks, n_chunks, B); break;
-    case 48: launch_tables_rp<48>(c, G_dev, nsig, d_chunks, n_chunks, B); break;
-    default: launch_tables_rp<64>(c, G_dev, nsig, d_chunks, n_chunks, B); break;
+    case 32: c->launches += launch_edge_tables<32>(c->stream, c->nsm, B, G_dev, d_chunks, n_chunks); break;
+    case 48: c->launches += launch_edge_tables<48>(c->stream, c->nsm, B, G_dev, d_chunks, n_chunks); break;
+    default: c->launches += launch_edge_tables<64>(c->stream, c->nsm, B, G_dev, d_chunks, n_chunks); break;
   }
 }
 
@@ -532,28 +538,22 @@ static int prepare_tables(Ctx *c, const double *G_dev, int m) {
   return nsig;
 }
 
-template <int RP>
-static void launch_sigma_rp(Ctx *c, const DevBasis &B, const ClassRec *d_classes, const WorkUnit *d_units, int n_units, int *counter,
-                            const double *G_dev, double *Sig_dev, double scale) {
-  const size_t smem = panel_smem_doubles<RP>() * sizeof(double);
-  CUDA_CHECK(cudaFuncSetAttribute(sigma_panel_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(int), c->stream));
-  int nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  const int grid = std::max(1, std::min(nsm, n_units));
-  sigma_panel_kernel<RP><<<grid, PANEL_THREADS, smem, c->stream>>>(B, d_classes, d_units, n_units, counter, G_dev,
-                                                                                 Sig_dev, scale);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
+static void launch_sigma_units(Ctx *c, const DevBasis &B, const ClassRec *d_classes, const WorkUnit *d_units, int n_units, int *counter,
+                               const double *G_dev, const SigmaOut &out) {
+  switch (c->RP) {
+    case 32: c->launches += launch_sigma_panel<32>(c->stream, c->nsm, B, d_classes, d_units, n_units, counter, G_dev, out); break;
+    case 48: c->launches += launch_sigma_panel<48>(c->stream, c->nsm, B, d_classes, d_units, n_units, counter, G_dev, out); break;
+    default: c->launches += launch_sigma_panel<64>(c->stream, c->nsm, B, d_classes, d_units, n_units, counter, G_dev, out); break;
+  }
 }
 
-static void launch_sigma_units(Ctx *c, const DevBasis &B, const ClassRec *d_classes, const WorkUnit *d_units, int n_units, int *counter,
-                               const double *G_dev, double *Sig_dev, double scale) {
-  switch (c->RP) {
-    case 32: launch_sigma_rp<32>(c, B, d_classes, d_units, n_units, counter, G_dev, Sig_dev, scale); break;
-    case 48: launch_sigma_rp<48>(c, B, d_classes, d_units, n_units, counter, G_dev, Sig_dev, scale); break;
-    default: launch_sigma_rp<64>(c, B, d_classes, d_units, n_units, counter, G_dev, Sig_dev, scale); break;
-  }
+static SigmaOut atomic_out(double *Sig_dev, double scale) {
+  SigmaOut o;
+  o.Sigma = Sig_dev;
+  o.scale = scale;
+  o.slots = nullptr;
+  o.slot_off = nullptr;
+  return o;
 }
 
 static std::vector<int> zero_flags_device(Ctx *c, const double *G_dev) {
@@ -569,6 +569,95 @@ static std::vector<int> zero_flags_device(Ctx *c, const double *G_dev) {
   return z;
 }
 
+// Ordered-mode plan of a unit list: slot offsets and per-block groups.  `group_of_unit[u]` numbers the
+// group of unit u; units of one group must be consecutive.
+static std::unique_ptr<OrderedPlan> make_plan(const Ctx *c, const std::vector<ClassRec> &classes, std::vector<WorkUnit> units,
+                                              const std::vector<int> &group_of_unit) {
+  auto P = std::make_unique<OrderedPlan>();
+  P->units = std::move(units);
+  const size_t nu = P->units.size();
+  P->slot_off.resize(nu);
+  long off = 0;
+  for (size_t u = 0; u < nu; ++u) {
+    const ClassRec &R = classes[P->units[u].cls];
+    P->slot_off[u] = off;
+    off += (long)c->r * R.bdims[2 * R.m] * R.bdims[0];
+  }
+  P->slot_doubles = off;
+  std::vector<std::vector<int2>> per_block(c->nb);
+  for (size_t u = 0; u < nu;) {
+    size_t v = u + 1;
+    while (v < nu && group_of_unit[v] == group_of_unit[u]) ++v;
+    per_block[classes[P->units[u].cls].b_out].push_back(make_int2((int)u, (int)v));
+    u = v;
+  }
+  P->blk_group0.assign(c->nb + 1, 0);
+  for (int b = 0; b < c->nb; ++b) {
+    P->blk_group0[b + 1] = P->blk_group0[b] + (int)per_block[b].size();
+    P->groups.insert(P->groups.end(), per_block[b].begin(), per_block[b].end());
+    P->max_block_elems = std::max(P->max_block_elems, c->r * c->dims[b] * c->dims[b]);
+  }
+  P->d_units.upload(P->units, c->stream);
+  P->d_slot_off.upload(P->slot_off, c->stream);
+  P->d_groups.upload(P->groups, c->stream);
+  P->d_blk_group0.upload(P->blk_group0, c->stream);
+  return P;
+}
+
+// Plan of a whole topology: per class (class order) runs of XCA_ORDERED_UNIT_TUPLES pole tuples.
+static OrderedPlan *ordered_plan(Ctx *c, ClassSet *cs) {
+  if (cs->ordered) return cs->ordered.get();
+  std::vector<WorkUnit> units;
+  std::vector<int> grp;
+  for (size_t k = 0; k < cs->classes.size(); ++k) {
+    const int npt = cs->classes[k].npt;
+    for (int s = 0; s < npt; s += XCA_ORDERED_UNIT_TUPLES) {
+      units.push_back(WorkUnit{(int)k, s, std::min(XCA_ORDERED_UNIT_TUPLES, npt - s)});
+      grp.push_back((int)k);
+    }
+  }
+  cs->ordered = make_plan(c, cs->classes, std::move(units), grp);
+  return cs->ordered.get();
+}
+
+// Sum of the unit slots in the plan's fixed order, Sigma_b += scale * S_b (ordered mode, second step).
+__global__ void sigma_ordered_reduce_kernel(const double *__restrict__ slots, const long *__restrict__ slot_off,
+                                            const int2 *__restrict__ groups, const int *__restrict__ blk_group0,
+                                            const long *__restrict__ goff, const int *__restrict__ dims, int r, double scale,
+                                            double *__restrict__ Sigma) {
+  const int b = blockIdx.y;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= r * dims[b] * dims[b]) return;
+  double S = 0.0;
+  for (int g = blk_group0[b]; g < blk_group0[b + 1]; ++g) {
+    const int2 gr = groups[g];
+    double cp = 0.0;
+    for (int u = gr.x; u < gr.y; ++u) cp = __dadd_rn(cp, slots[slot_off[u] + x]);
+    S = __dadd_rn(S, cp);
+  }
+  double *dst = Sigma + goff[b] + x;
+  *dst = __dadd_rn(*dst, __dmul_rn(scale, S));
+}
+
+static void launch_sigma_plan(Ctx *c, const std::vector<ClassRec> &classes, const ClassRec *d_classes, OrderedPlan *P,
+                              const double *G_dev, double *Sig_dev, double scale, int nsig) {
+  if (P->units.empty()) return;
+  (void)classes;
+  c->d_slots.resize(std::max<long>(P->slot_doubles, 1));
+  SigmaOut o;
+  o.Sigma = nullptr;
+  o.scale = 1.0;
+  o.slots = c->d_slots.ptr;
+  o.slot_off = P->d_slot_off.ptr;
+  c->d_counter.resize(1);
+  launch_sigma_units(c, c->basis(nsig), d_classes, P->d_units.ptr, (int)P->units.size(), c->d_counter.ptr, G_dev, o);
+  dim3 grid((unsigned)((P->max_block_elems + 127) / 128), (unsigned)c->nb);
+  sigma_ordered_reduce_kernel<<<grid, 128, 0, c->stream>>>(c->d_slots.ptr, P->d_slot_off.ptr, P->d_groups.ptr, P->d_blk_group0.ptr,
+                                                           c->d_goff.ptr, c->d_dims.ptr, c->r, scale, Sig_dev);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+}
+
 static void launch_sigma(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_dev, double scale, int nsig) {
   if (cs->units.empty()) return;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -577,9 +666,13 @@ static void launch_sigma(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_
     CUDA_CHECK(cudaEventCreate(&e1));
     CUDA_CHECK(cudaEventRecord(e0, c->stream));
   }
-  c->d_counter.resize(1);
-  launch_sigma_units(c, c->basis(nsig), cs->d_classes.ptr, cs->d_units.ptr, (int)cs->units.size(), c->d_counter.ptr, G_dev, Sig_dev,
-                     scale);
+  if (c->precision == XCA_PREC_FP64_ORDERED) {
+    launch_sigma_plan(c, cs->classes, cs->d_classes.ptr, ordered_plan(c, cs), G_dev, Sig_dev, scale, nsig);
+  } else {
+    c->d_counter.resize(1);
+    launch_sigma_units(c, c->basis(nsig), cs->d_classes.ptr, cs->d_units.ptr, (int)cs->units.size(), c->d_counter.ptr, G_dev,
+                       atomic_out(Sig_dev, scale));
+  }
   if (c->profile) {
     CUDA_CHECK(cudaEventRecord(e1, c->stream));
     c->prof_events.emplace_back(e0, e1);
@@ -769,16 +862,11 @@ static CorrSet *get_corr(Ctx *c, const Topology &T, const std::vector<int> &zero
   return ret;
 }
 
-template <int RP>
-static void launch_corr_rp(Ctx *c, CorrSet *cs, const WorkUnit *d_units, int n_units, const double *G_dev, double *g_dev,
-                           double scale, int nsig) {
+static void launch_corr(Ctx *c, CorrSet *cs, const WorkUnit *d_units, int n_units, const double *G_dev, double *g_dev, double scale,
+                        int nsig) {
   if (n_units == 0) return;
-  const size_t sm = (4 * (size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
-  CUDA_CHECK(cudaFuncSetAttribute(correlator_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  int nsm = 0;
-  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   const int warps_per_cta = 4;
-  const int grid = std::max(1, std::min(2 * nsm, (n_units + warps_per_cta - 1) / warps_per_cta));
+  const int grid = std::max(1, std::min(2 * c->nsm, (n_units + warps_per_cta - 1) / warps_per_cta));
   const long slab = (long)c->r * c->nmax * c->nmax;
   const long warp_doubles = (3 + 2L * c->nb) * slab + (long)c->r * c->n * c->n;
   c->d_corr_scratch.resize((size_t)grid * warps_per_cta * warp_doubles);
@@ -788,19 +876,18 @@ static void launch_corr_rp(Ctx *c, CorrSet *cs, const WorkUnit *d_units, int n_u
   CB.RFp = c->d_RFp.ptr;
   CB.mu_off = c->d_mu_off.ptr;
   CB.ka_off = c->d_ka_off.ptr;
-  correlator_kernel<RP><<<grid, 32 * warps_per_cta, sm, c->stream>>>(c->basis(nsig), CB, cs->d_classes.ptr, cs->d_chains.ptr,
-                                                                     cs->d_terms.ptr, d_units, n_units, c->d_counter.ptr, G_dev,
-                                                                     g_dev, scale, c->nmax, c->d_corr_scratch.ptr, warp_doubles);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
-}
-
-static void launch_corr(Ctx *c, CorrSet *cs, const WorkUnit *d_units, int n_units, const double *G_dev, double *g_dev, double scale,
-                        int nsig) {
+  const DevBasis B = c->basis(nsig);
   switch (c->RP) {
-    case 32: launch_corr_rp<32>(c, cs, d_units, n_units, G_dev, g_dev, scale, nsig); break;
-    case 48: launch_corr_rp<48>(c, cs, d_units, n_units, G_dev, g_dev, scale, nsig); break;
-    default: launch_corr_rp<64>(c, cs, d_units, n_units, G_dev, g_dev, scale, nsig); break;
+#define XCA_CORR(RPV)                                                                                                          \
+  case RPV:                                                                                                                    \
+    c->launches += launch_correlator<RPV>(c->stream, grid, warps_per_cta, B, CB, cs->d_classes.ptr, cs->d_chains.ptr, cs->d_terms.ptr, \
+                                          d_units, n_units, c->d_counter.ptr, G_dev, g_dev, scale, c->nmax, c->d_corr_scratch.ptr,  \
+                                          warp_doubles);                                                                       \
+    break;
+    XCA_CORR(32)
+    XCA_CORR(48)
+    XCA_CORR(64)
+#undef XCA_CORR
   }
 }
 
@@ -825,29 +912,13 @@ static void require_dyson(const Ctx *c) {
   if (!c->dyson_ready) throw Error(XCA_ERR_INVALID, "Dyson solver not set up (xca_dyson_setup)");
 }
 
-template <int RP>
-static void launch_dyson_rp(Ctx *c, const double *Sig_dev, double eta, int hermitize, double *G_dev) {
-  DysonBasis B = dyson_basis(c);
-  size_t sm = (2 * (size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
-  CUDA_CHECK(cudaFuncSetAttribute(dyson_coef_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  dyson_coef_kernel<RP><<<c->nb, 256, sm, c->stream>>>(B, Sig_dev, eta);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
-  dim3 grid((unsigned)((c->n_conv_rows + 63) / 64), (unsigned)c->nb);
-  dyson_convmat_kernel<RP><<<grid, 64, 0, c->stream>>>(B);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
-  dyson_lu_solve_kernel<<<c->nb, 1024, 0, c->stream>>>(B, c->d_rhs.ptr, G_dev, hermitize, c->d_status.ptr);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
-}
-
 static void launch_dyson(Ctx *c, const double *Sig_dev, double eta, int hermitize, double *G_dev) {
   CUDA_CHECK(cudaMemsetAsync(c->d_status.ptr, 0, sizeof(int), c->stream));
+  const DysonBasis B = dyson_basis(c);
   switch (c->RP) {
-    case 32: launch_dyson_rp<32>(c, Sig_dev, eta, hermitize, G_dev); break;
-    case 48: launch_dyson_rp<48>(c, Sig_dev, eta, hermitize, G_dev); break;
-    default: launch_dyson_rp<64>(c, Sig_dev, eta, hermitize, G_dev); break;
+    case 32: c->launches += launch_dyson<32>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr); break;
+    case 48: c->launches += launch_dyson<48>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr); break;
+    default: c->launches += launch_dyson<64>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr); break;
   }
 }
 
@@ -863,30 +934,22 @@ static void check_dyson_status(Ctx *c) {
   }
 }
 
-template <int RP>
-static double trace_beta_rp(Ctx *c, const double *G_dev) {
-  DysonBasis B = dyson_basis(c);
-  size_t sm = ((size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
-  CUDA_CHECK(cudaFuncSetAttribute(trace_beta_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+// sum_b Tr G_b(beta) (trace, block_sparse.cpp:852-861): per-block partial traces on the device, summed on
+// the host in block order.
+static double trace_beta(Ctx *c, const double *G_dev) {
+  const DysonBasis B = dyson_basis(c);
   c->d_red.resize(std::max(c->nb, 256));
-  trace_beta_kernel<RP><<<c->nb, 128, sm, c->stream>>>(B, G_dev, c->d_red.ptr);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
+  switch (c->RP) {
+    case 32: c->launches += launch_trace_beta<32>(c->stream, B, G_dev, c->d_red.ptr); break;
+    case 48: c->launches += launch_trace_beta<48>(c->stream, B, G_dev, c->d_red.ptr); break;
+    default: c->launches += launch_trace_beta<64>(c->stream, B, G_dev, c->d_red.ptr); break;
+  }
   std::vector<double> part(c->nb);
   CUDA_CHECK(cudaMemcpyAsync(part.data(), c->d_red.ptr, c->nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CUDA_CHECK(cudaStreamSynchronize(c->stream));
   double s = 0;
   for (double x : part) s += x;
   return s;
-}
-
-// sum_b Tr G_b(beta) (trace, block_sparse.cpp:852-861)
-static double trace_beta(Ctx *c, const double *G_dev) {
-  switch (c->RP) {
-    case 32: return trace_beta_rp<32>(c, G_dev);
-    case 48: return trace_beta_rp<48>(c, G_dev);
-    default: return trace_beta_rp<64>(c, G_dev);
-  }
 }
 
 // -------------------------------------------------------------------------------- allocation-free Sigma
@@ -977,6 +1040,7 @@ int xca_ctx_create(int device, xca_ctx **out) {
     throw Error(XCA_ERR_CUDA, std::string("no CUDA device available: ") + cudaGetErrorString(e));
   }
   set_device(c);
+  CUDA_CHECK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
   CUDA_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   *out = reinterpret_cast<xca_ctx *>(c);
   API_END
@@ -1202,6 +1266,8 @@ int xca_compute_self_energy_device_shard(xca_ctx *ctx, const double *G_dev, int 
   auto *c = reinterpret_cast<Ctx *>(ctx);
   if (!c->ready) throw Error(XCA_ERR_INVALID, "evaluator not set up");
   if (n_shards < 1 || shard < 0 || shard >= n_shards) throw Error(XCA_ERR_INVALID, "shard out of range");
+  if (n_shards > 1 && c->precision == XCA_PREC_FP64_ORDERED)
+    throw Error(XCA_ERR_UNSUPPORTED, "the ordered summation mode evaluates whole topologies on one device (n_shards must be 1)");
   set_device(c);
   Topology T = parse_topology(m, topology);
   auto zero = zero_flags_device(c, G_dev);
@@ -1341,10 +1407,13 @@ int xca_normalize_device(xca_ctx *ctx, double *G_dev, double *Z, double *deta) {
   check_dyson_status(c);
   const double z = -trace_beta(c, G_dev);
   const double de = std::log(std::fabs(z)) / c->beta;
-  dim3 grid(64, (unsigned)c->nb);
-  energy_shift_kernel<<<grid, 256, 0, c->stream>>>(dyson_basis(c), G_dev, de);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
+  // exp(-tau_t deta) per node on the host (libm, as the normalisation step's own arithmetic), then scaled
+  std::vector<double> fac(c->r);
+  for (int t = 0; t < c->r; ++t) fac[t] = std::exp(-((c->beta * c->tabs[t]) * de));
+  c->d_efac.resize(c->r);
+  CUDA_CHECK(cudaMemcpyAsync(c->d_efac.ptr, fac.data(), c->r * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  c->launches += launch_energy_shift(c->stream, dyson_basis(c), G_dev, c->d_efac.ptr);
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
   *Z = z;
   *deta = de;
   API_END
@@ -1357,9 +1426,7 @@ int xca_max_abs_diff_device(xca_ctx *ctx, const double *a_dev, const double *b_d
   set_device(c);
   const int blocks = 256;
   c->d_red.resize(std::max(c->nb, blocks));
-  max_abs_diff_kernel<<<blocks, 256, 0, c->stream>>>(a_dev, b_dev, c->slab, c->d_red.ptr);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
+  c->launches += launch_max_abs_diff(c->stream, blocks, a_dev, b_dev, c->slab, c->d_red.ptr);
   std::vector<double> part(blocks);
   CUDA_CHECK(cudaMemcpyAsync(part.data(), c->d_red.ptr, blocks * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CUDA_CHECK(cudaStreamSynchronize(c->stream));
@@ -1375,9 +1442,7 @@ int xca_axpby_device(xca_ctx *ctx, double alpha, const double *x_dev, double bet
   require_basis(c);
   set_device(c);
   const long n = c->slab;
-  axpby_kernel<<<(int)std::max<long>(1, std::min<long>(1184, (n + 255) / 256)), 256, 0, c->stream>>>(alpha, x_dev, beta, y_dev, n);
-  c->launches++;
-  CUDA_CHECK(cudaGetLastError());
+  c->launches += launch_axpby(c->stream, alpha, x_dev, beta, y_dev, n);
   API_END
 }
 
@@ -1479,7 +1544,14 @@ int xca_compute_self_energy(xca_ctx *ctx, const double *G, int m, const int *top
       long pix = q % npt, fb = q / npt;
       for (int k : cs->by_fbo[fb * omax + o]) units.push_back(WorkUnit{k, (int)pix, 1});
     }
-    if (!units.empty()) {
+    if (!units.empty() && c->precision == XCA_PREC_FP64_ORDERED) {
+      // every (flat index, class) item its own group, in list order: the sequential order of the list
+      std::vector<int> grp(units.size());
+      for (size_t u = 0; u < units.size(); ++u) grp[u] = (int)u;
+      auto P = make_plan(c, cs->classes, units, grp);
+      launch_sigma_plan(c, cs->classes, cs->d_classes.ptr, P.get(), c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
+      CUDA_CHECK(cudaStreamSynchronize(c->stream));
+    } else if (!units.empty()) {
       ClassSet tmp;
       tmp.classes = cs->classes;
       tmp.units = units;
@@ -1764,6 +1836,21 @@ int xca_synchronize(xca_ctx *ctx) {
   API_END
 }
 
+int xca_set_precision_mode(xca_ctx *ctx, int mode) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  if (mode != XCA_PREC_FP64 && mode != XCA_PREC_FP64_ORDERED)
+    throw Error(XCA_ERR_UNSUPPORTED, "precision mode " + std::to_string(mode) + " is not available");
+  c->precision = mode;
+  API_END
+}
+
+int xca_get_precision_mode(xca_ctx *ctx, int *mode) {
+  API_BEGIN
+  *mode = reinterpret_cast<Ctx *>(ctx)->precision;
+  API_END
+}
+
 int xca_kernel_launches(xca_ctx *ctx, long *out) {
   API_BEGIN
   *out = reinterpret_cast<Ctx *>(ctx)->launches;
@@ -1831,7 +1918,7 @@ int xca_compute_self_energy_device_noalloc(xca_ctx *ctx, const double *G_dev, in
   B.tab_off = d_tab_off;
   launch_tables(c, G_dev, nsig, d_chunks, (int)chunks.size(), B);
   if (!cs->units.empty())
-    launch_sigma_units(c, B, d_classes, d_units, (int)cs->units.size(), counter, G_dev, Sigma_dev, scale);
+    launch_sigma_units(c, B, d_classes, d_units, (int)cs->units.size(), counter, G_dev, atomic_out(Sigma_dev, scale));
   API_END
 }
 
