@@ -165,6 +165,30 @@ int xca_compute_single_ptcle_gf(xca_ctx *ctx, const double *G, int m, const int 
 int xca_compute_single_ptcle_gf_device(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
                                        double *g_dev);
 
+/* DiagramEvaluator::compute_one_time_correlator(G, ops_tau, ops_0, ad, topology, f_ix_vec)
+ * (c++/triqs_xca/block_sparse_backbone.cpp:843-866; Python eval_one_time_correlator,
+ * python/triqs_xca/block_sparse_solver.py:701-741): the correlator C(tau)[mu][ka] of one topology,
+ * eval_correlator (block_sparse_backbone.cpp:528-706) with the n_tau operators O_mu at tau and the n_0
+ * operators O'_ka at 0 in place of F_mu and F^dag_ka.  Each operator is given in block form, as
+ * setup_ops_from_triqs_2nd_quant_ops builds it (block_sparse_backbone.cpp:810-840): tau_index[mu * n_blocks
+ * + b] is the block O_mu maps block b to (-1: none) and tau_data packs, in (mu, b) order over present
+ * columns, the (d_target x d_b) complex block in the eigenbasis; zero_index / zero_data likewise.
+ * f_ix == NULL evaluates every flat index; corr_out is r x n_tau x n_0 complex. */
+int xca_compute_one_time_correlator(xca_ctx *ctx, const double *G, int n_tau, const int *tau_index, const double *tau_data, int n_0,
+                                    const int *zero_index, const double *zero_data, int m, const int *topology, const long *f_ix,
+                                    long n_fix, double *corr_out);
+
+/* convolve_ppsc(G1, G2) (c++/triqs_xca/block_sparse.cpp:832-850): per block the time-ordered DLR
+ * convolution (G1_b * G2_b)(tau) on the nodes.  Host packed complex slabs, or device real slabs. */
+int xca_convolve_ppsc(xca_ctx *ctx, const double *G1, const double *G2, double *H_out);
+int xca_convolve_ppsc_device(xca_ctx *ctx, const double *G1_dev, const double *G2_dev, double *H_dev);
+
+/* expectation_value(op, ad, G) (c++/triqs_xca/block_sparse.cpp:797-818): -sum_b Tr[O_b G_b(beta)] for a
+ * block-diagonal operator in the eigenbasis (ad.get_op_mat then U O U^dag): op_index[b] is b or -1 (no
+ * block; any other value gives XCA_ERR_INVALID, the reference asserts connection[b] == b) and op_data packs
+ * the (d_b x d_b) complex blocks of the present ones in block order.  out = (re, im). */
+int xca_expectation_value(xca_ctx *ctx, const double *G, const int *op_index, const double *op_data, double *out);
+
 /* Zero n_doubles of device memory on the context's stream. */
 int xca_zero_device(xca_ctx *ctx, double *dev, long n_doubles);
 

@@ -60,6 +60,8 @@ def lib():
         L.ora_items.argtypes = [P, dp, I, ip, LG, LG, lp, LG]
         L.ora_spgf.argtypes = [P, dp, I, ip, lp, LG, I, dp]
         L.ora_hyb_values.argtypes = [P, dp, dp]
+        L.ora_correlator.argtypes = [P, dp, I, ip, lp, LG, I, I, ip, dp, I, ip, dp, dp]
+        L.ora_expectation.argtypes = [P, I, ip, dp, ip, dp, dp]
         _LIB = L
     return _LIB
 
@@ -288,6 +290,30 @@ class Evaluator:
         _check(lib().ora_spgf(self._h, _dp(g), t.shape[0], _ip(t), fix_p, nfix, int(nthreads), _dp(out)))
         return out
 
+    def compute_one_time_correlator(self, G, ops_tau, ops_0, topology, f_ix=None, nthreads=0):
+        """``compute_one_time_correlator`` (``c++/triqs_xca/block_sparse_backbone.cpp:843-866``) with block operators
+        ``(index[nb], blocks[nb])`` (blocks[b] of shape (d_index[b], d_b), None where index[b] == -1)."""
+        t = np.ascontiguousarray(topology, dtype=np.int32)
+        g = self.pack(G)
+
+        def packed(ops):
+            idx = np.ascontiguousarray(np.concatenate([np.asarray(i, np.int32) for i, _ in ops]), dtype=np.int32)
+            parts = [_c(blk).ravel() for i, blks in ops for b, blk in zip(i, blks) if b >= 0]
+            data = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(1, np.complex128))
+            return idx, data
+
+        mi, md = packed(ops_tau)
+        ki, kd = packed(ops_0)
+        out = np.zeros((self.r, len(ops_tau), len(ops_0)), np.complex128)
+        if f_ix is None:
+            fix_p, nfix = None, 0
+        else:
+            fix = np.ascontiguousarray(np.atleast_1d(f_ix), dtype=np.int64)
+            fix_p, nfix = _lp(fix), len(fix)
+        _check(lib().ora_correlator(self._h, _dp(g), t.shape[0], _ip(t), fix_p, nfix, int(nthreads), len(ops_tau), _ip(mi), _dp(md),
+                                    len(ops_0), _ip(ki), _dp(kd), _dp(out)))
+        return out
+
     def hyb_values(self):
         v = np.zeros((self.r, self.n, self.n), np.complex128)
         vr = np.zeros_like(v)
@@ -362,6 +388,24 @@ def trace_beta(dlr, G):
     return tot
 
 
+def convolve_ppsc(dlr, beta, G1, G2):
+    """``convolve_ppsc`` (``c++/triqs_xca/block_sparse.cpp:832-850``): per block the time-ordered convolution."""
+    return [dlr.convolve(beta, dlr.vals2coefs(a), dlr.vals2coefs(b), time_order=True) for a, b in zip(G1, G2)]
+
+
+def expectation_value(dlr, G, op_index, op_blocks):
+    """``expectation_value`` (``c++/triqs_xca/block_sparse.cpp:797-818``) of a block-diagonal operator given as
+    (op_index[nb], op_blocks[nb]) in the Fock basis."""
+    dims = np.ascontiguousarray([g.shape[1] for g in G], dtype=np.int32)
+    idx = np.ascontiguousarray(op_index, dtype=np.int32)
+    parts = [_c(o).ravel() for i, o in zip(idx, op_blocks) if i >= 0]
+    data = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(1, np.complex128))
+    g = np.ascontiguousarray(np.concatenate([_c(x).ravel() for x in G]))
+    out = np.zeros(2)
+    _check(lib().ora_expectation(dlr._h, len(G), _ip(dims), _dp(g), _ip(idx), _dp(data), _dp(out)))
+    return complex(out[0], out[1])
+
+
 def solve_dyson(dlr, beta, G0, Sig, eta):
     """``solve_dyson`` (``block_sparse_solver.py:572-590``): per-block Dyson solve, then hermitize."""
     out = []
@@ -380,9 +424,44 @@ def normalize(dlr, beta, G, eta):
     return [g * fac[:, None, None] for g in G], eta + deta
 
 
+def z_alpha_minus_one_and_derivatives(dlr, beta, G0, Sig, alpha, eta):
+    """``Z_alpha_minus_one_and_derivative_and_2nd_derivative`` (``block_sparse_solver.py:800-816``)."""
+    Ga = solve_dyson(dlr, beta, G0, Sig if alpha == 1.0 else [alpha * s for s in Sig], eta)
+    Za = -trace_beta(dlr, Ga).real
+    G2 = convolve_ppsc(dlr, beta, Ga, Ga)
+    dZ = -trace_beta(dlr, G2).real
+    d2Z = -2 * trace_beta(dlr, convolve_ppsc(dlr, beta, G2, Ga)).real
+    return Za - 1, dZ, d2Z
+
+
+def deta_dalpha(dlr, beta, G0, Sig, alpha, eta):
+    """``deta_dalpha`` (``block_sparse_solver.py:819-838``): -Tr[G_a * Sigma * G_a] / Tr[G_a * G_a]."""
+    Ga = solve_dyson(dlr, beta, G0, Sig if alpha == 1.0 else [alpha * s for s in Sig], eta)
+    tr_gg = -trace_beta(dlr, convolve_ppsc(dlr, beta, Ga, Ga))
+    tr_gsg = -trace_beta(dlr, convolve_ppsc(dlr, beta, Ga, convolve_ppsc(dlr, beta, Sig, Ga)))
+    return -tr_gsg / tr_gg
+
+
+def chempot_newton(dlr, beta, G0, Sig, eta, **kwargs):
+    """``solve_ppsc_chempot_newton`` (``block_sparse_solver.py:1000-1029``): Halley's method on Z(eta) - 1."""
+    from scipy.optimize import root_scalar
+    sol = root_scalar(lambda e: z_alpha_minus_one_and_derivatives(dlr, beta, G0, Sig, 1.0, e), x0=eta, fprime=True, fprime2=True,
+                      method="halley", **kwargs)
+    return float(sol.root)
+
+
+def chempot_adiabatic_ode(dlr, beta, G0, Sig, tol, method="RK23"):
+    """``solve_ppsc_chempot_adiabatic_ode`` (``block_sparse_solver.py:896-923``)."""
+    from scipy.integrate import solve_ivp
+    sol = solve_ivp(lambda t, y: deta_dalpha(dlr, beta, G0, Sig, t, y[0]).real, (0.0, 1.0), np.array([0.0]), atol=tol, method=method,
+                    dense_output=True)
+    return float(sol.y[0, -1])
+
+
 def solve(dlr, ev, beta, G0, max_order, tol, maxiter, mix=1.0, spgf_max_order=None, nthreads=0, verbose=False, ordered=False,
-          G_init=None, eta_init=0.0):
-    """``BlockSparseSolver.solve`` with 'classic' normalization (``block_sparse_solver.py:240-355``).
+          G_init=None, eta_init=0.0, normalization="classic", eps=None):
+    """``BlockSparseSolver.solve`` (``block_sparse_solver.py:240-355``) with the 'classic', 'root', 'ode+classic'
+    or 'ode+root' normalization (``eps`` = the DLR accuracy, which sets the root / ODE tolerances).
     ``ordered``: Sigma summed in the fixed order of the device's ordered mode.  ``G_init``/``eta_init``:
     start from a previous solution (the reference's solver keeps self.G and self.eta between solves).
 
@@ -394,8 +473,13 @@ def solve(dlr, ev, beta, G0, max_order, tol, maxiter, mix=1.0, spgf_max_order=No
     Sig = None
     for it in range(1, maxiter + 1):
         Sig = sigma_total(ev, G, max_order, nthreads=nthreads, ordered=ordered)
+        if normalization in ("ode+classic", "ode+root"):
+            eta = chempot_adiabatic_ode(dlr, beta, G0, Sig, tol=100 * eps)
+        if normalization in ("root", "ode+root"):
+            eta = chempot_newton(dlr, beta, G0, Sig, eta, xtol=10 * eps)
         Gn = solve_dyson(dlr, beta, G0, Sig, eta)
-        Gn, eta = normalize(dlr, beta, Gn, eta)
+        if normalization in ("classic", "ode+classic"):
+            Gn, eta = normalize(dlr, beta, Gn, eta)
         diff = max(np.max(np.abs(a - b)) for a, b in zip(Gn, G))
         if verbose:
             print(f"iter = {it}, diff_G = {diff:2.2E}, eta = {eta:2.2E}")

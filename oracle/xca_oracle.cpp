@@ -1207,6 +1207,99 @@ int ora_spgf(void *ev, const double *G_, int m, const int *topo, const long *fix
   } catch (std::exception &e) { g_err = e.what(); return 1; }
 }
 
+// compute_one_time_correlator(G, ops_tau, ops_0, ad, topology, f_ix_vec) bsb.cpp:843-866: eval_correlator with
+// the given block operators (setup_ops_from_triqs_2nd_quant_ops, :810-840) in place of F_mu and F^dag_ka.
+// mu_index[mu * nb + b] (-1: none) and mu_data packing the (d_target x d_b) blocks in (mu, b) order; likewise
+// ka.  out is (r, nmu, nka) complex.
+int ora_correlator(void *ev, const double *G_, int m, const int *topo, const long *fix, long nfix, int nthreads, int nmu,
+                   const int *mu_index, const double *mu_data, int nka, const int *ka_index, const double *ka_data, double *out) {
+  try {
+    auto *E = (Evaluator *)ev;
+    Backbone B0(m, topo, E->n, E->p, true);
+    long nmax = B0.num_backbones();
+    long count = fix ? nfix : nmax;
+    for (long z = 0; fix && z < nfix; ++z)
+      if (fix[z] < 0 || fix[z] >= nmax) throw std::runtime_error("DiagramEvaluator::compute_one_time_correlator: f_ix out of range");
+    BlockG g = make_G(*E, (const cd *)G_);
+    auto build = [&](int nops, const int *index, const double *data, std::vector<BlockOp> &ops) {
+      const cd *dp = (const cd *)data;
+      ops.resize(nops);
+      for (int o = 0; o < nops; ++o) {
+        ops[o].index.assign(index + (size_t)o * E->nb, index + (size_t)(o + 1) * E->nb);
+        ops[o].blk.assign(E->nb, nullptr);
+        for (int b = 0; b < E->nb; ++b) {
+          const int t = ops[o].index[b];
+          if (t < 0) continue;
+          ops[o].blk[b] = dp;
+          dp += (size_t)E->dims[t] * E->dims[b];
+        }
+      }
+    };
+    std::vector<BlockOp> mu, ka;
+    build(nmu, mu_index, mu_data, mu);
+    build(nka, ka_index, ka_data, ka);
+    size_t tot = (size_t)E->r * nmu * nka;
+    std::vector<cd> acc(tot, 0.0);
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+#pragma omp parallel num_threads(nthreads)
+    {
+      Backbone B(m, topo, E->n, E->p, true);
+      Work w;
+      alloc_work(*E, w);
+      std::vector<cd> loc(tot, 0.0);
+#pragma omp for schedule(dynamic, 4)
+      for (long z = 0; z < count; ++z) {
+        long f = fix ? fix[z] : z;
+        B.set_flat_index(f, E->poles_beta);
+        eval_correlator(*E, B, g, mu, ka, f, w, loc.data());
+      }
+#pragma omp critical
+      for (size_t x = 0; x < tot; ++x) acc[x] += loc[x];
+    }
+    std::copy(acc.begin(), acc.end(), (cd *)out);
+    return 0;
+  } catch (std::exception &e) { g_err = e.what(); return 1; }
+}
+
+// expectation_value(op, ad, G) block_sparse.cpp:797-818: sum += -trace(O_b G_b(beta)) over the blocks with an
+// operator block (op_index[b] == b), G_b(beta) by DLR evaluation; the trace entries (O G)_xx as fused
+// multiply-adds over the inner index, the diagonal and the blocks summed in order.
+int ora_expectation(void *dv, int nb, const int *dims, const double *G_, const int *op_index, const double *op_data, double *out) {
+  try {
+    const Dlr &D = *(Dlr *)dv;
+    const int r = D.r;
+    const cd *G = (const cd *)G_, *op = (const cd *)op_data;
+    cd sum = 0;
+    size_t goff = 0;
+    for (int b = 0; b < nb; ++b) {
+      const int d = dims[b];
+      const size_t sz = (size_t)r * d * d;
+      if (op_index[b] != -1 && op_index[b] != b) throw std::invalid_argument("expectation_value: operator must be block diagonal");
+      if (op_index[b] == b) {
+        std::vector<cd> c(sz), gb((size_t)d * d);
+        D.vals2coefs(G + goff, (long)d * d, c.data());
+        D.coefs2eval(c.data(), (long)d * d, 1.0, gb.data());
+        cd tr = 0;
+        for (int x = 0; x < d; ++x) {
+          cd s = 0;
+          for (int y = 0; y < d; ++y) s = cfma(op[x * d + y], gb[y * d + x], s);
+          tr += s;
+        }
+        sum += -tr;
+        op += (size_t)d * d;
+      }
+      goff += sz;
+    }
+    out[0] = sum.real();
+    out[1] = sum.imag();
+    return 0;
+  } catch (std::exception &e) { g_err = e.what(); return 1; }
+}
+
 // Hybridization values / reflected values and kernel tables (for cross-checks)
 int ora_hyb_values(void *ev, double *vals, double *vals_refl) {
   auto *E = (Evaluator *)ev;

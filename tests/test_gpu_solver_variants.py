@@ -1,0 +1,81 @@
+"""Root and ODE normalizations of the self-consistent solve (block_sparse_solver.py:296-336, 744-1030) and the
+solver's state I/O (block_sparse_solver.py:1178-1204), on the device, against the oracle's restatement.
+
+Parity: in the ordered summation mode every Dyson solve, convolution and trace agrees with the oracle bit
+for bit and scipy's root / ODE iterations see the same numbers, so the solves agree to round-off (1e-13).
+The normalizations must also agree with one another to the convergence tolerance, as the reference's own
+test does (test/python/block_sparse_normalization.py:111-137)."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from xca_b200 import models
+
+pytestmark = pytest.mark.gpu
+
+BETA, LAM, EPS = 10.0, 100.0, 1e-10
+
+
+def _solver(precision="fp64_ordered"):
+    from xca_b200.block_sparse_solver import BlockSparseSolver
+    from xca_b200.pycppdlr import MeshDLRImTime
+    mesh = MeshDLRImTime(beta=BETA, statistic="Fermion", w_max=LAM / BETA, eps=EPS)
+    m = models.anderson(mesh.dlr_rf, mesh.dlr_it.it, BETA, LAM, EPS)
+    S = BlockSparseSolver(m.ad, BETA, LAM / BETA, EPS, precision=precision)
+    delta = np.zeros((S.r, 2, 2), np.complex128)
+    dv = models.bethe_delta(BETA, S.it)
+    delta[:, 0, 0] = dv
+    delta[:, 1, 1] = dv
+    S.Delta_tau = delta
+    return S, m
+
+
+def _max_diff(A, B):
+    return max(float(np.max(np.abs(a - b))) for a, b in zip(A, B))
+
+
+@pytest.mark.parametrize("normalization", ["root", "ode+classic", "ode+root"])
+def test_normalization_variant_vs_oracle(normalization):
+    S, m = _solver()
+    S.solve(max_order=2, tol=1e-8, maxiter=40, normalization=normalization)
+    d = O.Dlr(LAM, EPS, rf=S.rf, it=S.it)
+    ev = O.Evaluator(d, BETA, S.hyb_poles, S.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
+    G, Sig, eta, g, n_iter, diff = O.solve(d, ev, BETA, m.G0, 2, 1e-8, 40, spgf_max_order=2, ordered=True, normalization=normalization,
+                                           eps=EPS)
+    print(f"{normalization}: iterations {S.n_ppsc_iter} / {n_iter}, |dG| {_max_diff(S.G, G):.2e}, |deta| {abs(S.eta - eta):.2e}, "
+          f"Z = {-O.trace_beta(d, G).real:.15f}")
+    assert S.n_ppsc_iter == n_iter and S.diff_G < 1e-8
+    assert _max_diff(S.G, G) <= 1e-13
+    assert abs(S.eta - eta) <= 1e-13
+    assert float(np.max(np.abs(S.G_tau - g))) <= 1e-13
+    # Z(eta) = 1 after a root normalization
+    if normalization.endswith("root"):
+        assert abs(-O.trace_beta(d, G).real - 1.0) < 1e-8
+
+
+def test_normalizations_agree():
+    # the reference's check: NCA to diff_G < 1e-4 with each normalization, single-particle G within 1e-4
+    gs = {}
+    for normalization in ("classic", "root", "ode+classic", "ode+root"):
+        S, _ = _solver("fp64")
+        S.solve(max_order=1, tol=1e-4, maxiter=40, normalization=normalization)
+        assert S.diff_G < 1e-4
+        gs[normalization] = S.G_tau
+    for k, g in gs.items():
+        assert float(np.max(np.abs(g - gs["classic"]))) < 1e-4, k
+
+
+def test_state_save_load_resume(tmp_path):
+    # NCA, save, load into a new solver, then OCA: the same as NCA then OCA without the round trip
+    from xca_b200.block_sparse_solver import BlockSparseSolver
+    S, _ = _solver()
+    S.solve(max_order=1, tol=1e-10, maxiter=60)
+    path = str(tmp_path / "state.npz")
+    S.save(path)
+    R = BlockSparseSolver.load(path)
+    assert R == S
+    S.solve(max_order=2, tol=1e-10, maxiter=60)
+    R.solve(max_order=2, tol=1e-10, maxiter=60)
+    assert R.n_ppsc_iter == S.n_ppsc_iter
+    assert _max_diff(R.G, S.G) == 0.0 and R.eta == S.eta

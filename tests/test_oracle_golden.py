@@ -278,3 +278,25 @@ def test_oracle_item_list_is_stable():
     a = ev.item_list(G, [[0, 2], [1, 4], [3, 5]], 0, 2000)
     b = ev.item_list(G, [[0, 2], [1, 4], [3, 5]], 0, 2000)
     assert a.shape[0] > 0 and np.array_equal(a, b)
+
+
+def test_get_op_mat_matches_field_operator_blocks():
+    # the block form of c_k from AtomDiag.get_op_mat is the F slab of k's symmetry set
+    from xca_b200 import models
+    from xca_b200.atom_diag import FockSpace
+    d = O.Dlr(40.0, 1e-8)
+    m = models.kanamori_2orb(d.rf, d.it, 4.0, 40.0, 1e-8)
+    fs = FockSpace(m.n)
+    sinds = {}
+    for o in range(m.n):
+        sinds[o] = sum(1 for o2 in range(o) if m.labels[o2] == m.labels[o])
+    for o in range(m.n):
+        idx, blks = m.ad.get_op_mat(fs.c(o))
+        s = m.labels[o]
+        assert np.array_equal(idx, m.F_index[s])
+        for b in range(len(idx)):
+            if idx[b] >= 0:
+                assert np.array_equal(blks[b], m.F_blocks[s][b][sinds[o]])
+    # a density is block diagonal
+    idx, _ = m.ad.get_op_mat(fs.n_op(1))
+    assert all(i in (-1, b) for b, i in enumerate(idx))

@@ -76,6 +76,10 @@ SIGNATURES = {
     "xca_synchronize": [P],
     "xca_kernel_launches": [P, lp],
     "xca_set_precision_mode": [P, I],
+    "xca_compute_one_time_correlator": [P, dp, I, ip, dp, I, ip, dp, I, ip, lp, L, dp],
+    "xca_convolve_ppsc": [P, dp, dp, dp],
+    "xca_convolve_ppsc_device": [P, P, P, P],
+    "xca_expectation_value": [P, dp, ip, dp, dp],
     "xca_get_precision_mode": [P, ip],
 }
 _RESTYPES = {"xca_last_error": ctypes.c_char_p}

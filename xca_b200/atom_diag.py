@@ -54,8 +54,9 @@ class AtomDiag:
     only Fock states for which it returns True (used for the N = 4..6 d-shell model).
     """
 
-    def __init__(self, H, n, quantum_numbers=None, restrict=None):
+    def __init__(self, H, n, quantum_numbers=None, restrict=None, subspaces=None):
         H = np.asarray(H)
+        self.H = H
         self.n = n
         self.fock = FockSpace(n)
         dim = 1 << n
@@ -63,7 +64,11 @@ class AtomDiag:
         keep = [s for s in range(dim) if restrict is None or restrict(s)]
         self.c_full = [self.fock.c(k) for k in range(n)]
         self.cdag_full = [self.fock.cdag(k) for k in range(n)]
-        if quantum_numbers is not None:
+        if subspaces is not None:
+            # an explicit partition (as saved by to_dict): lists of Fock states
+            subspaces = [[int(x) for x in sub] for sub in subspaces]
+            keep = sorted(x for sub in subspaces for x in sub)
+        elif quantum_numbers is not None:
             qn = [np.asarray(q) for q in quantum_numbers]
             groups = {}
             order = []
@@ -154,8 +159,40 @@ class AtomDiag:
             groups.setdefault(find(s), []).append(s)
         return list(groups.values())
 
+    def to_dict(self):
+        """The Hamiltonian and the subspace partition, from which ``from_dict`` rebuilds this object."""
+        return {"H": self.H, "n": self.n, "subspaces": [fs.copy() for fs in self.fock_states]}
+
+    @classmethod
+    def from_dict(cls, d):
+        return cls(d["H"], int(d["n"]), subspaces=d["subspaces"])
+
     def get_subspace_dims(self):
         return [len(fs) for fs in self.fock_states]
+
+    def get_op_mat(self, op):
+        """Block form of a Fock-space operator ``op`` (a dense 2^n x 2^n matrix, e.g. built from
+        ``FockSpace.c`` / ``n_op``): per subspace b the subspace it maps b to (-1 if none) and the
+        (d_target x d_b) block in the Fock basis.  These are the blocks that the reference builds from
+        ``ad.get_op_mat(op)`` and the unitary matrices (``setup_ops_from_triqs_2nd_quant_ops``,
+        ``c++/triqs_xca/block_sparse_backbone.cpp:810-840``; ``expectation_value``,
+        ``c++/triqs_xca/block_sparse.cpp:803-811``): the basis of G and of the field operators here."""
+        op = np.asarray(op)
+        nb = self.n_subspaces
+        index = np.full(nb, -1, dtype=np.int32)
+        blocks = [None] * nb
+        for b, fi in enumerate(self.fock_states):
+            sub = op[:, fi]
+            rows = np.nonzero(np.any(np.abs(sub) > 0, axis=1))[0]
+            tgt = {self._state_sub[int(x)] for x in rows if int(x) in self._state_sub}
+            if len(tgt) > 1:
+                raise ValueError("AtomDiag.get_op_mat: the operator maps a subspace into several subspaces")
+            if not tgt:
+                continue
+            t = tgt.pop()
+            index[b] = t
+            blocks[b] = np.asarray(op[np.ix_(self.fock_states[t], fi)], dtype=np.complex128)
+        return index, blocks
 
 
 def get_operators(ad, n=None):

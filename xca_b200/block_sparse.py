@@ -210,6 +210,64 @@ class DiagramEvaluator:
                                            rows_n, ctypes.byref(n)))
         return rows[:rows_n]
 
+    def compute_one_time_correlator(self, G_ppsc, ops_tau, ops_0, ad, topology, f_ix=None):
+        """C(tau)[mu][ka] of one topology with the operators ops_tau at tau and ops_0 at 0, (r, len(ops_tau),
+        len(ops_0)) complex (``compute_one_time_correlator``, bsb.cpp:843-866).  An operator is a dense Fock-space
+        matrix (converted with ``ad.get_op_mat``) or already in block form ``(index, blocks)``."""
+        t, m = self._topo(topology)
+        g = self.pack(G_ppsc)
+
+        def blocked(ops):
+            idx, parts = [], []
+            for op in ops:
+                i, blks = op if isinstance(op, tuple) else ad.get_op_mat(op)
+                i = np.asarray(i, np.int32)
+                if i.shape != (len(self.dims),):
+                    raise ValueError(f"operator block index of shape {i.shape}, expected ({len(self.dims)},)")
+                idx.append(i)
+                for b, tb in enumerate(i):
+                    if tb >= 0:
+                        blk = np.asarray(blks[b], np.complex128)
+                        if blk.shape != (self.dims[tb], self.dims[b]):
+                            raise ValueError(f"operator block {b} has shape {blk.shape}, expected {(self.dims[tb], self.dims[b])}")
+                        parts.append(blk.ravel())
+            data = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(1, np.complex128))
+            return np.ascontiguousarray(np.concatenate(idx)), data
+
+        mi, md = blocked(ops_tau)
+        ki, kd = blocked(ops_0)
+        out = np.zeros((self.r, len(ops_tau), len(ops_0)), np.complex128)
+        if f_ix is None:
+            fp, nf = None, 0
+        else:
+            fix = np.ascontiguousarray(np.atleast_1d(f_ix), dtype=np.int64)
+            fp, nf = _lib.as_lp(fix), len(fix)
+        _lib.check(_lib.lib().xca_compute_one_time_correlator(
+            self._ctx, _lib.as_dp(g.view(np.float64)), len(ops_tau), _lib.as_ip(mi), _lib.as_dp(md.view(np.float64)), len(ops_0),
+            _lib.as_ip(ki), _lib.as_dp(kd.view(np.float64)), m, _lib.as_ip(t), fp, nf, _lib.as_dp(out.view(np.float64))))
+        return out
+
+    def convolve_ppsc(self, G1, G2):
+        """Per block the time-ordered DLR convolution (G1 * G2)(tau) (``convolve_ppsc``, block_sparse.cpp:832-850)."""
+        a, b = self.pack(G1), self.pack(G2)
+        out = np.zeros_like(a)
+        _lib.check(_lib.lib().xca_convolve_ppsc(self._ctx, _lib.as_dp(a.view(np.float64)), _lib.as_dp(b.view(np.float64)),
+                                                _lib.as_dp(out.view(np.float64))))
+        return self.unpack(out)
+
+    def expectation_value(self, op, ad, G_ppsc):
+        """-sum_b Tr[O_b G_b(beta)] of a block-diagonal Fock-space operator (``expectation_value``,
+        block_sparse.cpp:797-818); ``op`` a dense Fock-space matrix or ``(index, blocks)``."""
+        idx, blks = op if isinstance(op, tuple) else ad.get_op_mat(op)
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        parts = [np.asarray(blks[b], np.complex128).ravel() for b in range(len(idx)) if idx[b] >= 0]
+        data = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(1, np.complex128))
+        g = self.pack(G_ppsc)
+        out = np.zeros(2)
+        _lib.check(_lib.lib().xca_expectation_value(self._ctx, _lib.as_dp(g.view(np.float64)), _lib.as_ip(idx),
+                                                    _lib.as_dp(data.view(np.float64)), _lib.as_dp(out)))
+        return complex(out[0], out[1])
+
     def trace(self, G_ppsc):
         """sum_b Tr G_b(beta) from the DLR expansion of each block (``trace``, block_sparse.cpp:852-861)."""
         g = self.pack(G_ppsc)
@@ -246,6 +304,9 @@ class DiagramEvaluator:
         Z, de = ctypes.c_double(), ctypes.c_double()
         _lib.check(_lib.lib().xca_normalize_device(self._ctx, ctypes.c_void_p(G_dev), ctypes.byref(Z), ctypes.byref(de)))
         return Z.value, de.value
+
+    def convolve_ppsc_device(self, G1_dev, G2_dev, H_dev):
+        _lib.check(_lib.lib().xca_convolve_ppsc_device(self._ctx, ctypes.c_void_p(G1_dev), ctypes.c_void_p(G2_dev), ctypes.c_void_p(H_dev)))
 
     def trace_device(self, G_dev):
         out = np.zeros(2)
@@ -337,3 +398,86 @@ class DiagramEvaluator:
         out = ctypes.c_long()
         _lib.check(_lib.lib().xca_kernel_launches(self._ctx, ctypes.byref(out)))
         return out.value
+
+
+# ---------------------------------------------------------------- free functions of the reference's module
+class _BlockBasis:
+    """Device context holding only a DLR basis and a block structure (the state the free functions need)."""
+
+    def __init__(self, beta, lam, eps, rf, it, dims, device=0):
+        L = _lib.lib()
+        self._ctx = ctypes.c_void_p()
+        _lib.check(L.xca_ctx_create(int(device), ctypes.byref(self._ctx)))
+        self.rf = np.ascontiguousarray(rf, dtype=float)
+        self.it = np.ascontiguousarray(it, dtype=float)
+        self.dims = np.ascontiguousarray(dims, dtype=np.int32)
+        self.r = len(self.rf)
+        _lib.check(L.xca_basis_setup(self._ctx, float(beta), float(lam), float(eps), self.r, _lib.as_dp(self.rf), _lib.as_dp(self.it),
+                                     len(self.dims), _lib.as_ip(self.dims)))
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx and _lib._lib is not None:
+            _lib._lib.xca_ctx_destroy(ctx)
+            self._ctx = None
+
+
+_BASES = {}
+
+
+def _basis_for(G, mesh):
+    blocks = _blocks_of(G)
+    dims = tuple(int(g.shape[1]) for g in blocks)
+    key = (mesh.beta, mesh.lam, mesh.eps, dims)
+    if key not in _BASES:
+        _BASES[key] = _BlockBasis(mesh.beta, mesh.lam, mesh.eps, mesh.dlr_rf, mesh.dlr_it.it, dims)
+    return _BASES[key], blocks
+
+
+def _packed(blocks):
+    return np.ascontiguousarray(np.concatenate([np.asarray(g, np.complex128).ravel() for g in blocks]))
+
+
+def _unpacked(flat, dims, r):
+    out, off = [], 0
+    for d in dims:
+        out.append(flat[off:off + r * d * d].reshape(r, d, d).copy())
+        off += r * d * d
+    return out
+
+
+def convolve_ppsc(G1, G2, mesh):
+    """``convolve_ppsc(G1, G2)`` (``c++/triqs_xca/block_sparse.cpp:832-850``) on the DLR mesh ``mesh``
+    (TRIQS Gfs carry their mesh; here it is passed alongside the blocks)."""
+    B, b1 = _basis_for(G1, mesh)
+    b2 = _blocks_of(G2)
+    a, b = _packed(b1), _packed(b2)
+    if a.shape != b.shape:
+        raise ValueError("convolve_ppsc: G1 and G2 have different block structures")
+    out = np.zeros_like(a)
+    _lib.check(_lib.lib().xca_convolve_ppsc(B._ctx, _lib.as_dp(a.view(np.float64)), _lib.as_dp(b.view(np.float64)),
+                                            _lib.as_dp(out.view(np.float64))))
+    return _unpacked(out, B.dims, B.r)
+
+
+def trace(G, mesh):
+    """``trace(G)`` = sum_b Tr G_b(beta) (``c++/triqs_xca/block_sparse.cpp:852-861``)."""
+    B, blocks = _basis_for(G, mesh)
+    g = _packed(blocks)
+    out = np.zeros(2)
+    _lib.check(_lib.lib().xca_trace(B._ctx, _lib.as_dp(g.view(np.float64)), _lib.as_dp(out)))
+    return complex(out[0], out[1])
+
+
+def expectation_value(op, ad, G, mesh):
+    """``expectation_value(op, ad, G)`` = -sum_b Tr[O_b G_b(beta)] (``c++/triqs_xca/block_sparse.cpp:797-818``)."""
+    B, blocks = _basis_for(G, mesh)
+    idx, blks = op if isinstance(op, tuple) else ad.get_op_mat(op)
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    parts = [np.asarray(blks[b], np.complex128).ravel() for b in range(len(idx)) if idx[b] >= 0]
+    data = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(1, np.complex128))
+    g = _packed(blocks)
+    out = np.zeros(2)
+    _lib.check(_lib.lib().xca_expectation_value(B._ctx, _lib.as_dp(g.view(np.float64)), _lib.as_ip(idx), _lib.as_dp(data.view(np.float64)),
+                                                _lib.as_dp(out)))
+    return complex(out[0], out[1])

@@ -24,7 +24,9 @@ from .models import dlr_fit_hybridization, rel2abs
 from .pycppdlr import MeshDLRImTime
 
 # device buffer slots of the solver's slabs (the evaluator's buffers 0..9 stay free for callers)
-_SLOTS = {"G": 10, "Gn": 11, "S": 12}
+_SLOTS = {"G": 10, "Gn": 11, "S": 12, "Sa": 13, "Gt": 14, "W1": 15, "W2": 16}
+
+NORMALIZATIONS = ("classic", "root", "ode+classic", "ode+root")
 
 
 class BlockSparseSolver:
@@ -90,8 +92,10 @@ class BlockSparseSolver:
     def solve(self, max_order, tol=1e-4, maxiter=10, mix=1.0, hyb_comp=False, normalization="classic", spgf_max_order=None,
               verbose=None):
         """BlockSparseSolver.solve (block_sparse_solver.py:240-355) with the 'classic' normalisation."""
-        if normalization != "classic":
-            raise NotImplementedError(f"normalization {normalization!r} is not available on the device path")
+        if normalization not in NORMALIZATIONS:
+            raise NotImplementedError(f"normalization {normalization!r} is not available on the device path "
+                                      f"(available: {', '.join(NORMALIZATIONS)})")
+        self.normalization = normalization
         verbose = self.verbose if verbose is None else verbose
         self.max_order = max_order
         self.spgf_max_order = spgf_max_order if spgf_max_order is not None else max_order
@@ -103,9 +107,16 @@ class BlockSparseSolver:
         t0 = time.perf_counter()
         for it in range(1, maxiter + 1):
             self._sigma_device(max_order)
+            if normalization in ("ode+classic", "ode+root"):
+                self.solve_ppsc_chempot_adiabatic_ode(tol=100 * self.eps)
+            if normalization in ("root", "ode+root"):
+                self.solve_ppsc_chempot_newton(xtol=10 * self.eps)
             d.dyson_solve_device(self._buf["S"], self.eta, self._buf["Gn"], hermitize=True)
-            Z, deta = d.normalize_device(self._buf["Gn"])
-            self.eta += deta
+            if normalization in ("classic", "ode+classic"):
+                Z, deta = d.normalize_device(self._buf["Gn"])
+                self.eta += deta
+            else:
+                Z = -d.trace_device(self._buf["Gn"]).real
             self.diff_G = d.max_abs_diff_device(self._buf["Gn"], self._buf["G"])
             if verbose:
                 print(f"iter = {it}, diff_G = {self.diff_G:2.2E}, Z = {Z:+2.6E}, eta = {self.eta:2.2E}")
@@ -121,6 +132,143 @@ class BlockSparseSolver:
         if self.spgf_max_order > 0:
             self.G_tau = self.eval_single_particle_greens_function(self.G, self.spgf_max_order)
         return self
+
+    # -- eta from Z(eta) = 1 ('root' / 'ode' normalizations, block_sparse_solver.py:744-1030).  G_alpha solves the
+    # Dyson equation with alpha * Sigma (the current Sigma on the device) at eta; every Dyson solve, convolution
+    # and trace runs on the device, the scalar root / ODE iteration on the host with scipy, as the reference.
+    def _g_alpha(self, alpha, eta):
+        d = self.d
+        src = self._buf["S"]
+        if alpha != 1.0:
+            d.zero_device(self._buf["Sa"], d.slab)
+            d.axpby_device(alpha, self._buf["S"], 0.0, self._buf["Sa"])
+            src = self._buf["Sa"]
+        d.dyson_solve_device(src, float(eta), self._buf["Gt"], hermitize=True)
+        return self._buf["Gt"]
+
+    def Z_alpha_minus_one_and_derivative_and_2nd_derivative(self, alpha, eta):
+        """Z_alpha - 1 and its first two eta derivatives: Z = -Tr G(beta), dZ/deta = -Tr (G * G)(beta),
+        d2Z/deta2 = -2 Tr ((G * G) * G)(beta) (block_sparse_solver.py:800-816)."""
+        d = self.d
+        G = self._g_alpha(alpha, eta)
+        Za = -d.trace_device(G).real
+        d.convolve_ppsc_device(G, G, self._buf["W1"])
+        dZ = -d.trace_device(self._buf["W1"]).real
+        d.convolve_ppsc_device(self._buf["W1"], G, self._buf["W2"])
+        d2Z = -2 * d.trace_device(self._buf["W2"]).real
+        return Za - 1, dZ, d2Z
+
+    def deta_dalpha(self, alpha, eta):
+        """d eta / d alpha = -Tr[G_a * Sigma * G_a] / Tr[G_a * G_a] (block_sparse_solver.py:819-838)."""
+        d = self.d
+        G = self._g_alpha(alpha, eta)
+        d.convolve_ppsc_device(G, G, self._buf["W1"])
+        tr_gg = -d.trace_device(self._buf["W1"])
+        d.convolve_ppsc_device(self._buf["S"], G, self._buf["W1"])
+        d.convolve_ppsc_device(G, self._buf["W1"], self._buf["W2"])
+        tr_gsg = -d.trace_device(self._buf["W2"])
+        return -tr_gsg / tr_gg
+
+    def solve_ppsc_chempot_newton(self, **kwargs):
+        """eta with Z(eta) = 1 by Halley's method from the current eta (solve_ppsc_chempot_newton,
+        block_sparse_solver.py:1000-1029)."""
+        from scipy.optimize import root_scalar
+        sol = root_scalar(lambda eta: self.Z_alpha_minus_one_and_derivative_and_2nd_derivative(1.0, eta), x0=self.eta, fprime=True,
+                          fprime2=True, method="halley", **kwargs)
+        self.eta = float(sol.root)
+        return sol
+
+    def solve_ppsc_chempot_adiabatic_ode(self, tol=1e-9, method="RK23"):
+        """eta(alpha = 1) from d eta / d alpha along alpha in [0, 1], eta(0) = 0 (solve_ppsc_chempot_adiabatic_ode,
+        block_sparse_solver.py:896-923)."""
+        from scipy.integrate import solve_ivp
+        sol = solve_ivp(lambda t, y: self.deta_dalpha(t, y[0]).real, (0.0, 1.0), np.array([0.0]), atol=tol, method=method,
+                        dense_output=True)
+        self.eta = float(sol.y[0, -1])
+        return sol
+
+    # -- state I/O (__reduce_to_dict__ / __factory_from_dict__, block_sparse_solver.py:1178-1204): everything but
+    # the device evaluator; h5 is not available here, so the state goes to a numpy .npz archive
+    _STATE_ARRAYS = ("G", "Sigma", "G0", "Delta_tau", "hyb_poles", "hyb_coeffs", "G_tau")
+    _STATE_SCALARS = ("beta", "w_max", "eps", "eta", "eta0", "n_ppsc_iter", "diff_G", "max_order", "spgf_max_order", "precision",
+                      "normalization", "verbose")
+
+    def __reduce_to_dict__(self):
+        out = {"atom_diag": self.ad.to_dict()}
+        for k in self._STATE_ARRAYS + self._STATE_SCALARS:
+            if hasattr(self, k):
+                v = getattr(self, k)
+                out[k] = [np.array(g) for g in v] if isinstance(v, list) else v
+        return out
+
+    @classmethod
+    def __factory_from_dict__(cls, name, d):
+        from .atom_diag import AtomDiag
+        ret = cls(AtomDiag.from_dict(d["atom_diag"]), d["beta"], d["w_max"], d["eps"], verbose=False,
+                  precision=d.get("precision", "fp64"))
+        for k in cls._STATE_ARRAYS + cls._STATE_SCALARS:
+            if k in d:
+                setattr(ret, k, d[k])
+        return ret
+
+    def __eq__(self, other):
+        a, b = self.__reduce_to_dict__(), other.__reduce_to_dict__()
+        if a.keys() != b.keys():
+            return False
+
+        def same(x, y):
+            if isinstance(x, dict):
+                return x.keys() == y.keys() and all(same(x[k], y[k]) for k in x)
+            if isinstance(x, (list, tuple)):
+                return len(x) == len(y) and all(same(u, v) for u, v in zip(x, y))
+            if isinstance(x, np.ndarray) or isinstance(y, np.ndarray):
+                return np.array_equal(np.asarray(x), np.asarray(y))
+            return x == y
+
+        return all(same(a[k], b[k]) for k in a)
+
+    def save(self, path):
+        """Write the solver state to ``path`` (.npz)."""
+        flat = {}
+
+        def put(prefix, v):
+            if isinstance(v, dict):
+                for k, x in v.items():
+                    put(f"{prefix}{k}/", x)
+            elif isinstance(v, list):
+                flat[f"{prefix}len"] = np.array(len(v))
+                for i, x in enumerate(v):
+                    put(f"{prefix}{i}/", x)
+            else:
+                flat[prefix.rstrip("/")] = np.asarray(v) if v is not None else np.array("None")
+
+        put("", self.__reduce_to_dict__())
+        np.savez_compressed(path, **flat)
+
+    @classmethod
+    def load(cls, path):
+        """Solver rebuilt from a file written by ``save``; a later ``solve`` continues from its G and eta."""
+        z = np.load(path, allow_pickle=False)
+        tree = {}
+        for key in z.files:
+            parts = key.split("/")
+            node = tree
+            for p in parts[:-1]:
+                node = node.setdefault(p, {})
+            node[parts[-1]] = z[key]
+
+        def build(node):
+            if isinstance(node, dict):
+                if "len" in node and set(node) == {"len"} | {str(i) for i in range(int(node["len"]))}:
+                    return [build(node[str(i)]) for i in range(int(node["len"]))]
+                return {k: build(v) for k, v in node.items()}
+            if node.dtype.kind == "U":
+                s = str(node)
+                return None if s == "None" else s
+            return node.item() if node.ndim == 0 else node
+
+        d = build(tree)
+        return cls.__factory_from_dict__(cls.__name__, d)
 
     def eval_pseudo_particle_self_energy(self, G, max_order):
         """Sigma of orders 1..max_order for a host G (block_sparse_solver.py:597-640)."""

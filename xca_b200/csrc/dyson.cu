@@ -38,6 +38,26 @@ int launch_trace_beta(cudaStream_t s, const DysonBasis &B, const double *G, doub
   return 1;
 }
 
+template <int RP>
+int launch_convolve_ppsc(cudaStream_t s, const DysonBasis &B, const double *G1, const double *G2, double *H) {
+  const size_t sm = (2 * (size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
+  if (cudaFuncSetAttribute(convolve_ppsc_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    check_launch("convolve_ppsc_kernel attributes");
+  convolve_ppsc_kernel<RP><<<B.nb, 256, sm, s>>>(B, G1, G2, H);
+  check_launch("convolve_ppsc_kernel");
+  return 1;
+}
+
+template <int RP>
+int launch_expectation_beta(cudaStream_t s, const DysonBasis &B, const double *G, const double *ops, const long *op_off, double *out) {
+  const size_t sm = ((size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
+  if (cudaFuncSetAttribute(expectation_beta_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    check_launch("expectation_beta_kernel attributes");
+  expectation_beta_kernel<RP><<<B.nb, 128, sm, s>>>(B, G, ops, op_off, out);
+  check_launch("expectation_beta_kernel");
+  return 1;
+}
+
 int launch_energy_shift(cudaStream_t s, const DysonBasis &B, double *G, const double *fac) {
   dim3 grid(64, (unsigned)B.nb);
   energy_shift_kernel<<<grid, 256, 0, s>>>(B, G, fac);
@@ -61,6 +81,12 @@ int launch_axpby(cudaStream_t s, double alpha, const double *x, double beta, dou
 template int launch_dyson<32>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *);
 template int launch_dyson<48>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *);
 template int launch_dyson<64>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *);
+template int launch_convolve_ppsc<32>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);
+template int launch_convolve_ppsc<48>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);
+template int launch_convolve_ppsc<64>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);
+template int launch_expectation_beta<32>(cudaStream_t, const DysonBasis &, const double *, const double *, const long *, double *);
+template int launch_expectation_beta<48>(cudaStream_t, const DysonBasis &, const double *, const double *, const long *, double *);
+template int launch_expectation_beta<64>(cudaStream_t, const DysonBasis &, const double *, const double *, const long *, double *);
 template int launch_trace_beta<32>(cudaStream_t, const DysonBasis &, const double *, double *);
 template int launch_trace_beta<48>(cudaStream_t, const DysonBasis &, const double *, double *);
 template int launch_trace_beta<64>(cudaStream_t, const DysonBasis &, const double *, double *);

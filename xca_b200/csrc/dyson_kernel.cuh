@@ -368,3 +368,98 @@ __global__ void axpby_kernel(double alpha, const double *__restrict__ x, double 
 }
 
 }  // namespace xca
+
+namespace xca {
+
+// convolve_ppsc (c++/triqs_xca/block_sparse.cpp:832-850): per block, H = convolve(beta, K^-1 G1_b, K^-1 G2_b,
+// TIME_ORDERED) on the nodes, with the operation order of the CPU restatement: f = K^-1 G1, ft = W f,
+// g = K^-1 G2, gt = W g; Q_l = ft_l g_l + f_l gt_l and P'_l = K(0, om_l) (f_l g_l) (fused multiply-adds over
+// the inner index, the f gt term first); H(t_i) = fma(t_i, sum_l (beta K_il) P'_l, sum_l (beta K_il) Q_l).
+// One CTA per block; work holds 6 r d^2 doubles per block at B.woff.
+template <int RP>
+__global__ void __launch_bounds__(256) convolve_ppsc_kernel(DysonBasis B, const double *__restrict__ G1, const double *__restrict__ G2,
+                                                             double *__restrict__ H) {
+  extern __shared__ __align__(16) double smem[];
+  double *sLU = smem, *sW = sLU + RP * RP + RP;
+  int *sPerm = reinterpret_cast<int *>(sW + RP * RP);
+  stage_lu_w<RP>(B, sLU, sW, sPerm);
+  const int b = blockIdx.x, r = B.r, d = B.dims[b], dd = d * d;
+  double *f = B.work + B.woff[b], *ft = f + (long)r * dd, *g = ft + (long)r * dd, *gt = g + (long)r * dd;
+  double *Q = gt + (long)r * dd, *P = Q + (long)r * dd;
+  coefs_and_hilbert<RP, true>(sLU, sW, sPerm, r, dd, G1 + B.goff[b], f, ft);
+  coefs_and_hilbert<RP, true>(sLU, sW, sPerm, r, dd, G2 + B.goff[b], g, gt);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < r * dd; idx += blockDim.x) {
+    const int l = idx / dd, e = idx - l * dd, x = e / d, z = e - x * d;
+    const double *fl = f + (long)l * dd + x * d, *ftl = ft + (long)l * dd + x * d;
+    const double *gl = g + (long)l * dd + z, *gtl = gt + (long)l * dd + z;
+    double sq = 0.0, sp = 0.0;
+    for (int y = 0; y < d; ++y) {
+      sq = fmad(ftl[y], gl[y * d], fmad(fl[y], gtl[y * d], sq));
+      sp = fmad(fl[y], gl[y * d], sp);
+    }
+    Q[idx] = sq;
+    P[idx] = mul(B.k0[l], sp);
+  }
+  __syncthreads();
+  double *h = H + B.goff[b];
+  for (int idx = threadIdx.x; idx < r * dd; idx += blockDim.x) {
+    const int i = idx / dd, e = idx - i * dd;
+    double h1 = 0.0, h2 = 0.0;
+    for (int l = 0; l < r; ++l) {
+      const double bk = B.BKp[l * RP + i];
+      h1 = fmad(bk, Q[(long)l * dd + e], h1);
+      h2 = fmad(bk, P[(long)l * dd + e], h2);
+    }
+    h[idx] = fmad(B.tabs[i], h2, h1);
+  }
+}
+
+// expectation_value (c++/triqs_xca/block_sparse.cpp:797-818), per block b with a diagonal operator block O_b
+// (op_off[b] >= 0): G_b(beta) by DLR evaluation (K^-1 per entry, then sum_l K(1, om_l) c_l from zero in
+// ascending l), then out[b] = Tr[O_b G_b(beta)] = sum_x (sum_y O[x][y] G(beta)[y][x]) (fused multiply-adds
+// over y, the x sums in order); out[b] = 0 for blocks without an operator block.  work: r d^2 per block.
+template <int RP>
+__global__ void __launch_bounds__(128) expectation_beta_kernel(DysonBasis B, const double *__restrict__ G, const double *__restrict__ ops,
+                                                                const long *__restrict__ op_off, double *__restrict__ out) {
+  extern __shared__ __align__(16) double smem[];
+  double *sLU = smem;
+  int *sPerm = reinterpret_cast<int *>(sLU + RP * RP + RP);
+  for (int i = threadIdx.x; i < RP * RP + RP; i += blockDim.x) sLU[i] = B.LUp[i];
+  for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
+  __syncthreads();
+  const int b = blockIdx.x, r = B.r, d = B.dims[b], dd = d * d;
+  if (op_off[b] < 0) {
+    if (threadIdx.x == 0) out[b] = 0.0;
+    return;
+  }
+  const double *g = G + B.goff[b];
+  double *gb = B.work + B.woff[b];
+  for (int col = threadIdx.x; col < dd; col += blockDim.x) {
+    double x[RP];
+#pragma unroll
+    for (int i = 0; i < RP; ++i) {
+      const int src = sPerm[i];
+      x[i] = src >= 0 ? g[(long)src * dd + col] : 0.0;
+    }
+    lu_solve_reg<RP>(sLU, x);
+    double v = 0.0;
+#pragma unroll
+    for (int l = 0; l < RP; ++l)
+      if (l < r) v = add(v, mul(B.k1[l], x[l]));
+    gb[col] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double *O = ops + op_off[b];
+    double tr = 0.0;
+    for (int x = 0; x < d; ++x) {
+      double s = 0.0;
+      for (int y = 0; y < d; ++y) s = fmad(O[x * d + y], gb[y * d + x], s);
+      tr = add(tr, s);
+    }
+    out[b] = tr;
+  }
+}
+
+}  // namespace xca

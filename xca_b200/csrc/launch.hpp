@@ -32,6 +32,12 @@ int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const do
 template <int RP>
 int launch_trace_beta(cudaStream_t s, const DysonBasis &B, const double *G, double *out);
 
+template <int RP>
+int launch_convolve_ppsc(cudaStream_t s, const DysonBasis &B, const double *G1, const double *G2, double *H);
+
+template <int RP>
+int launch_expectation_beta(cudaStream_t s, const DysonBasis &B, const double *G, const double *ops, const long *op_off, double *out);
+
 int launch_energy_shift(cudaStream_t s, const DysonBasis &B, double *G, const double *fac);
 int launch_max_abs_diff(cudaStream_t s, int blocks, const double *a, const double *b, long n, double *out);
 int launch_axpby(cudaStream_t s, double alpha, const double *x, double beta, double *y, long n);

@@ -42,8 +42,10 @@ struct CorrClass {
 
 struct CorrBasis {
   const double *RFp;        // RP x RP column-major: K(t_i, -om_l) (reflect), 0 in the pad
-  const long *mu_off;       // [o * nb + b]: offset of F_o's (d_target x d_b) slab in ops (-1: none)
-  const long *ka_off;       // [o * nb + b]: offset of F^dag_o's slab in ops (-1: none)
+  const double *ops;        // slabs of the external operators (the evaluator's F / F^dag slabs for g(tau))
+  const long *mu_off;       // [mu * nb + b]: offset of O_mu's (d_target x d_b) slab in ops (-1: none)
+  const long *ka_off;       // [ka * nb + b]: offset of O'_ka's slab in ops (-1: none)
+  int nmu, nka;             // operators at tau and at 0 (the result is r x nmu x nka)
 };
 
 // Per-item pole data, decoded as Backbone::set_pole_inds (c++/triqs_xca/backbone.cpp:86-150).
@@ -207,7 +209,7 @@ __device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, 
 
 // Dynamic shared memory: LU (+ reciprocal diagonal) | W | BK | RF (column-major) | perm (RP ints).
 // Per-warp global scratch (`warp_doubles` each): T | X | Y (r * nmax^2 each), right chains and left chains
-// (nb slots of r * nmax^2 each), accumulator (r * n * n).
+// (nb slots of r * nmax^2 each), accumulator (r * nmu * nka).
 template <int RP>
 __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis CB, const CorrClass *__restrict__ classes,
                                                          const CorrChain *__restrict__ chains, const CorrTerm *__restrict__ terms,
@@ -225,7 +227,7 @@ __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis C
   }
   for (int i = threadIdx.x; i < RP; i += blockDim.x) sPerm[i] = B.perm[i];
   __syncthreads();
-  const int r = B.r, n = B.n, nb = B.nb;
+  const int r = B.r, nb = B.nb, nmu = CB.nmu, nka = CB.nka;
   const int lane = threadIdx.x & 31;
   const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long slab = (long)r * nmax * nmax;
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis C
   double *T = wb, *X = wb + slab, *Y = wb + 2 * slab;
   double *Rs = wb + 3 * slab, *Ls = Rs + (long)nb * slab;
   double *acc = Ls + (long)nb * slab;
-  for (int i = lane; i < r * n * n; i += 32) acc[i] = 0.0;
+  for (int i = lane; i < r * nmu * nka; i += 32) acc[i] = 0.0;
   __syncwarp();
   bool any = false;
   while (true) {
@@ -326,8 +328,8 @@ __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis C
         const CorrTerm &P = terms[C.term0 + k];
         const double *R = Rs + (long)P.rchain * slab;
         const double *L = Ls + (long)P.lchain * slab;
-        const double *Om = B.ops + CB.mu_off[P.mu * nb + P.e0];  // (c2 x c1)
-        const double *Ok = B.ops + CB.ka_off[P.ka * nb + P.e2];  // (c0 x c3)
+        const double *Om = CB.ops + CB.mu_off[P.mu * nb + P.e0];  // (c2 x c1)
+        const double *Ok = CB.ops + CB.ka_off[P.ka * nb + P.e2];  // (c0 x c3)
         const int c0 = P.c0, c1 = P.c1, c2 = P.c2, c3 = P.c3;
         for (int t = lane; t < r; t += 32) {
           const double *Rt = R + (long)t * c1 * c0, *Lt = L + (long)t * c3 * c2;
@@ -342,7 +344,7 @@ __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis C
               }
               s = fmad(tm, Ok[jj * c3 + i], s);
             }
-          double *a = acc + ((long)t * n + P.mu) * n + P.ka;
+          double *a = acc + ((long)t * nmu + P.mu) * nka + P.ka;
           *a = add(*a, s);
         }
         __syncwarp();
@@ -350,7 +352,7 @@ __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis C
     }
   }
   if (any)
-    for (int i = lane; i < r * n * n; i += 32) atomicAdd(gout + i, mul(scale, acc[i]));
+    for (int i = lane; i < r * nmu * nka; i += 32) atomicAdd(gout + i, mul(scale, acc[i]));
 }
 
 }  // namespace xca

@@ -202,6 +202,17 @@ struct CorrSet {
   DevBuf<WorkUnit> d_units;
 };
 
+// External operators of a correlator: O_mu at tau (mu < nmu) and O'_ka at 0 (ka < nka), each a block
+// operator (target block per block column, -1: none; a (d_target x d_b) slab per present column).  For
+// the single-particle Green's function they are F_o and F^dag_o of every orbital.
+struct ExtOps {
+  int nmu = 0, nka = 0;
+  std::vector<int> mu_idx, ka_idx;  // [op * nb + b]
+  const double *d_ops = nullptr;
+  const long *d_mu_off = nullptr, *d_ka_off = nullptr;
+  std::string key;                  // block structure, part of the work-list cache key
+};
+
 struct Ctx {
   int device = 0;
   int nsm = 148;  // streaming multiprocessors of the device
@@ -242,6 +253,9 @@ struct Ctx {
   std::vector<double> RFp;                // RP x RP column-major: K(t_i, -om_l)
   DevBuf<double> d_RFp, d_corr_scratch;
   DevBuf<long> d_mu_off, d_ka_off;
+  ExtOps spgf_ops;                        // F_o / F^dag_o of every orbital
+  DevBuf<double> d_xops;                  // one-time correlator: uploaded operator slabs
+  DevBuf<long> d_xmu_off, d_xka_off;
   std::map<std::string, std::unique_ptr<ClassSet>> noalloc_classes;  // host-only work lists of the allocation-free call
   int unit_batches = 4;  // panel batches per work unit
   int precision = XCA_PREC_FP64;
@@ -258,6 +272,8 @@ struct Ctx {
   std::vector<long> woff, moff;           // per-block work and system-matrix offsets
   long n_conv_rows = 0;                   // largest r d_b^2 (rows of the convolution-matrix kernel grid)
   DevBuf<double> d_k1, d_rf, d_g0, d_g0c, d_g0t, d_dwork, d_mats, d_rhs, d_red, d_efac;
+  DevBuf<double> d_bwork, d_ba, d_bb, d_bc, d_xop;  // convolve_ppsc / expectation_value scratch and operands
+  DevBuf<long> d_bwoff, d_xop_off;
   DevBuf<long> d_woff, d_moff;
   DevBuf<int> d_status;
 
@@ -724,8 +740,8 @@ static void real_part(const double *cplx, long n, std::vector<double> &out, cons
 // tuple) the right chains (set_directions / eval_correlator's walk over vertices 1 .. vct0-1,
 // block_sparse_backbone.cpp:540-566), the left chains (vertices vct0+1 .. 2m-1, :567-600) and the
 // (mu, b, ka) terms of the trace contraction (:602-706) that close; classes without a term are dropped.
-static CorrSet *get_corr(Ctx *c, const Topology &T, const std::vector<int> &zero) {
-  const std::string key = class_key(T, zero);
+static CorrSet *get_corr(Ctx *c, const Topology &T, const std::vector<int> &zero, const ExtOps &X) {
+  const std::string key = class_key(T, zero) + "|" + X.key;
   auto itc = c->corr_cache.find(key);
   if (itc != c->corr_cache.end()) return itc->second.get();
   auto cs = std::make_unique<CorrSet>();
@@ -820,16 +836,16 @@ static CorrSet *get_corr(Ctx *c, const Topology &T, const std::vector<int> &zero
       std::vector<CorrTerm> terms;
       std::vector<int> rused(nb, -1), lused(nb, -1);
       std::vector<int> rlist, llist;
-      for (int mu = 0; mu < n; ++mu)
+      for (int mu = 0; mu < X.nmu; ++mu)
         for (int b = 0; b < nb; ++b) {
           const int e0 = rend[b];
           if (incomplete(e0)) continue;
-          const int e1 = c->F_idx[c->labels[mu] * nb + e0];
+          const int e1 = X.mu_idx[mu * nb + e0];
           if (incomplete(e1)) continue;
           const int e2 = lend[e1];
           if (incomplete(e2)) continue;
-          for (int ka = 0; ka < n; ++ka) {
-            if (c->Fd_idx[c->labels[ka] * nb + e2] != b) continue;
+          for (int ka = 0; ka < X.nka; ++ka) {
+            if (X.ka_idx[ka * nb + e2] != b) continue;
             if (rused[b] < 0) { rused[b] = (int)rlist.size(); rlist.push_back(b); }
             if (lused[e1] < 0) { lused[e1] = (int)llist.size(); llist.push_back(e1); }
             CorrTerm P;
@@ -862,20 +878,23 @@ static CorrSet *get_corr(Ctx *c, const Topology &T, const std::vector<int> &zero
   return ret;
 }
 
-static void launch_corr(Ctx *c, CorrSet *cs, const WorkUnit *d_units, int n_units, const double *G_dev, double *g_dev, double scale,
-                        int nsig) {
+static void launch_corr(Ctx *c, CorrSet *cs, const ExtOps &X, const WorkUnit *d_units, int n_units, const double *G_dev, double *g_dev,
+                        double scale, int nsig) {
   if (n_units == 0) return;
   const int warps_per_cta = 4;
   const int grid = std::max(1, std::min(2 * c->nsm, (n_units + warps_per_cta - 1) / warps_per_cta));
   const long slab = (long)c->r * c->nmax * c->nmax;
-  const long warp_doubles = (3 + 2L * c->nb) * slab + (long)c->r * c->n * c->n;
+  const long warp_doubles = (3 + 2L * c->nb) * slab + (long)c->r * X.nmu * X.nka;
   c->d_corr_scratch.resize((size_t)grid * warps_per_cta * warp_doubles);
   c->d_counter.resize(1);
   CUDA_CHECK(cudaMemsetAsync(c->d_counter.ptr, 0, sizeof(int), c->stream));
   CorrBasis CB;
   CB.RFp = c->d_RFp.ptr;
-  CB.mu_off = c->d_mu_off.ptr;
-  CB.ka_off = c->d_ka_off.ptr;
+  CB.ops = X.d_ops;
+  CB.mu_off = X.d_mu_off;
+  CB.ka_off = X.d_ka_off;
+  CB.nmu = X.nmu;
+  CB.nka = X.nka;
   const DevBasis B = c->basis(nsig);
   switch (c->RP) {
 #define XCA_CORR(RPV)                                                                                                          \
@@ -919,6 +938,31 @@ static void launch_dyson(Ctx *c, const double *Sig_dev, double eta, int hermitiz
     case 32: c->launches += launch_dyson<32>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr); break;
     case 48: c->launches += launch_dyson<48>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr); break;
     default: c->launches += launch_dyson<64>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr); break;
+  }
+}
+
+// DysonBasis whose work area is the per-block scratch of the block-wise DLR operations (6 r d_b^2
+// doubles per block), for calls that need no Dyson set-up.
+static DysonBasis block_op_basis(Ctx *c) {
+  if (!c->d_bwoff.ptr || c->d_bwork.n < (size_t)(6 * c->slab)) {
+    std::vector<long> off(c->nb);
+    long o = 0;
+    for (int b = 0; b < c->nb; ++b) { off[b] = o; o += 6L * c->r * c->dims[b] * c->dims[b]; }
+    c->d_bwoff.upload(off, c->stream);
+    c->d_bwork.resize(std::max(o, 1L));
+  }
+  DysonBasis B = dyson_basis(c);
+  B.work = c->d_bwork.ptr;
+  B.woff = c->d_bwoff.ptr;
+  return B;
+}
+
+static void launch_convolve_blocks(Ctx *c, const double *G1_dev, const double *G2_dev, double *H_dev) {
+  const DysonBasis B = block_op_basis(c);
+  switch (c->RP) {
+    case 32: c->launches += launch_convolve_ppsc<32>(c->stream, B, G1_dev, G2_dev, H_dev); break;
+    case 48: c->launches += launch_convolve_ppsc<48>(c->stream, B, G1_dev, G2_dev, H_dev); break;
+    default: c->launches += launch_convolve_ppsc<64>(c->stream, B, G1_dev, G2_dev, H_dev); break;
   }
 }
 
@@ -982,6 +1026,49 @@ static void noalloc_fits(size_t need, const char *what) {
     throw Error(XCA_ERR_INVALID, std::string("xca_compute_self_energy_device_noalloc: ") + what + " need " +
                                      std::to_string(need) + " bytes of scratch, the fixed scratch array holds " +
                                      std::to_string(NOALLOC_SCRATCH_BYTES) + "; use xca_compute_self_energy_device");
+}
+
+// Host entry of a correlator over the external operators X (compute_single_ptcle_gf and
+// compute_one_time_correlator): every flat index (f_ix == NULL) or the listed ones.
+static void correlator_host(Ctx *c, const double *G, int m, const int *topology, const long *f_ix, long n_fix, const ExtOps &X,
+                            double *g_out, const char *who) {
+  Topology T = parse_topology(m, topology);
+  const long omax = ipow(c->n, m - 1), npt = ipow(c->p, m - 1);
+  const long nmaxb = (1L << (m - 1)) * omax * npt;
+  std::vector<double> g;
+  real_part(G, c->slab, g, "G");
+  const long nout = (long)c->r * X.nmu * X.nka;
+  c->d_G.resize(c->slab);
+  c->d_Sig.resize(std::max(c->slab, nout));
+  CUDA_CHECK(cudaMemcpyAsync(c->d_G.ptr, g.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  zero_kernel<<<64, 256, 0, c->stream>>>(c->d_Sig.ptr, nout);
+  c->launches++;
+  auto zero = zero_flags_device(c, c->d_G.ptr);
+  CorrSet *cs = get_corr(c, T, zero, X);
+  int nsig = prepare_tables(c, c->d_G.ptr, m);
+  if (f_ix == nullptr) {
+    launch_corr(c, cs, X, cs->d_units.ptr, (int)cs->units.size(), c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
+  } else {
+    std::vector<WorkUnit> units;
+    for (long z = 0; z < n_fix; ++z) {
+      const long f = f_ix[z];
+      if (f < 0 || f >= nmaxb) throw Error(XCA_ERR_RUNTIME, std::string("DiagramEvaluator::") + who + ": f_ix out of range");
+      const long o = f % omax, q = f / omax, pix = q % npt, fb = q / npt;
+      const int k = cs->cls_of_fbo[fb * omax + o];
+      if (k >= 0) units.push_back(WorkUnit{k, (int)pix, 1});
+    }
+    DevBuf<WorkUnit> du;
+    du.upload(units, c->stream);
+    launch_corr(c, cs, X, du.ptr, (int)units.size(), c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
+    CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  }
+  std::vector<double> out(nout);
+  CUDA_CHECK(cudaMemcpyAsync(out.data(), c->d_Sig.ptr, nout * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  for (long i = 0; i < nout; ++i) {
+    g_out[2 * i] = out[i];
+    g_out[2 * i + 1] = 0.0;
+  }
 }
 
 }  // namespace xca
@@ -1223,6 +1310,19 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
     }
     c->d_mu_off.upload(mo, s);
     c->d_ka_off.upload(ko, s);
+    ExtOps &X = c->spgf_ops;
+    X.nmu = X.nka = n;
+    X.mu_idx.assign((size_t)n * n_blocks, -1);
+    X.ka_idx.assign((size_t)n * n_blocks, -1);
+    for (int o = 0; o < n; ++o)
+      for (int b = 0; b < n_blocks; ++b) {
+        X.mu_idx[(size_t)o * n_blocks + b] = c->F_idx[labels[o] * n_blocks + b];
+        X.ka_idx[(size_t)o * n_blocks + b] = c->Fd_idx[labels[o] * n_blocks + b];
+      }
+    X.d_ops = c->d_ops.ptr;
+    X.d_mu_off = c->d_mu_off.ptr;
+    X.d_ka_off = c->d_ka_off.ptr;
+    X.key = "spgf";
   }
   CUDA_CHECK(cudaStreamSynchronize(s));
   c->ready = true;
@@ -1453,9 +1553,9 @@ int xca_compute_single_ptcle_gf_device(xca_ctx *ctx, const double *G_dev, int m,
   set_device(c);
   Topology T = parse_topology(m, topology);
   auto zero = zero_flags_device(c, G_dev);
-  CorrSet *cs = get_corr(c, T, zero);
+  CorrSet *cs = get_corr(c, T, zero, c->spgf_ops);
   int nsig = prepare_tables(c, G_dev, m);
-  launch_corr(c, cs, cs->d_units.ptr, (int)cs->units.size(), G_dev, g_dev, scale, nsig);
+  launch_corr(c, cs, c->spgf_ops, cs->d_units.ptr, (int)cs->units.size(), G_dev, g_dev, scale, nsig);
   API_END
 }
 
@@ -1464,43 +1564,127 @@ int xca_compute_single_ptcle_gf(xca_ctx *ctx, const double *G, int m, const int 
   auto *c = reinterpret_cast<Ctx *>(ctx);
   if (!c->ready) throw Error(XCA_ERR_INVALID, "evaluator not set up");
   set_device(c);
-  Topology T = parse_topology(m, topology);
-  const long omax = ipow(c->n, m - 1), npt = ipow(c->p, m - 1);
-  const long nmaxb = (1L << (m - 1)) * omax * npt;
+  correlator_host(c, G, m, topology, f_ix, n_fix, c->spgf_ops, g_out, "compute_single_ptcle_gf");
+  API_END
+}
+
+int xca_convolve_ppsc(xca_ctx *ctx, const double *G1, const double *G2, double *H_out) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_basis(c);
+  set_device(c);
+  std::vector<double> a, b;
+  real_part(G1, c->slab, a, "G1");
+  real_part(G2, c->slab, b, "G2");
+  c->d_ba.resize(c->slab);
+  c->d_bb.resize(c->slab);
+  c->d_bc.resize(c->slab);
+  CUDA_CHECK(cudaMemcpyAsync(c->d_ba.ptr, a.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CUDA_CHECK(cudaMemcpyAsync(c->d_bb.ptr, b.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  launch_convolve_blocks(c, c->d_ba.ptr, c->d_bb.ptr, c->d_bc.ptr);
+  std::vector<double> h(c->slab);
+  CUDA_CHECK(cudaMemcpyAsync(h.data(), c->d_bc.ptr, c->slab * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  for (long i = 0; i < c->slab; ++i) { H_out[2 * i] = h[i]; H_out[2 * i + 1] = 0.0; }
+  API_END
+}
+
+int xca_convolve_ppsc_device(xca_ctx *ctx, const double *G1_dev, const double *G2_dev, double *H_dev) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_basis(c);
+  set_device(c);
+  launch_convolve_blocks(c, G1_dev, G2_dev, H_dev);
+  API_END
+}
+
+int xca_expectation_value(xca_ctx *ctx, const double *G, const int *op_index, const double *op_data, double *out) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_basis(c);
+  set_device(c);
+  std::vector<long> off(c->nb, -1);
+  long pos = 0;
+  for (int b = 0; b < c->nb; ++b) {
+    const int t = op_index[b];
+    if (t == -1) continue;
+    if (t != b) throw Error(XCA_ERR_INVALID, "expectation_value: the operator must be block diagonal (connection[b] == b)");
+    off[b] = pos;
+    pos += (long)c->dims[b] * c->dims[b];
+  }
+  std::vector<double> ops;
+  real_part(op_data, pos, ops, "operator");
   std::vector<double> g;
   real_part(G, c->slab, g, "G");
-  const long nout = (long)c->r * c->n * c->n;
-  c->d_G.resize(c->slab);
-  c->d_Sig.resize(std::max(c->slab, nout));
-  CUDA_CHECK(cudaMemcpyAsync(c->d_G.ptr, g.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  zero_kernel<<<64, 256, 0, c->stream>>>(c->d_Sig.ptr, nout);
-  c->launches++;
-  auto zero = zero_flags_device(c, c->d_G.ptr);
-  CorrSet *cs = get_corr(c, T, zero);
-  int nsig = prepare_tables(c, c->d_G.ptr, m);
-  if (f_ix == nullptr) {
-    launch_corr(c, cs, cs->d_units.ptr, (int)cs->units.size(), c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
-  } else {
-    std::vector<WorkUnit> units;
-    for (long z = 0; z < n_fix; ++z) {
-      const long f = f_ix[z];
-      if (f < 0 || f >= nmaxb) throw Error(XCA_ERR_RUNTIME, "DiagramEvaluator::compute_single_ptcle_gf: f_ix out of range");
-      const long o = f % omax, q = f / omax, pix = q % npt, fb = q / npt;
-      const int k = cs->cls_of_fbo[fb * omax + o];
-      if (k >= 0) units.push_back(WorkUnit{k, (int)pix, 1});
-    }
-    DevBuf<WorkUnit> du;
-    du.upload(units, c->stream);
-    launch_corr(c, cs, du.ptr, (int)units.size(), c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
-    CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  c->d_ba.resize(c->slab);
+  c->d_xop.resize(std::max(pos, 1L));
+  c->d_xop_off.upload(off, c->stream);
+  c->d_red.resize(std::max(c->nb, 256));
+  CUDA_CHECK(cudaMemcpyAsync(c->d_ba.ptr, g.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (pos) CUDA_CHECK(cudaMemcpyAsync(c->d_xop.ptr, ops.data(), pos * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  const DysonBasis B = block_op_basis(c);
+  switch (c->RP) {
+    case 32: c->launches += launch_expectation_beta<32>(c->stream, B, c->d_ba.ptr, c->d_xop.ptr, c->d_xop_off.ptr, c->d_red.ptr); break;
+    case 48: c->launches += launch_expectation_beta<48>(c->stream, B, c->d_ba.ptr, c->d_xop.ptr, c->d_xop_off.ptr, c->d_red.ptr); break;
+    default: c->launches += launch_expectation_beta<64>(c->stream, B, c->d_ba.ptr, c->d_xop.ptr, c->d_xop_off.ptr, c->d_red.ptr); break;
   }
-  std::vector<double> out(nout);
-  CUDA_CHECK(cudaMemcpyAsync(out.data(), c->d_Sig.ptr, nout * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  std::vector<double> part(c->nb);
+  CUDA_CHECK(cudaMemcpyAsync(part.data(), c->d_red.ptr, c->nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CUDA_CHECK(cudaStreamSynchronize(c->stream));
-  for (long i = 0; i < nout; ++i) {
-    g_out[2 * i] = out[i];
-    g_out[2 * i + 1] = 0.0;
-  }
+  // sum += -trace(O_b G_b(beta)) block after block (block_sparse.cpp:805-813)
+  double sum = 0.0;
+  for (int b = 0; b < c->nb; ++b)
+    if (off[b] >= 0) sum += -part[b];
+  out[0] = sum;
+  out[1] = 0.0;
+  API_END
+}
+
+int xca_compute_one_time_correlator(xca_ctx *ctx, const double *G, int n_tau, const int *tau_index, const double *tau_data, int n_0,
+                                    const int *zero_index, const double *zero_data, int m, const int *topology, const long *f_ix,
+                                    long n_fix, double *corr_out) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c->ready) throw Error(XCA_ERR_INVALID, "evaluator not set up");
+  if (n_tau < 1 || n_0 < 1) throw Error(XCA_ERR_INVALID, "compute_one_time_correlator: empty operator list");
+  set_device(c);
+  const int nb = c->nb;
+  ExtOps X;
+  X.nmu = n_tau;
+  X.nka = n_0;
+  X.mu_idx.assign(tau_index, tau_index + (size_t)n_tau * nb);
+  X.ka_idx.assign(zero_index, zero_index + (size_t)n_0 * nb);
+  // operator slabs: the ops at tau, then the ops at 0, each a (d_target x d_b) block per present column
+  std::vector<long> mo((size_t)n_tau * nb, -1), ko((size_t)n_0 * nb, -1);
+  std::vector<double> data;
+  std::ostringstream key;
+  key << "ot" << n_tau << ":" << n_0;
+  auto load = [&](int nops, const std::vector<int> &idx, const double *src, std::vector<long> &offs, const char *what) {
+    long pos = 0;
+    for (int o = 0; o < nops; ++o)
+      for (int b = 0; b < nb; ++b) {
+        const int t = idx[(size_t)o * nb + b];
+        key << "," << t;
+        if (t == -1) continue;
+        if (t < -1 || t >= nb) throw Error(XCA_ERR_INVALID, std::string(what) + ": block index out of range");
+        const long sz = (long)c->dims[t] * c->dims[b];
+        offs[(size_t)o * nb + b] = (long)data.size();
+        std::vector<double> re;
+        real_part(src + 2 * pos, sz, re, what);
+        data.insert(data.end(), re.begin(), re.end());
+        pos += sz;
+      }
+  };
+  load(n_tau, X.mu_idx, tau_data, mo, "ops_tau");
+  load(n_0, X.ka_idx, zero_data, ko, "ops_0");
+  X.key = key.str();
+  c->d_xops.upload(data, c->stream);
+  c->d_xmu_off.upload(mo, c->stream);
+  c->d_xka_off.upload(ko, c->stream);
+  X.d_ops = c->d_xops.ptr;
+  X.d_mu_off = c->d_xmu_off.ptr;
+  X.d_ka_off = c->d_xka_off.ptr;
+  correlator_host(c, G, m, topology, f_ix, n_fix, X, corr_out, "compute_one_time_correlator");
   API_END
 }
 
