@@ -56,6 +56,7 @@ def lib():
         L.ora_num_spgf_backbones.argtypes = [P, I, ip]
         L.ora_sigma.argtypes = [P, dp, I, ip, lp, LG, I, dp, lp, dp]
         L.ora_sigma_ordered.argtypes = [P, dp, I, ip, LG, I, dp, lp]
+        L.ora_sigma_list_ordered.argtypes = [P, dp, I, ip, lp, LG, I, dp]
         L.ora_items.restype = LG
         L.ora_items.argtypes = [P, dp, I, ip, LG, LG, lp, LG]
         L.ora_spgf.argtypes = [P, dp, I, ip, lp, LG, I, dp]
@@ -264,6 +265,16 @@ class Evaluator:
         out = np.empty_like(g)
         items = np.zeros(1, np.int64)
         _check(lib().ora_sigma_ordered(self._h, _dp(g), t.shape[0], _ip(t), int(unit), int(nthreads), _dp(out), _lp(items)))
+        return self.unpack(out)
+
+    def compute_self_energy_list_ordered(self, G, topology, f_ix, nthreads=0):
+        """``compute_self_energy(G, topology, f_ix_vec)`` with the additions into Sigma in list order (the
+        order of the device's ordered mode for a flat-index list); the items are evaluated in parallel."""
+        t = np.ascontiguousarray(topology, dtype=np.int32)
+        g = self.pack(G)
+        out = np.empty_like(g)
+        fix = np.ascontiguousarray(np.atleast_1d(f_ix), dtype=np.int64)
+        _check(lib().ora_sigma_list_ordered(self._h, _dp(g), t.shape[0], _ip(t), _lp(fix), len(fix), int(nthreads), _dp(out)))
         return self.unpack(out)
 
     def item_list(self, G, topology, f0=0, f1=None):

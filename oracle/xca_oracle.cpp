@@ -1136,6 +1136,56 @@ int ora_sigma_ordered(void *ev, const double *G_, int m, const int *topo, long u
   } catch (std::exception &e) { g_err = e.what(); return 1; }
 }
 
+// compute_self_energy(G, topology, f_ix_vec) with the additions into Sigma in list order (for each listed
+// flat index its items in (b_ix, p_kap) order, each block's sum from zero), the order of the device's
+// ordered mode for a flat-index list.  The items are evaluated in parallel and summed afterwards.
+int ora_sigma_list_ordered(void *ev, const double *G_, int m, const int *topo, const long *fix, long nfix, int nthreads, double *Sig_out) {
+  try {
+    auto *E = (Evaluator *)ev;
+    Backbone B0(m, topo, E->n, E->p, false);
+    const long nmax = B0.num_backbones();
+    for (long z = 0; z < nfix; ++z)
+      if (fix[z] < 0 || fix[z] >= nmax) throw std::runtime_error("DiagramEvaluator::eval_self_energy: f_ix out of range");
+    BlockG g = make_G(*E, (const cd *)G_);
+    std::vector<size_t> off(E->nb + 1, 0);
+    for (int b = 0; b < E->nb; ++b) off[b + 1] = off[b] + (size_t)E->r * E->dims[b] * E->dims[b];
+    // per listed index: its contributions (block, slab) in visit order
+    std::vector<std::vector<std::pair<int, std::vector<cd>>>> parts(nfix);
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+#pragma omp parallel num_threads(nthreads)
+    {
+      Backbone B(m, topo, E->n, E->p, false);
+      Work w;
+      alloc_work(*E, w);
+#pragma omp for schedule(dynamic, 1)
+      for (long z = 0; z < nfix; ++z) {
+        B.set_flat_index(fix[z], E->poles_beta);
+        find_paths(*E, B, g, w, [&](int b, int pk, int pm) {
+          std::vector<cd> one((size_t)E->r * E->dims[b] * E->dims[b], 0.0);
+          eval_fixed(*E, B, g, w, b, pk, pm, one);
+          parts[z].emplace_back(b, std::move(one));
+        });
+      }
+    }
+    std::vector<cd> Sig(off[E->nb], 0.0);
+    for (long z = 0; z < nfix; ++z)
+      for (auto &pr : parts[z])
+        for (size_t x = 0; x < pr.second.size(); ++x) Sig[off[pr.first] + x] += pr.second[x];
+    for (int b = 0; b < E->nb; ++b) {
+      double mx = 0;
+      for (size_t x = off[b]; x < off[b + 1]; ++x) mx = std::max(mx, std::abs(Sig[x]));
+      if (mx < 1e-16)
+        for (size_t x = off[b]; x < off[b + 1]; ++x) Sig[x] = 0;
+    }
+    std::copy(Sig.begin(), Sig.end(), (cd *)Sig_out);
+    return 0;
+  } catch (std::exception &e) { g_err = e.what(); return 1; }
+}
+
 // Valid item list of find_path_self_energy for flat indices [f0, f1): rows (f_ix, b_ix, p_kap, ind_path[0..2m-2]).
 long ora_items(void *ev, const double *G_, int m, const int *topo, long f0, long f1, long *out, long max_rows) {
   auto *E = (Evaluator *)ev;

@@ -22,6 +22,9 @@ XCA_PREC_FP64_ORDERED = 1
 XCA_ORDERED_UNIT_TUPLES = 64
 PRECISION_MODES = {"fp64": XCA_PREC_FP64, "fp64_ordered": XCA_PREC_FP64_ORDERED}
 
+# launch-shape parameters (xca_set_tuning)
+TUNING = {"unit_batches": 0, "wide_unit_tuples": 1, "wide_ctas_per_sm": 2}
+
 _lib = None
 
 D = ctypes.c_double
@@ -76,6 +79,8 @@ SIGNATURES = {
     "xca_synchronize": [P],
     "xca_kernel_launches": [P, lp],
     "xca_set_precision_mode": [P, I],
+    "xca_set_tuning": [P, I, I],
+    "xca_get_tuning": [P, I, ip],
     "xca_compute_one_time_correlator": [P, dp, I, ip, dp, I, ip, dp, I, ip, lp, L, dp],
     "xca_convolve_ppsc": [P, dp, dp, dp],
     "xca_convolve_ppsc_device": [P, P, P, P],

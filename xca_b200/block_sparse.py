@@ -288,6 +288,21 @@ class DiagramEvaluator:
             raise NotImplementedError(f"precision mode {mode!r} is not available ({sorted(_lib.PRECISION_MODES)})")
         _lib.check(_lib.lib().xca_set_precision_mode(self._ctx, _lib.PRECISION_MODES[mode]))
 
+    def set_tuning(self, **params):
+        """Launch-shape parameters of the Sigma kernels (unit_batches, wide_unit_tuples, wide_ctas_per_sm)."""
+        for k, v in params.items():
+            if k not in _lib.TUNING:
+                raise ValueError(f"unknown tuning parameter {k!r} ({sorted(_lib.TUNING)})")
+            _lib.check(_lib.lib().xca_set_tuning(self._ctx, _lib.TUNING[k], int(v)))
+
+    def get_tuning(self):
+        out = {}
+        for k, i in _lib.TUNING.items():
+            v = ctypes.c_int()
+            _lib.check(_lib.lib().xca_get_tuning(self._ctx, i, ctypes.byref(v)))
+            out[k] = v.value
+        return out
+
     # ---------------------------------------------------------------- device-resident use
     def dyson_setup(self, G0):
         """Dyson solvers of every block for the atomic propagator G0 (``DysonItPPSC(beta, itops, G0_b)`` for each

@@ -9,8 +9,8 @@ diff_G) come back to the host.
 
 TRIQS is not available here, so the local problem is given as an ``xca_b200.atom_diag.AtomDiag`` and the
 hybridization as a dense ``(r, n, n)`` array of Delta(tau) on the DLR nodes (``Delta_tau``); with
-``hyb_comp=False`` the solver fits it on the DLR poles exactly as the reference does (:171-176).
-Adapol pole compression (``hyb_comp=True``) is not available.
+``hyb_comp=False`` the solver fits it on the DLR poles exactly as the reference does (:171-176), with
+``hyb_comp=True`` it compresses it to a few poles (``xca_b200.hyb_fit``, in place of adapol, :151-169).
 """
 
 import time
@@ -20,6 +20,7 @@ import numpy as np
 from . import diag
 from .atom_diag import atomic_pseudo_particle_greens_function
 from .block_sparse import BlockOpSymQuartet, DiagramEvaluator
+from .hyb_fit import compress_hybridization
 from .models import dlr_fit_hybridization, rel2abs
 from .pycppdlr import MeshDLRImTime
 
@@ -56,11 +57,17 @@ class BlockSparseSolver:
         self.G_tau = None
         self.timings = {}
 
-    # -- hybridization (hyb_comp=False path of fit_hybridization, block_sparse_solver.py:146-185)
-    def fit_hybridization(self, compression=False):
+    # -- hybridization (fit_hybridization, block_sparse_solver.py:146-185): one pole per DLR frequency, or with
+    # ``compression`` a few real poles fitted to tolerance ``tol`` (xca_b200.hyb_fit); fit_error as the reference
+    def fit_hybridization(self, tol=None, compression=False):
         if compression:
-            raise NotImplementedError("adapol pole compression is not available; use hyb_comp=False")
-        self.hyb_poles, self.hyb_coeffs = dlr_fit_hybridization(self.rf, self.it, self.beta, self.Delta_tau)
+            if tol is None or tol <= 0:
+                raise ValueError("tol must be provided and positive when compression is enabled")
+            self.hyb_poles, self.hyb_coeffs, self.hyb_fit_error = compress_hybridization(self.rf, self.it, self.beta, self.Delta_tau, tol)
+        else:
+            self.hyb_poles, self.hyb_coeffs = dlr_fit_hybridization(self.rf, self.it, self.beta, self.Delta_tau)
+            self.hyb_fit_error = self.eps
+        self.hyb_compression = bool(compression)
 
     def init_diagram_evaluator(self):
         self.d = DiagramEvaluator.from_arrays(self.beta, self.beta * self.w_max, self.eps, self.rf, self.it, self.hyb_poles,
@@ -89,8 +96,8 @@ class BlockSparseSolver:
                 fac = (-1) ** order * sign * (-1) ** (order + 1)
                 d.compute_self_energy_device(self._buf["G"], topo, float(fac), self._buf["S"])
 
-    def solve(self, max_order, tol=1e-4, maxiter=10, mix=1.0, hyb_comp=False, normalization="classic", spgf_max_order=None,
-              verbose=None):
+    def solve(self, max_order, tol=1e-4, maxiter=10, mix=1.0, hyb_tol=None, hyb_comp=False, normalization="classic",
+              spgf_max_order=None, verbose=None):
         """BlockSparseSolver.solve (block_sparse_solver.py:240-355) with the 'classic' normalisation."""
         if normalization not in NORMALIZATIONS:
             raise NotImplementedError(f"normalization {normalization!r} is not available on the device path "
@@ -99,7 +106,9 @@ class BlockSparseSolver:
         verbose = self.verbose if verbose is None else verbose
         self.max_order = max_order
         self.spgf_max_order = spgf_max_order if spgf_max_order is not None else max_order
-        self.fit_hybridization(compression=hyb_comp and max_order > 1)
+        # compression is skipped for NCA, whose backbones use no pole representation (block_sparse_solver.py:289)
+        self.hyb_tol = hyb_tol if hyb_tol is not None else 0.1 * tol
+        self.fit_hybridization(tol=self.hyb_tol, compression=hyb_comp and max_order > 1)
         self.init_diagram_evaluator()
         d = self.d
         self._upload("G", self.G)
@@ -191,7 +200,7 @@ class BlockSparseSolver:
     # the device evaluator; h5 is not available here, so the state goes to a numpy .npz archive
     _STATE_ARRAYS = ("G", "Sigma", "G0", "Delta_tau", "hyb_poles", "hyb_coeffs", "G_tau")
     _STATE_SCALARS = ("beta", "w_max", "eps", "eta", "eta0", "n_ppsc_iter", "diff_G", "max_order", "spgf_max_order", "precision",
-                      "normalization", "verbose")
+                      "normalization", "verbose", "hyb_tol", "hyb_fit_error", "hyb_compression")
 
     def __reduce_to_dict__(self):
         out = {"atom_diag": self.ad.to_dict()}

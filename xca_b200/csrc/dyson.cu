@@ -12,9 +12,64 @@ static void check_launch(const char *what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Blocked LU and substitution of every block's system (the blocked kernels of dyson_kernel.cuh); n_max is
+// the largest system dimension r d_b and d_max the largest block dimension.
+static int launch_blocked_lu(cudaStream_t s, const DysonBasis &B, int n_max, int d_max, double *rhs, double *G, int hermitize,
+                             int *status) {
+  int launches = 0;
+  dim3 gi(64, (unsigned)B.nb);
+  lu_rhs_init_kernel<<<gi, 256, 0, s>>>(B, rhs);
+  check_launch("lu_rhs_init_kernel");
+  ++launches;
+  const int tiles = (n_max + 63) / 64;
+  for (int k0 = 0; k0 < n_max; k0 += LU_NB) {
+    lu_panel_kernel<<<B.nb, 1024, 0, s>>>(B, rhs, k0, status);
+    check_launch("lu_panel_kernel");
+    const int rest = n_max - k0 - LU_NB;
+    if (rest > 0) {
+      lu_u12_kernel<<<dim3((unsigned)((rest + 127) / 128), 1, (unsigned)B.nb), 128, 0, s>>>(B, k0);
+      check_launch("lu_u12_kernel");
+      const unsigned t = (unsigned)((rest + 63) / 64);
+      lu_trail_kernel<<<dim3(t, t, (unsigned)B.nb), 256, 0, s>>>(B, k0);
+      check_launch("lu_trail_kernel");
+      launches += 2;
+    }
+    ++launches;
+  }
+  (void)tiles;
+  const unsigned dcol = (unsigned)((d_max + 127) / 128);
+  for (int k0 = 0; k0 < n_max; k0 += LU_NB) {
+    lu_fwd_panel_kernel<<<B.nb, 128, 0, s>>>(B, rhs, k0);
+    check_launch("lu_fwd_panel_kernel");
+    const int rest = n_max - k0 - LU_NB;
+    if (rest > 0) {
+      lu_fwd_trail_kernel<<<dim3((unsigned)((rest + 1) / 2), dcol, (unsigned)B.nb), dim3(128, 2), 0, s>>>(B, rhs, k0);
+      check_launch("lu_fwd_trail_kernel");
+      ++launches;
+    }
+    ++launches;
+  }
+  const int last = ((n_max - 1) / LU_NB) * LU_NB;
+  for (int k0 = last; k0 >= 0; k0 -= LU_NB) {
+    // a block whose system is smaller than k0 starts at its own last panel: the panel kernels skip
+    // k0 >= N, so every block is processed from its bottom panel upward
+    lu_bwd_panel_kernel<<<B.nb, 128, 0, s>>>(B, rhs, k0);
+    check_launch("lu_bwd_panel_kernel");
+    if (k0 > 0) {
+      lu_bwd_trail_kernel<<<dim3((unsigned)((k0 + 1) / 2), dcol, (unsigned)B.nb), dim3(128, 2), 0, s>>>(B, rhs, k0);
+      check_launch("lu_bwd_trail_kernel");
+      ++launches;
+    }
+    ++launches;
+  }
+  lu_store_kernel<<<dim3(64, (unsigned)B.nb), 256, 0, s>>>(B, rhs, G, hermitize);
+  check_launch("lu_store_kernel");
+  return launches + 1;
+}
+
 template <int RP>
 int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const double *Sigma, double eta, int hermitize, double *rhs,
-                 double *G, int *status) {
+                 double *G, int *status, int n_max, int d_max) {
   const size_t sm = (2 * (size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
   if (cudaFuncSetAttribute(dyson_coef_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
     check_launch("dyson_coef_kernel attributes");
@@ -23,6 +78,7 @@ int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const do
   dim3 grid((unsigned)((n_conv_rows + 63) / 64), (unsigned)B.nb);
   dyson_convmat_kernel<RP><<<grid, 64, 0, s>>>(B);
   check_launch("dyson_convmat_kernel");
+  if (n_max > DYSON_BLOCKED_MIN_N) return 2 + launch_blocked_lu(s, B, n_max, d_max, rhs, G, hermitize, status);
   dyson_lu_solve_kernel<<<B.nb, 1024, 0, s>>>(B, rhs, G, hermitize, status);
   check_launch("dyson_lu_solve_kernel");
   return 3;
@@ -78,9 +134,12 @@ int launch_axpby(cudaStream_t s, double alpha, const double *x, double beta, dou
   return 1;
 }
 
-template int launch_dyson<32>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *);
-template int launch_dyson<48>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *);
-template int launch_dyson<64>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *);
+template int launch_dyson<32>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *, int,
+                               int);
+template int launch_dyson<48>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *, int,
+                               int);
+template int launch_dyson<64>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *, int,
+                               int);
 template int launch_convolve_ppsc<32>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);
 template int launch_convolve_ppsc<48>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);
 template int launch_convolve_ppsc<64>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);

@@ -463,3 +463,264 @@ __global__ void __launch_bounds__(128) expectation_beta_kernel(DysonBasis B, con
 }
 
 }  // namespace xca
+
+namespace xca {
+
+// ---------------------------------------------------------------------------------------------------------
+// Blocked LU with partial pivoting and substitution for large Dyson systems (N = r d in the thousands for
+// the five-orbital d shell).  Panels of LU_NB columns; every matrix element still receives the elimination
+// updates a_ij <- a_ij - l_ik u_kj of the unblocked getrf in ascending k, each product and difference
+// separately rounded, and every right-hand-side entry the fused multiply-adds of the substitutions in the
+// order of the CPU restatement (forward k ascending, backward k descending with the division by U_kk), so
+// the result equals the unblocked kernel's bit for bit; only the number of passes over the matrix changes.
+// Every kernel takes the Fock-space block from blockIdx.z / blockIdx.x and returns at once for blocks
+// whose system is smaller than the current panel.
+constexpr int LU_NB = 32;
+
+__device__ __forceinline__ long lu_dim(const DysonBasis &B, int b) { return (long)B.r * B.dims[b]; }
+
+// Panel factorisation of columns [k0, k0 + LU_NB) over all rows: pivot search, full-row interchange (matrix
+// and right-hand side), column scaling, rank-1 updates inside the panel.  One CTA per block.
+__global__ void __launch_bounds__(1024) lu_panel_kernel(DysonBasis B, double *__restrict__ rhs, int k0, int *__restrict__ status) {
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  __shared__ int s_piv;
+  const int b = blockIdx.x;
+  const int N = (int)lu_dim(B, b), d = B.dims[b];
+  if (k0 >= N) return;
+  const int kend = min(k0 + LU_NB, N);
+  double *A = B.mats + B.moff[b];
+  double *x = rhs + B.goff[b];
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  for (int k = k0; k < kend; ++k) {
+    double bv = -1.0;
+    int bi = N;
+    for (int i = k + tid; i < N; i += nt) argmax_combine(bv, bi, fabs(A[(long)i * N + k]), i);
+    for (int o = 16; o > 0; o >>= 1) {
+      const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+      argmax_combine(bv, bi, v2, i2);
+    }
+    if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+    __syncthreads();
+    if (warp == 0) {
+      bv = lane < (nt >> 5) ? red_v[lane] : -1.0;
+      bi = lane < (nt >> 5) ? red_i[lane] : N;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        argmax_combine(bv, bi, v2, i2);
+      }
+      if (lane == 0) s_piv = bi;
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p >= N) {  // a column of NaN: flag and leave the block
+      if (tid == 0) atomicExch(status, 1);
+      return;
+    }
+    if (p != k) {
+      for (int j = tid; j < N; j += nt) {
+        const double t = A[(long)k * N + j];
+        A[(long)k * N + j] = A[(long)p * N + j];
+        A[(long)p * N + j] = t;
+      }
+      for (int j = tid; j < d; j += nt) {
+        const double t = x[(long)k * d + j];
+        x[(long)k * d + j] = x[(long)p * d + j];
+        x[(long)p * d + j] = t;
+      }
+    }
+    __syncthreads();
+    const double piv = A[(long)k * N + k];
+    if (piv == 0.0) {
+      if (tid == 0) atomicExch(status, 1);
+      return;
+    }
+    for (int i = k + 1 + tid; i < N; i += nt) A[(long)i * N + k] = __ddiv_rn(A[(long)i * N + k], piv);
+    __syncthreads();
+    const int w = kend - k - 1;
+    if (w > 0)
+      for (long e = tid; e < (long)(N - k - 1) * w; e += nt) {
+        const int i = k + 1 + (int)(e / w), j = k + 1 + (int)(e - (e / w) * w);
+        A[(long)i * N + j] = __dsub_rn(A[(long)i * N + j], mul(A[(long)i * N + k], A[(long)k * N + j]));
+      }
+    __syncthreads();
+  }
+}
+
+// Panel rows right of the panel (U12): for every column j >= k0 + LU_NB, the panel's updates
+// a_ij -= l_ik a_kj for k0 <= k < i < k0 + LU_NB in ascending k.  One thread per column.
+__global__ void __launch_bounds__(128) lu_u12_kernel(DysonBasis B, int k0) {
+  __shared__ double L[LU_NB][LU_NB + 1];
+  const int b = blockIdx.z;
+  const int N = (int)lu_dim(B, b);
+  const int kend = min(k0 + LU_NB, N), nb = kend - k0;
+  if (kend >= N) return;
+  const double *A0 = B.mats + B.moff[b];
+  for (int e = threadIdx.x; e < LU_NB * LU_NB; e += blockDim.x) {
+    const int i = e / LU_NB, k = e - i * LU_NB;
+    L[i][k] = (i < nb && k < nb) ? A0[(long)(k0 + i) * N + k0 + k] : 0.0;
+  }
+  __syncthreads();
+  const int j = kend + blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  double *A = B.mats + B.moff[b];
+  double a[LU_NB];
+#pragma unroll
+  for (int i = 0; i < LU_NB; ++i) a[i] = i < nb ? A[(long)(k0 + i) * N + j] : 0.0;
+#pragma unroll
+  for (int k = 0; k < LU_NB; ++k)
+#pragma unroll
+    for (int i = k + 1; i < LU_NB; ++i)
+      if (i < nb) a[i] = __dsub_rn(a[i], mul(L[i][k], a[k]));
+#pragma unroll
+  for (int i = 1; i < LU_NB; ++i)
+    if (i < nb) A[(long)(k0 + i) * N + j] = a[i];
+}
+
+// Trailing update A22 -= L21 U12 for rows and columns >= k0 + LU_NB: 64 x 64 tiles, 256 threads with 4 x 4
+// entries each; every entry takes the panel's updates in ascending k, separately rounded.
+__global__ void __launch_bounds__(256) lu_trail_kernel(DysonBasis B, int k0) {
+  __shared__ double Ls[64][LU_NB + 1];
+  __shared__ double Us[LU_NB][64 + 1];
+  const int b = blockIdx.z;
+  const int N = (int)lu_dim(B, b);
+  const int kend = min(k0 + LU_NB, N), nb = kend - k0;
+  const int i0 = kend + blockIdx.y * 64, j0 = kend + blockIdx.x * 64;
+  if (i0 >= N || j0 >= N) return;
+  double *A = B.mats + B.moff[b];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < 64 * LU_NB; e += 256) {
+    const int i = e / LU_NB, k = e - i * LU_NB;
+    Ls[i][k] = (i0 + i < N && k < nb) ? A[(long)(i0 + i) * N + k0 + k] : 0.0;
+    const int kk = e / 64, jj = e - kk * 64;
+    Us[kk][jj] = (j0 + jj < N && kk < nb) ? A[(long)(k0 + kk) * N + j0 + jj] : 0.0;
+  }
+  __syncthreads();
+  const int ty = tid / 16, tx = tid - ty * 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int i = i0 + ty * 4 + a, j = j0 + tx * 4 + c;
+      acc[a][c] = (i < N && j < N) ? A[(long)i * N + j] : 0.0;
+    }
+  for (int k = 0; k < nb; ++k) {
+    double l[4], u[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) l[a] = Ls[ty * 4 + a][k];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) u[c] = Us[k][tx * 4 + c];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[a][c] = __dsub_rn(acc[a][c], mul(l[a], u[c]));
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int i = i0 + ty * 4 + a, j = j0 + tx * 4 + c;
+      if (i < N && j < N) A[(long)i * N + j] = acc[a][c];
+    }
+}
+
+// Forward substitution with the unit lower factor, panel [k0, k0 + LU_NB): in-panel rows (one thread per
+// right-hand-side column), then the rows below (64-row tiles).  x_ij <- fma(-L_ik, x_kj, x_ij), k ascending.
+__global__ void __launch_bounds__(128) lu_fwd_panel_kernel(DysonBasis B, double *__restrict__ rhs, int k0) {
+  const int b = blockIdx.x;
+  const int N = (int)lu_dim(B, b), d = B.dims[b];
+  if (k0 >= N) return;
+  const int kend = min(k0 + LU_NB, N);
+  const double *A = B.mats + B.moff[b];
+  double *x = rhs + B.goff[b];
+  for (int j = threadIdx.x; j < d; j += blockDim.x)
+    for (int k = k0; k < kend; ++k) {
+      const double xk = x[(long)k * d + j];
+      for (int i = k + 1; i < kend; ++i) x[(long)i * d + j] = fmad(-A[(long)i * N + k], xk, x[(long)i * d + j]);
+    }
+}
+
+__global__ void __launch_bounds__(256) lu_fwd_trail_kernel(DysonBasis B, double *__restrict__ rhs, int k0) {
+  __shared__ double Xs[LU_NB][129];
+  const int b = blockIdx.z;
+  const int N = (int)lu_dim(B, b), d = B.dims[b];
+  const int kend = min(k0 + LU_NB, N), nb = kend - k0;
+  const int i = kend + blockIdx.x * blockDim.y + threadIdx.y;
+  const int j = blockIdx.y * 128 + threadIdx.x;
+  if (kend >= N || blockIdx.y * 128 >= d) return;
+  const double *A = B.mats + B.moff[b];
+  double *x = rhs + B.goff[b];
+  for (int e = threadIdx.y * blockDim.x + threadIdx.x; e < LU_NB * 128; e += blockDim.x * blockDim.y) {
+    const int k = e / 128, jj = e - k * 128;
+    Xs[k][jj] = (k < nb && blockIdx.y * 128 + jj < d) ? x[(long)(k0 + k) * d + blockIdx.y * 128 + jj] : 0.0;
+  }
+  __syncthreads();
+  if (i >= N || j >= d) return;
+  double v = x[(long)i * d + j];
+  for (int k = 0; k < nb; ++k) v = fmad(-A[(long)i * N + k0 + k], Xs[k][threadIdx.x], v);
+  x[(long)i * d + j] = v;
+}
+
+// Backward substitution with the upper factor, panel [k0, k0 + LU_NB) from the bottom: in-panel rows
+// (x_kj <- x_kj / U_kk, then the rows above it in the panel), then the rows above the panel; k descending.
+__global__ void __launch_bounds__(128) lu_bwd_panel_kernel(DysonBasis B, double *__restrict__ rhs, int k0) {
+  const int b = blockIdx.x;
+  const int N = (int)lu_dim(B, b), d = B.dims[b];
+  if (k0 >= N) return;
+  const int kend = min(k0 + LU_NB, N);
+  const double *A = B.mats + B.moff[b];
+  double *x = rhs + B.goff[b];
+  for (int j = threadIdx.x; j < d; j += blockDim.x)
+    for (int k = kend - 1; k >= k0; --k) {
+      const double xk = __ddiv_rn(x[(long)k * d + j], A[(long)k * N + k]);
+      x[(long)k * d + j] = xk;
+      for (int i = k0; i < k; ++i) x[(long)i * d + j] = fmad(-A[(long)i * N + k], xk, x[(long)i * d + j]);
+    }
+}
+
+__global__ void __launch_bounds__(256) lu_bwd_trail_kernel(DysonBasis B, double *__restrict__ rhs, int k0) {
+  __shared__ double Xs[LU_NB][129];
+  const int b = blockIdx.z;
+  const int N = (int)lu_dim(B, b), d = B.dims[b];
+  if (k0 >= N || k0 == 0 || blockIdx.y * 128 >= d) return;
+  const int kend = min(k0 + LU_NB, N), nb = kend - k0;
+  const int i = blockIdx.x * blockDim.y + threadIdx.y;
+  const int j = blockIdx.y * 128 + threadIdx.x;
+  const double *A = B.mats + B.moff[b];
+  double *x = rhs + B.goff[b];
+  for (int e = threadIdx.y * blockDim.x + threadIdx.x; e < LU_NB * 128; e += blockDim.x * blockDim.y) {
+    const int k = e / 128, jj = e - k * 128;
+    Xs[k][jj] = (k < nb && blockIdx.y * 128 + jj < d) ? x[(long)(k0 + k) * d + blockIdx.y * 128 + jj] : 0.0;
+  }
+  __syncthreads();
+  if (i >= k0 || j >= d) return;
+  double v = x[(long)i * d + j];
+  for (int k = nb - 1; k >= 0; --k) v = fmad(-A[(long)i * N + k0 + k], Xs[k][threadIdx.x], v);
+  x[(long)i * d + j] = v;
+}
+
+// G_out <- x, hermitized (G(t) + G(t)^T) / 2 when asked (solve_dyson, block_sparse_solver.py:582-586).
+__global__ void lu_store_kernel(DysonBasis B, const double *__restrict__ rhs, double *__restrict__ G_out, int hermitize) {
+  const int b = blockIdx.y;
+  const int d = B.dims[b], dd = d * d;
+  const double *x = rhs + B.goff[b];
+  double *g = G_out + B.goff[b];
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < (long)B.r * dd; e += (long)gridDim.x * blockDim.x) {
+    const int t = (int)(e / dd), ij = (int)(e - (long)t * dd), i = ij / d, j = ij - i * d;
+    const double v = x[e];
+    g[e] = hermitize ? mul(0.5, add(v, x[(long)t * dd + j * d + i])) : v;
+  }
+}
+
+// Right-hand side x <- G0 for every block.
+__global__ void lu_rhs_init_kernel(DysonBasis B, double *__restrict__ rhs) {
+  const int b = blockIdx.y;
+  const long n = (long)B.r * B.dims[b] * B.dims[b];
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+    rhs[B.goff[b] + e] = B.g0[B.goff[b] + e];
+}
+
+}  // namespace xca

@@ -16,6 +16,12 @@ template <int RP>
 int launch_sigma_panel(cudaStream_t s, int nsm, const DevBasis &B, const ClassRec *classes, const WorkUnit *units, int n_units,
                        int *counter, const double *G, const SigmaOut &out);
 
+// Wide-chain Sigma kernel (sigma_wide.cuh) over n_units units with `grid` CTAs, three slabs of `slab`
+// doubles per CTA in scratch.
+template <int RP>
+int launch_sigma_wide(cudaStream_t s, int grid, const DevBasis &B, const ClassRec *classes, const WorkUnit *units, int n_units,
+                      int *counter, const double *G, const SigmaOut &out, double *scratch, long slab);
+
 // Usable panel columns of the panel kernels of rank RP.
 template <int RP>
 int panel_width();
@@ -25,9 +31,12 @@ int launch_correlator(cudaStream_t s, int grid, int warps_per_cta, const DevBasi
                       const CorrChain *chains, const CorrTerm *terms, const WorkUnit *units, int n_units, int *counter,
                       const double *G, double *g, double scale, int nmax, double *scratch, long warp_doubles);
 
+// Systems larger than this (N = r d_b) are factorised by the blocked kernels, smaller ones by one CTA each.
+constexpr int DYSON_BLOCKED_MIN_N = 512;
+
 template <int RP>
 int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const double *Sigma, double eta, int hermitize, double *rhs,
-                 double *G, int *status);
+                 double *G, int *status, int n_max, int d_max);
 
 template <int RP>
 int launch_trace_beta(cudaStream_t s, const DysonBasis &B, const double *G, double *out);

@@ -61,6 +61,7 @@ struct ClassRec {
   int npt;                 // pole tuples p^(m-1)
   int batch;               // items a CTA evaluates together as panel columns: batch * dcmax <= panel width
   int dcmax;               // panel columns of one item at the widest point of the chain
+  int wide;                // 1: dcmax exceeds the panel width, evaluated by sigma_wide_kernel
   int la[MAXM], lb[MAXM];  // line endpoints
   int ind_path[2 * MAXM - 1];
   int bdims[2 * MAXM + 1];

@@ -119,15 +119,26 @@ __device__ __forceinline__ long corr_edge_tab(const DevBasis &B, const CorrClass
   return B.tab_off[b] + sig * 2 * r * dd;
 }
 
-// Time-ordered DLR convolution of one edge for one item, in place in T (r x rows x cols), X and Y scratch.
+// Barrier of the threads that share one item: the warp (CTA = false) or the whole CTA.
+template <bool CTA>
+__device__ __forceinline__ void item_sync() {
+  if (CTA)
+    __syncthreads();
+  else
+    __syncwarp();
+}
+
+// Time-ordered DLR convolution of one edge for one item, in place in T (r x rows x cols), X and Y scratch,
+// by the `nt` threads of a warp (CTA = false, lane = thread index) or of a CTA (CTA = true).
 // LEFT: T <- conv(GK, T) with GK (d x d) = table, T (d x cols) (integrate_left_edge);
 // RIGHT: T <- conv(T, GK) with T (rows x d) (integrate_right_edge).  The table holds fc = K^-1 GK and W fc.
-template <int RP, bool LEFT>
+template <int RP, bool LEFT, bool CTA = false>
 __device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, const double *sW, const double *sBK, const int *sPerm,
-                                          const double *tb, int rows, int cols, int d, double *T, double *X, double *Y, int lane) {
+                                          const double *tb, int rows, int cols, int d, double *T, double *X, double *Y, int lane,
+                                          int nt = 32) {
   const int r = B.r, dc = rows * cols, dd = d * d;
   // (a) coefficients of T (in place) and their Hilbert transform W Tc (into X), one column per lane
-  for (int col = lane; col < dc; col += 32) {
+  for (int col = lane; col < dc; col += nt) {
     double x[RP];
 #pragma unroll
     for (int i = 0; i < RP; ++i) {
@@ -140,10 +151,10 @@ __device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, 
       if (i < r) T[i * dc + col] = x[i];
     matvec_reg<RP>(sW, x, r, X + col, dc);
   }
-  __syncwarp();
+  item_sync<CTA>();
   const double *fc = tb, *fw = tb + (long)r * dd;
   // (b) Q_l (into Y)
-  for (int idx = lane; idx < r * dc; idx += 32) {
+  for (int idx = lane; idx < r * dc; idx += nt) {
     const int l = idx / dc, rem = idx - l * dc, x = rem / cols, z = rem - x * cols;
     double a = 0.0;
     if (LEFT) {
@@ -157,17 +168,17 @@ __device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, 
     }
     Y[idx] = a;
   }
-  __syncwarp();
+  item_sync<CTA>();
   // (c) h1 = (beta K) Q (into X)
-  for (int col = lane; col < dc; col += 32) {
+  for (int col = lane; col < dc; col += nt) {
     double q[RP];
 #pragma unroll
     for (int i = 0; i < RP; ++i) q[i] = i < r ? Y[i * dc + col] : 0.0;
     matvec_reg<RP>(sBK, q, r, X + col, dc);
   }
-  __syncwarp();
+  item_sync<CTA>();
   // (d) P'_l = K(0, om_l) (f_l g_l) (into Y)
-  for (int idx = lane; idx < r * dc; idx += 32) {
+  for (int idx = lane; idx < r * dc; idx += nt) {
     const int l = idx / dc, rem = idx - l * dc, x = rem / cols, z = rem - x * cols;
     double a = 0.0;
     if (LEFT) {
@@ -179,9 +190,9 @@ __device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, 
     }
     Y[idx] = mul(B.k0[l], a);
   }
-  __syncwarp();
+  item_sync<CTA>();
   // (e) h = h1 + t_i (beta K) P' (into T)
-  for (int col = lane; col < dc; col += 32) {
+  for (int col = lane; col < dc; col += nt) {
     double q[RP];
 #pragma unroll
     for (int i = 0; i < RP; ++i) q[i] = i < r ? Y[i * dc + col] : 0.0;
@@ -204,7 +215,7 @@ __device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, 
       }
     }
   }
-  __syncwarp();
+  item_sync<CTA>();
 }
 
 // Dynamic shared memory: LU (+ reciprocal diagonal) | W | BK | RF (column-major) | perm (RP ints).

@@ -166,7 +166,8 @@ struct Topology {
 // (directions, orbital tuple, symmetry set); for a list of flat indices every (flat index, class) item is
 // its own unit and group, in list order.
 struct OrderedPlan {
-  std::vector<WorkUnit> units;
+  std::vector<WorkUnit> units;  // the panel kernel's units [0, n_panel), then the wide kernel's
+  int n_panel = 0;
   std::vector<long> slot_off;
   long slot_doubles = 0;
   std::vector<int2> groups;
@@ -188,7 +189,12 @@ struct ClassSet {
   long long n_items = 0;
   std::map<std::pair<int, int>, std::unique_ptr<ClassSet>> shards;
   std::unique_ptr<OrderedPlan> ordered;
+  // classes too wide for a panel: their units (runs of Ctx::wide_unit_tuples pole tuples) and the per-CTA slab
+  std::vector<WorkUnit> wide_units;
+  DevBuf<WorkUnit> d_wide_units;
+  long wide_slab = 0;  // r x widest state over the wide classes
 };
+
 
 struct CorrSet {
   std::vector<CorrClass> classes;
@@ -237,8 +243,10 @@ struct Ctx {
   int RP = 0;                                   // padded rank of the register-resident columns
   std::vector<double> LUp, Wp, BKp;             // RP x RP padded matrices
   std::vector<int> perm;                        // RP
-  std::vector<long> tab_off;                    // per block offset into the edge tables
+  std::vector<long> tab_off;                    // per block offset into the edge tables (all signatures)
   long nsig_alloc = 0;
+  long tab_doubles_full = 0, tab_doubles_small = 0;
+  DevBuf<long> d_tab_off_small;                 // per block offsets of the 1 + 2p signature layout (orders <= 2)
   // device copies
   DevBuf<double> d_tabs, d_k0, d_kitp, d_kitm, d_kpow, d_polesb, d_hval, d_hrefl, d_ops;
   DevBuf<int> d_dims, d_set_to_orb, d_perm, d_pinv;
@@ -257,9 +265,13 @@ struct Ctx {
   DevBuf<double> d_xops;                  // one-time correlator: uploaded operator slabs
   DevBuf<long> d_xmu_off, d_xka_off;
   std::map<std::string, std::unique_ptr<ClassSet>> noalloc_classes;  // host-only work lists of the allocation-free call
-  int unit_batches = 4;  // panel batches per work unit
+  int unit_batches = 4;      // panel batches per work unit (tunable, XCA_TUNE_UNIT_BATCHES)
+  int wide_unit_tuples = 4;  // pole tuples per work unit of the wide kernel (XCA_TUNE_WIDE_UNIT_TUPLES)
+  int wide_ctas_per_sm = 2;  // CTAs of the wide kernel per SM (XCA_TUNE_WIDE_CTAS_PER_SM)
   int precision = XCA_PREC_FP64;
   DevBuf<double> d_slots;  // ordered mode: per-unit partial sums
+  DevBuf<double> d_wide_scratch;  // wide kernel: three slabs per CTA
+  DevBuf<int> d_wide_counter;
   std::map<int, std::pair<int, std::unique_ptr<DevBuf<int2>>>> chunk_bufs;  // edge-table panel chunks per signature count
   // profiling: CUDA events around every Sigma launch (enabled on request), user events, L2 flush buffer
   bool profile = false;
@@ -281,7 +293,7 @@ struct Ctx {
     DevBasis B;
     B.r = r; B.p = p; B.n = n; B.nb = nb; B.nq = nq; B.beta = beta;
     B.LUp = d_LUp.ptr; B.perm = d_perm.ptr; B.pinv = d_pinv.ptr; B.Wp = d_Wp.ptr; B.BKp = d_BKp.ptr; B.tabs = d_tabs.ptr; B.k0 = d_k0.ptr;
-    B.tab = d_tab.ptr; B.tab_off = d_tab_off.ptr; B.nsig = nsig;
+    B.tab = d_tab.ptr; B.tab_off = nsig == nsig_alloc ? d_tab_off.ptr : d_tab_off_small.ptr; B.nsig = nsig;
     B.kitp = d_kitp.ptr; B.kitm = d_kitm.ptr; B.kpow = d_kpow.ptr; B.polesb = d_polesb.ptr;
     B.hval = d_hval.ptr; B.hrefl = d_hrefl.ptr; B.goff = d_goff.ptr; B.dims = d_dims.ptr; B.ops = d_ops.ptr;
     B.F_off = d_F_off.ptr; B.Fd_off = d_Fd_off.ptr; B.Fb_off = d_Fb_off.ptr; B.Fdb_off = d_Fdb_off.ptr;
@@ -489,10 +501,8 @@ static std::unique_ptr<ClassSet> build_classes(Ctx *c, const Topology &T, const 
             for (int i = vct0; i <= nv; ++i) w = std::max(w, bd[i] * bd[0]);
             R.dcmax = w;
             const int nc = panel_nc_host(c->RP);
-            if (R.dcmax > nc)
-              throw Error(XCA_ERR_UNSUPPORTED, "block chain too wide for the panel kernel (" + std::to_string(R.dcmax) +
-                                                   " entries per item, panel width " + std::to_string(nc) + ")");
-            R.batch = std::min(PANEL_BMAX, nc / R.dcmax);
+            R.wide = R.dcmax > nc ? 1 : 0;
+            R.batch = R.wide ? 1 : std::min(PANEL_BMAX, nc / R.dcmax);
           }
           for (int v = 0; v < nv; ++v) {
             R.vline[v] = vline[v];
@@ -506,14 +516,16 @@ static std::unique_ptr<ClassSet> build_classes(Ctx *c, const Topology &T, const 
         }
     }
   for (size_t k = 0; k < cs->classes.size(); ++k) {
-    const long usz = (long)cs->classes[k].batch * c->unit_batches;
+    const ClassRec &R = cs->classes[k];
+    const long usz = R.wide ? c->wide_unit_tuples : (long)R.batch * c->unit_batches;
     for (long s = 0; s < npt; s += usz) {
       WorkUnit u;
       u.cls = (int)k;
       u.first = (int)s;
       u.count = (int)std::min<long>(usz, npt - s);
-      cs->units.push_back(u);
+      (R.wide ? cs->wide_units : cs->units).push_back(u);
     }
+    if (R.wide) cs->wide_slab = std::max(cs->wide_slab, (long)c->r * R.dcmax);
   }
   cs->n_items = (long long)cs->classes.size() * npt;
   return cs;
@@ -526,6 +538,7 @@ static ClassSet *get_classes(Ctx *c, const Topology &T, const std::vector<int> &
   auto cs = build_classes(c, T, zero);
   cs->d_classes.upload(cs->classes, c->stream);
   cs->d_units.upload(cs->units, c->stream);
+  cs->d_wide_units.upload(cs->wide_units, c->stream);
   ClassSet *ret = cs.get();
   c->class_cache[key] = std::move(cs);
   return ret;
@@ -543,6 +556,15 @@ static void launch_tables(Ctx *c, const double *G_dev, int nsig, const int2 *d_c
 // Edge tables of the current G for every signature an order-m topology can use.
 static int prepare_tables(Ctx *c, const double *G_dev, int m) {
   const int nsig = (m >= 3) ? (int)c->nsig_alloc : 1 + 2 * c->p;
+  const long need = (m >= 3) ? c->tab_doubles_full : c->tab_doubles_small;
+  if ((size_t)need > c->d_tab.n) {
+    size_t free_b = 0, total_b = 0;
+    CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    if ((double)need * 8.0 > 0.85 * (double)(free_b + c->d_tab.n * 8))
+      throw Error(XCA_ERR_UNSUPPORTED, "edge tables of order " + std::to_string(m) + " need " + std::to_string(need * 8) +
+                                           " bytes of device memory, more than is free");
+    c->d_tab.resize(need);
+  }
   auto it = c->chunk_bufs.find(nsig);
   if (it == c->chunk_bufs.end()) {
     const auto ch = table_chunks(c, nsig);
@@ -586,12 +608,21 @@ static std::vector<int> zero_flags_device(Ctx *c, const double *G_dev) {
 }
 
 // Ordered-mode plan of a unit list: slot offsets and per-block groups.  `group_of_unit[u]` numbers the
-// group of unit u; units of one group must be consecutive.
-static std::unique_ptr<OrderedPlan> make_plan(const Ctx *c, const std::vector<ClassRec> &classes, std::vector<WorkUnit> units,
+// group of unit u (groups are listed in increasing number within a block); the units of a group belong to
+// one class.  The panel kernel's units are placed first, then the wide kernel's.
+static std::unique_ptr<OrderedPlan> make_plan(const Ctx *c, const std::vector<ClassRec> &classes, const std::vector<WorkUnit> &units,
                                               const std::vector<int> &group_of_unit) {
   auto P = std::make_unique<OrderedPlan>();
-  P->units = std::move(units);
-  const size_t nu = P->units.size();
+  const size_t nu = units.size();
+  std::vector<int> grp;
+  for (int pass = 0; pass < 2; ++pass)
+    for (size_t u = 0; u < nu; ++u)
+      if (classes[units[u].cls].wide == pass) {
+        P->units.push_back(units[u]);
+        grp.push_back(group_of_unit[u]);
+      }
+  P->n_panel = 0;
+  for (const WorkUnit &w : P->units) P->n_panel += classes[w.cls].wide ? 0 : 1;
   P->slot_off.resize(nu);
   long off = 0;
   for (size_t u = 0; u < nu; ++u) {
@@ -600,17 +631,20 @@ static std::unique_ptr<OrderedPlan> make_plan(const Ctx *c, const std::vector<Cl
     off += (long)c->r * R.bdims[2 * R.m] * R.bdims[0];
   }
   P->slot_doubles = off;
-  std::vector<std::vector<int2>> per_block(c->nb);
+  // groups: consecutive units of equal group number, then per block in increasing group number
+  std::vector<std::vector<std::pair<int, int2>>> per_block(c->nb);
   for (size_t u = 0; u < nu;) {
     size_t v = u + 1;
-    while (v < nu && group_of_unit[v] == group_of_unit[u]) ++v;
-    per_block[classes[P->units[u].cls].b_out].push_back(make_int2((int)u, (int)v));
+    while (v < nu && grp[v] == grp[u]) ++v;
+    per_block[classes[P->units[u].cls].b_out].push_back({grp[u], make_int2((int)u, (int)v)});
     u = v;
   }
   P->blk_group0.assign(c->nb + 1, 0);
   for (int b = 0; b < c->nb; ++b) {
-    P->blk_group0[b + 1] = P->blk_group0[b] + (int)per_block[b].size();
-    P->groups.insert(P->groups.end(), per_block[b].begin(), per_block[b].end());
+    auto &lst = per_block[b];
+    std::stable_sort(lst.begin(), lst.end(), [](const std::pair<int, int2> &a, const std::pair<int, int2> &x) { return a.first < x.first; });
+    P->blk_group0[b + 1] = P->blk_group0[b] + (int)lst.size();
+    for (const auto &g : lst) P->groups.push_back(g.second);
     P->max_block_elems = std::max(P->max_block_elems, c->r * c->dims[b] * c->dims[b]);
   }
   P->d_units.upload(P->units, c->stream);
@@ -632,7 +666,7 @@ static OrderedPlan *ordered_plan(Ctx *c, ClassSet *cs) {
       grp.push_back((int)k);
     }
   }
-  cs->ordered = make_plan(c, cs->classes, std::move(units), grp);
+  cs->ordered = make_plan(c, cs->classes, units, grp);
   return cs->ordered.get();
 }
 
@@ -655,18 +689,44 @@ __global__ void sigma_ordered_reduce_kernel(const double *__restrict__ slots, co
   *dst = __dadd_rn(*dst, __dmul_rn(scale, S));
 }
 
+// The wide kernel over n_units units (per-CTA slabs of `slab` doubles, three each).
+static void launch_wide_units(Ctx *c, const DevBasis &B, const ClassRec *d_classes, const WorkUnit *d_units, int n_units, long slab,
+                              const double *G_dev, const SigmaOut &out) {
+  if (n_units == 0) return;
+  const int grid = std::max(1, std::min(c->wide_ctas_per_sm * c->nsm, n_units));
+  c->d_wide_scratch.resize((size_t)grid * 3 * std::max(slab, 1L));
+  c->d_wide_counter.resize(1);
+  switch (c->RP) {
+    case 32: c->launches += launch_sigma_wide<32>(c->stream, grid, B, d_classes, d_units, n_units, c->d_wide_counter.ptr, G_dev, out, c->d_wide_scratch.ptr, slab); break;
+    case 48: c->launches += launch_sigma_wide<48>(c->stream, grid, B, d_classes, d_units, n_units, c->d_wide_counter.ptr, G_dev, out, c->d_wide_scratch.ptr, slab); break;
+    default: c->launches += launch_sigma_wide<64>(c->stream, grid, B, d_classes, d_units, n_units, c->d_wide_counter.ptr, G_dev, out, c->d_wide_scratch.ptr, slab); break;
+  }
+}
+
+static long plan_wide_slab(const Ctx *c, const std::vector<ClassRec> &classes, const OrderedPlan *P) {
+  long slab = 0;
+  for (size_t u = P->n_panel; u < P->units.size(); ++u) slab = std::max(slab, (long)c->r * classes[P->units[u].cls].dcmax);
+  return slab;
+}
+
 static void launch_sigma_plan(Ctx *c, const std::vector<ClassRec> &classes, const ClassRec *d_classes, OrderedPlan *P,
                               const double *G_dev, double *Sig_dev, double scale, int nsig) {
   if (P->units.empty()) return;
-  (void)classes;
   c->d_slots.resize(std::max<long>(P->slot_doubles, 1));
   SigmaOut o;
   o.Sigma = nullptr;
   o.scale = 1.0;
   o.slots = c->d_slots.ptr;
   o.slot_off = P->d_slot_off.ptr;
+  const DevBasis B = c->basis(nsig);
   c->d_counter.resize(1);
-  launch_sigma_units(c, c->basis(nsig), d_classes, P->d_units.ptr, (int)P->units.size(), c->d_counter.ptr, G_dev, o);
+  if (P->n_panel > 0) launch_sigma_units(c, B, d_classes, P->d_units.ptr, P->n_panel, c->d_counter.ptr, G_dev, o);
+  const int n_wide = (int)P->units.size() - P->n_panel;
+  if (n_wide > 0) {
+    SigmaOut ow = o;
+    ow.slot_off = P->d_slot_off.ptr + P->n_panel;
+    launch_wide_units(c, B, d_classes, P->d_units.ptr + P->n_panel, n_wide, plan_wide_slab(c, classes, P), G_dev, ow);
+  }
   dim3 grid((unsigned)((P->max_block_elems + 127) / 128), (unsigned)c->nb);
   sigma_ordered_reduce_kernel<<<grid, 128, 0, c->stream>>>(c->d_slots.ptr, P->d_slot_off.ptr, P->d_groups.ptr, P->d_blk_group0.ptr,
                                                            c->d_goff.ptr, c->d_dims.ptr, c->r, scale, Sig_dev);
@@ -675,7 +735,7 @@ static void launch_sigma_plan(Ctx *c, const std::vector<ClassRec> &classes, cons
 }
 
 static void launch_sigma(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_dev, double scale, int nsig) {
-  if (cs->units.empty()) return;
+  if (cs->units.empty() && cs->wide_units.empty()) return;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (c->profile) {
     CUDA_CHECK(cudaEventCreate(&e0));
@@ -686,8 +746,11 @@ static void launch_sigma(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_
     launch_sigma_plan(c, cs->classes, cs->d_classes.ptr, ordered_plan(c, cs), G_dev, Sig_dev, scale, nsig);
   } else {
     c->d_counter.resize(1);
-    launch_sigma_units(c, c->basis(nsig), cs->d_classes.ptr, cs->d_units.ptr, (int)cs->units.size(), c->d_counter.ptr, G_dev,
-                       atomic_out(Sig_dev, scale));
+    if (!cs->units.empty())
+      launch_sigma_units(c, c->basis(nsig), cs->d_classes.ptr, cs->d_units.ptr, (int)cs->units.size(), c->d_counter.ptr, G_dev,
+                         atomic_out(Sig_dev, scale));
+    launch_wide_units(c, c->basis(nsig), cs->d_classes.ptr, cs->d_wide_units.ptr, (int)cs->wide_units.size(), cs->wide_slab, G_dev,
+                      atomic_out(Sig_dev, scale));
   }
   if (c->profile) {
     CUDA_CHECK(cudaEventRecord(e1, c->stream));
@@ -934,10 +997,11 @@ static void require_dyson(const Ctx *c) {
 static void launch_dyson(Ctx *c, const double *Sig_dev, double eta, int hermitize, double *G_dev) {
   CUDA_CHECK(cudaMemsetAsync(c->d_status.ptr, 0, sizeof(int), c->stream));
   const DysonBasis B = dyson_basis(c);
+  const int n_max = c->r * c->nmax, d_max = c->nmax;
   switch (c->RP) {
-    case 32: c->launches += launch_dyson<32>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr); break;
-    case 48: c->launches += launch_dyson<48>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr); break;
-    default: c->launches += launch_dyson<64>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr); break;
+    case 32: c->launches += launch_dyson<32>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max); break;
+    case 48: c->launches += launch_dyson<48>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max); break;
+    default: c->launches += launch_dyson<64>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max); break;
   }
 }
 
@@ -1276,19 +1340,24 @@ int xca_evaluator_setup(xca_ctx *ctx, double beta, double lambda, double eps, in
         for (long j = 0; j < nc; ++j) c->hrefl[(size_t)i * nc + j] = std::fma(k, cfs[(size_t)l * nc + j], c->hrefl[(size_t)i * nc + j]);
       }
   }
-  // edge tables: per block, 1 + 2p + 4p^2 signatures of [fc | W fc] (r d^2 each)
+  // edge tables: per block, 1 + 2p (orders <= 2) or 1 + 2p + 4p^2 (order 3) signatures of [fc | W fc]
+  // (r d^2 each), allocated on first use by prepare_tables
   c->nsig_alloc = 1 + 2L * p + 4L * p * p;
   c->tab_off.assign(n_blocks, 0);
-  long toff = 0;
+  std::vector<long> small_off(n_blocks, 0);
+  long toff = 0, soff = 0;
   for (int b = 0; b < n_blocks; ++b) {
     c->tab_off[b] = toff;
+    small_off[b] = soff;
     toff += c->nsig_alloc * 2L * r * block_dims[b] * block_dims[b];
+    soff += (1 + 2L * p) * 2L * r * block_dims[b] * block_dims[b];
   }
-  if ((double)toff * 8.0 > 24e9) throw Error(XCA_ERR_UNSUPPORTED, "edge tables would exceed 24 GB");
-  c->d_tab.resize(toff);
+  c->tab_doubles_full = toff;
+  c->tab_doubles_small = soff;
   // upload
   cudaStream_t s = c->stream;
   c->d_tab_off.upload(c->tab_off, s);
+  c->d_tab_off_small.upload(small_off, s);
   c->d_kitp.upload(c->kitp, s); c->d_kitm.upload(c->kitm, s);
   c->d_kpow.upload(c->kpow, s); c->d_polesb.upload(c->polesb, s);
   c->d_hval.upload(c->hval, s); c->d_hrefl.upload(c->hrefl, s); c->d_ops.upload(c->ops, s);
@@ -1382,8 +1451,11 @@ int xca_compute_self_energy_device_shard(xca_ctx *ctx, const double *G_dev, int 
       auto sub = std::make_unique<ClassSet>();
       sub->classes = cs->classes;
       for (size_t u = shard; u < cs->units.size(); u += n_shards) sub->units.push_back(cs->units[u]);
+      for (size_t u = shard; u < cs->wide_units.size(); u += n_shards) sub->wide_units.push_back(cs->wide_units[u]);
+      sub->wide_slab = cs->wide_slab;
       sub->d_classes.upload(sub->classes, c->stream);
       sub->d_units.upload(sub->units, c->stream);
+      sub->d_wide_units.upload(sub->wide_units, c->stream);
       it = cs->shards.emplace(key, std::move(sub)).first;
     }
     launch_sigma(c, it->second.get(), G_dev, Sigma_dev, scale, nsig);
@@ -1738,9 +1810,14 @@ int xca_compute_self_energy(xca_ctx *ctx, const double *G, int m, const int *top
     } else if (!units.empty()) {
       ClassSet tmp;
       tmp.classes = cs->classes;
-      tmp.units = units;
+      for (const WorkUnit &w : units) {
+        const ClassRec &R = cs->classes[w.cls];
+        (R.wide ? tmp.wide_units : tmp.units).push_back(w);
+        if (R.wide) tmp.wide_slab = std::max(tmp.wide_slab, (long)c->r * R.dcmax);
+      }
       tmp.d_classes.upload(tmp.classes, c->stream);
       tmp.d_units.upload(tmp.units, c->stream);
+      tmp.d_wide_units.upload(tmp.wide_units, c->stream);
       launch_sigma(c, &tmp, c->d_G.ptr, c->d_Sig.ptr, 1.0, nsig);
       CUDA_CHECK(cudaStreamSynchronize(c->stream));
     }
@@ -2029,6 +2106,40 @@ int xca_set_precision_mode(xca_ctx *ctx, int mode) {
   API_END
 }
 
+int xca_set_tuning(xca_ctx *ctx, int param, int value) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  int *slot = nullptr;
+  int lo = 1, hi = 1;
+  switch (param) {
+    case XCA_TUNE_UNIT_BATCHES: slot = &c->unit_batches; hi = 64; break;
+    case XCA_TUNE_WIDE_UNIT_TUPLES: slot = &c->wide_unit_tuples; hi = 1024; break;
+    case XCA_TUNE_WIDE_CTAS_PER_SM: slot = &c->wide_ctas_per_sm; hi = 8; break;
+    default: throw Error(XCA_ERR_INVALID, "unknown tuning parameter " + std::to_string(param));
+  }
+  if (value < lo || value > hi)
+    throw Error(XCA_ERR_INVALID, "tuning value " + std::to_string(value) + " out of range [" + std::to_string(lo) + ", " +
+                                     std::to_string(hi) + "]");
+  if (*slot != value) {
+    *slot = value;
+    c->class_cache.clear();  // work lists are cut with these sizes
+    c->noalloc_classes.clear();
+  }
+  API_END
+}
+
+int xca_get_tuning(xca_ctx *ctx, int param, int *value) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  switch (param) {
+    case XCA_TUNE_UNIT_BATCHES: *value = c->unit_batches; break;
+    case XCA_TUNE_WIDE_UNIT_TUPLES: *value = c->wide_unit_tuples; break;
+    case XCA_TUNE_WIDE_CTAS_PER_SM: *value = c->wide_ctas_per_sm; break;
+    default: throw Error(XCA_ERR_INVALID, "unknown tuning parameter " + std::to_string(param));
+  }
+  API_END
+}
+
 int xca_get_precision_mode(xca_ctx *ctx, int *mode) {
   API_BEGIN
   *mode = reinterpret_cast<Ctx *>(ctx)->precision;
@@ -2081,6 +2192,9 @@ int xca_compute_self_energy_device_noalloc(xca_ctx *ctx, const double *G_dev, in
   auto itc = c->noalloc_classes.find(key);
   if (itc == c->noalloc_classes.end()) itc = c->noalloc_classes.emplace(key, build_classes(c, T, zero)).first;
   const ClassSet *cs = itc->second.get();
+  if (!cs->wide_units.empty())
+    throw Error(XCA_ERR_UNSUPPORTED, "xca_compute_self_energy_device_noalloc: block chains wider than the panel kernel's panel are "
+                                     "not supported; use xca_compute_self_energy_device");
   const size_t off_units = off_classes + align256(cs->classes.size() * sizeof(ClassRec));
   noalloc_fits(off_units + cs->units.size() * sizeof(WorkUnit), "the edge tables and work list of this topology");
   // contents: everything is rewritten before use except the unit counter, which must start at zero

@@ -218,3 +218,94 @@ def seeded_G(model, seed=0):
             c[l] = A @ A.T
         G.append(np.einsum("il,lab->iab", K, c).astype(np.complex128))
     return G
+
+
+def wigner_3j(j1, j2, j3, m1, m2, m3):
+    """Wigner 3j symbol of integer arguments (Racah's formula)."""
+    from math import factorial, sqrt
+    if m1 + m2 + m3 != 0 or abs(m1) > j1 or abs(m2) > j2 or abs(m3) > j3:
+        return 0.0
+    if j3 < abs(j1 - j2) or j3 > j1 + j2:
+        return 0.0
+    f = factorial
+    tri = f(j1 + j2 - j3) * f(j1 - j2 + j3) * f(-j1 + j2 + j3) / f(j1 + j2 + j3 + 1)
+    pre = sqrt(tri * f(j1 + m1) * f(j1 - m1) * f(j2 + m2) * f(j2 - m2) * f(j3 + m3) * f(j3 - m3))
+    s = 0.0
+    for t in range(0, j1 + j2 + j3 + 1):
+        den = [t, j3 - j2 + t + m1, j3 - j1 + t - m2, j1 + j2 - j3 - t, j1 - t - m1, j2 - t + m2]
+        if min(den) < 0:
+            continue
+        s += (-1) ** t / np.prod([float(f(x)) for x in den])
+    return (-1) ** (j1 - j2 - m3) * pre * s
+
+
+def slater_u_matrix(l, radial_integrals):
+    """Slater-Condon interaction U[m1, m2, m3, m4] in the spherical-harmonic basis (m = -l..l):
+    sum_k F^k (2l+1)^2 (l k l; 0 0 0)^2 sum_q (-1)^(m1+q+m2) (l k l; -m1 q m3) (l k l; -m2 -q m4), k = 0, 2, .., 2l."""
+    n = 2 * l + 1
+    U = np.zeros((n, n, n, n))
+    ms = range(-l, l + 1)
+    for ik, Fk in enumerate(radial_integrals):
+        k = 2 * ik
+        w0 = (2 * l + 1) ** 2 * wigner_3j(l, k, l, 0, 0, 0) ** 2
+        if w0 == 0.0:
+            continue
+        for a1, m1 in enumerate(ms):
+            for a2, m2 in enumerate(ms):
+                for a3, m3 in enumerate(ms):
+                    for a4, m4 in enumerate(ms):
+                        s = 0.0
+                        for q in range(-k, k + 1):
+                            s += (-1) ** (m1 + q + m2) * wigner_3j(l, k, l, -m1, q, m3) * wigner_3j(l, k, l, -m2, -q, m4)
+                        U[a1, a2, a3, a4] += Fk * w0 * s
+    return U
+
+
+def slater_hamiltonian(n_orb, U, mu):
+    """H = 1/2 sum_{s1 s2} sum U[a1, a2, a3, a4] c^dag_{s1 a1} c^dag_{s2 a2} c_{s2 a4} c_{s1 a3} - mu N as a dense
+    Fock-space matrix (orbital index s * n_orb + a), built by applying the operators to every basis state."""
+    n = 2 * n_orb
+    dim = 1 << n
+    states = np.arange(dim, dtype=np.int64)
+
+    def apply(k, dag, st, sign):
+        bit = np.int64(1) << k
+        occ = (st & bit) != 0
+        ok = ~occ if dag else occ
+        below = st & (bit - 1)
+        par = np.array([bin(int(x)).count("1") & 1 for x in below]) if len(below) else np.zeros(0, int)
+        sign = np.where(ok, sign * np.where(par == 1, -1.0, 1.0), 0.0)
+        return st ^ bit, sign
+
+    H = np.zeros((dim, dim))
+    nz = np.argwhere(np.abs(U) > 1e-14)
+    for s1 in range(2):
+        for s2 in range(2):
+            for a1, a2, a3, a4 in nz:
+                st, sg = states, np.ones(dim)
+                st, sg = apply(s1 * n_orb + a3, False, st, sg)
+                st, sg = apply(s2 * n_orb + a4, False, st, sg)
+                st, sg = apply(s2 * n_orb + a2, True, st, sg)
+                st, sg = apply(s1 * n_orb + a1, True, st, sg)
+                keep = sg != 0.0
+                np.add.at(H, (st[keep], states[keep]), 0.5 * U[a1, a2, a3, a4] * sg[keep])
+    H -= mu * np.diag([bin(s).count("1") for s in range(dim)]).astype(float)
+    return H
+
+
+def dshell_5orb(rf, it, beta=20.0, lam=200.0, eps=1e-8, F0=4.0, J=0.7, F4_over_F2=0.625, n_min=4, n_max=6):
+    """Five-orbital d shell with the Slater-Condon interaction (F0, and F2, F4 with F2 + F4 = 14 J and F4 / F2 =
+    0.625), mu at half filling mu = (45 F0 - 70/49 F2 - 630/441 F4) / 10
+    (benchmarks/slater_condon/slater_condon_interaction.py:29), restricted to N = 4..6 (672 states, 16 (N_up, N_dn)
+    blocks up to 100 x 100), diagonal Bethe hybridization t = 1."""
+    F2 = 14.0 * J / (1.0 + F4_over_F2)
+    F4 = F4_over_F2 * F2
+    mu = (45 * F0 - 70 / 49 * F2 - 630 / 441 * F4) / 10.0
+    U = slater_u_matrix(2, [F0, F2, F4])
+    H = slater_hamiltonian(5, U, mu)
+    ad = AtomDiag(H, 10, quantum_numbers=spin_qn(5), restrict=lambda s: n_min <= bin(s).count("1") <= n_max)
+    d = bethe_delta(beta, it)
+    delta = np.zeros((len(it), 10, 10), np.complex128)
+    for i in range(10):
+        delta[:, i, i] = d
+    return _finish("dshell_5orb", beta, lam, eps, 10, ad, rf, it, delta_vals=delta, extra={"mu": mu, "F": (F0, F2, F4)})
