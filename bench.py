@@ -42,6 +42,9 @@ def parse():
     ap.add_argument("--serving", action="store_true",
                     help="instead of the Sigma metric: a Poisson stream of whole self-consistent solves through the solve server")
     ap.add_argument("--serving-requests", type=int, default=64)
+    ap.add_argument("--no-serving", action="store_true", help="skip the served-solves measurement of the default line")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--no-variants", action="store_true", help="skip the compressed-hybridization variant")
     return ap.parse_args()
 
 
@@ -204,7 +207,47 @@ def run_serving(args):
            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
            "mean_iterations": float(np.mean([r.n_iter for r in res])),
            "converged": int(sum(r.diff_G < 1e-8 for r in res)), "wall_s": t1 - t0}
-    print(json.dumps(out), flush=True)
+    return out
+
+
+def compressed_variant(m, G, device):
+    """The same evaluation with the Bethe hybridization compressed to a few poles inside the band
+    (fit_hybridization(compression=True), xca_b200.hyb_fit, tolerance 1e-10) in place of one pole per DLR
+    frequency: evals/s and the change of Sigma (the DLR-pole evaluation amplifies input rounding, see the
+    conditioning test)."""
+    import torch
+    from xca_b200 import hyb_fit
+    from xca_b200.block_sparse import BlockOpSymQuartet, DiagramEvaluator
+    from xca_b200.distributed import self_energy_sharded
+    dv = m.extra.get("delta_diag")
+    if dv is None:
+        from xca_b200 import models
+        dv = models.bethe_delta(m.beta, m.it)
+    delta = np.zeros((m.r, m.n, m.n))
+    for i in range(m.n):
+        delta[:, i, i] = dv
+    poles, coeffs, err = hyb_fit.compress_hybridization(m.rf, m.it, m.beta, delta, 1e-10)
+    Fq = BlockOpSymQuartet(m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks, m.dims)
+    res = {}
+    for name, (p, c) in (("dlr", (m.hyb_poles, m.hyb_coeffs)), ("compressed", (poles, coeffs))):
+        ev = DiagramEvaluator.from_arrays(m.beta, m.lam, m.eps, m.rf, m.it, p, c, Fq, device=device)
+        dev = torch.device("cuda", device)
+        G_t = torch.tensor(np.concatenate([g.real.ravel() for g in G]), dtype=torch.float64, device=dev)
+        S_t = torch.zeros(ev.slab, dtype=torch.float64, device=dev)
+        terms = topologies()
+        for _ in range(2):
+            self_energy_sharded(ev, G_t.data_ptr(), S_t.data_ptr(), terms, 0, 1)
+        ms = []
+        for _ in range(3):
+            ev.flush_l2(256 << 20)
+            ev.event_record(0)
+            self_energy_sharded(ev, G_t.data_ptr(), S_t.data_ptr(), terms, 0, 1)
+            ev.event_record(1)
+            ms.append(ev.event_elapsed(0, 1))
+        res[name] = (float(np.median(ms)), S_t.cpu().numpy())
+    diff = float(np.max(np.abs(res["compressed"][1] - res["dlr"][1])) / np.max(np.abs(res["dlr"][1])))
+    return {"value": 1000.0 / res["compressed"][0], "unit": UNIT, "poles": int(len(poles)), "fit_error": float(err),
+            "sigma_rel_change_vs_dlr_poles": diff, "ms_per_step": res["compressed"][0]}
 
 
 def run_reference(args, rank):
@@ -246,7 +289,7 @@ def main():
         return
     if args.serving:
         if rank == 0:
-            run_serving(args)
+            print(json.dumps(run_serving(args)), flush=True)
         return
     import torch
     dist = None
@@ -275,6 +318,14 @@ def main():
     def step():
         self_energy_sharded(ev, G_t.data_ptr(), S_t.data_ptr(), topos, rank, world, allreduce if world > 1 else None)
 
+    tuning = None
+    if world == 1 and not args.no_tune:
+        # launch shapes of the panel kernel for this workload (xca_b200.autotune), before the warm-up steps
+        from xca_b200 import autotune
+        setting, table = autotune.tune_sigma(ev, G_t.data_ptr(), S_t.data_ptr(), [(t, f) for _, t, f in topos], reps=1,
+                                             params=["unit_batches"])
+        tuning = {"setting": setting, "sweep_ms": [[n, v, round(ms, 3)] for n, v, ms in table[1:]],
+                  "default_ms": round(table[0][2], 3)}
     for _ in range(args.warmup):
         step()
     ev.synchronize()
@@ -339,6 +390,12 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_object(args.cpu_seconds)
+    variants = None
+    if rank == 0 and world == 1 and not args.no_variants:
+        variants = {"compressed_hybridization": compressed_variant(m, G, local)}
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        serving = run_serving(args)
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": t_step, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
@@ -352,7 +409,8 @@ def main():
                                            "(xca_fp64_mma_probe) throughputs measured on this GPU",
                             "peak_fp64_fma": peak_fma, "peak_fp64_mma": peak_mma,
                             "kernel_ms_per_step": sigma_ms / max(args.steps, 1), "launches_per_step": sigma_launches / max(args.steps, 1)},
-               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
+               "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+               "tuning": tuning, "variants": variants, "serving": serving}
         print(json.dumps(out), flush=True)
     if dist is not None:
         dist.barrier()

@@ -44,7 +44,7 @@ def test_result_same_alone_and_in_mix():
 
 def test_memory_budget_refuses_oversized_request():
     req = synthetic_request("anderson", 10.0, 2.0, 1)
-    need = footprint_bytes(req.atom_diag, req.delta_tau.shape[0], req.delta_tau.shape[0])
+    need = footprint_bytes(req.atom_diag, req.delta_tau.shape[0], req.delta_tau.shape[0], req.max_order)
     srv = SolveServer(max_concurrent=2, hbm_budget=need - 1)
     fut = srv.submit(req)
     with pytest.raises(MemoryError):

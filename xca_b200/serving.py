@@ -53,11 +53,12 @@ class SolveResult:
         return self.t_done - self.t_submit
 
 
-def footprint_bytes(atom_diag, r, n_poles):
+def footprint_bytes(atom_diag, r, n_poles, max_order=3):
     """Device memory of one solve: G, Σ and Dyson slabs, edge tables, Dyson system matrices, operators."""
     dims = np.asarray(atom_diag.get_subspace_dims(), dtype=np.int64)
     slab = int(r * np.sum(dims ** 2))
-    nsig = 1 + 2 * n_poles + 4 * n_poles * n_poles  # the evaluator sizes its edge tables for order 3
+    # edge tables of the orders the solve evaluates (1 + 2p signatures, 1 + 2p + 4p^2 for third order)
+    nsig = 1 + 2 * n_poles + (4 * n_poles * n_poles if max_order >= 3 else 0)
     tables = nsig * 2 * slab
     mats = int(np.sum((r * dims) ** 2))
     n = atom_diag.n
@@ -124,7 +125,7 @@ class SolveServer:
     @staticmethod
     def _need(req):
         r = req.delta_tau.shape[0]
-        return footprint_bytes(req.atom_diag, r, r)
+        return footprint_bytes(req.atom_diag, r, r, req.max_order)
 
     def _run(self, req, fut, t_sub, need):
         t_start = time.perf_counter()
