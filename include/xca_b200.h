@@ -146,11 +146,14 @@ int xca_compute_self_energy_device_shard(xca_ctx *ctx, const double *G_dev, int 
  * tables, work list, block norms, unit counter) lives in one fixed 64 MiB array compiled into the
  * library, which every device that loads the library holds until the process exits.  The call itself
  * makes no cudaMalloc/cudaFree; the evaluator's set-up (xca_evaluator_setup) still allocates its tables
- * once beforehand.  Sizes whose scratch exceeds 64 MiB are rejected with XCA_ERR_INVALID before any
- * launch (for example third-order topologies on large bases: the edge tables grow as p^2).  The first
- * call on a device looks up the array's device address (once per device, with that device current);
- * make that first call before any stream capture.  All calls on a device share the array: calls that
- * overlap on the GPU (other contexts or threads on the same device) race and must be serialised. */
+ * once beforehand.  Sizes whose scratch exceeds 64 MiB are rejected with XCA_ERR_INVALID (for example
+ * third-order topologies on large bases: the edge tables grow as p^2): the edge tables' size is checked
+ * before any launch, the work list's after the block-norm kernel, which has by then written the block
+ * norms into the array.  Block chains wider than the panel kernel's panel give XCA_ERR_UNSUPPORTED.  The
+ * call reads the block norms back, so it waits for the context's stream.  The first call on a device
+ * looks up the array's device address (once per device, with that device current); make that first call
+ * before any stream capture.  All calls on a device share the array: calls that overlap on the GPU (other
+ * contexts or threads on the same device) race and must be serialised. */
 int xca_compute_self_energy_device_noalloc(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
                                            double *Sigma_dev);
 
@@ -266,6 +269,11 @@ int xca_get_precision_mode(xca_ctx *ctx, int *mode);
 #define XCA_TUNE_WIDE_CTAS_PER_SM 2
 int xca_set_tuning(xca_ctx *ctx, int param, int value);
 int xca_get_tuning(xca_ctx *ctx, int param, int *value);
+
+/* Number of device allocations (cudaMalloc) the library's own buffers have made in this process since it was
+ * loaded, over every context (no counterpart in the reference; lets a caller check that a call allocated
+ * nothing). */
+int xca_device_allocations(long *out);
 
 /* Number of kernels this library launched on the context since creation. */
 int xca_kernel_launches(xca_ctx *ctx, long *out);

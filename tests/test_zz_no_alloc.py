@@ -46,6 +46,12 @@ def _evaluator(beta, lam, eps):
     return m, DiagramEvaluator.from_arrays(beta, lam, eps, rf, it, m.hyb_poles, m.hyb_coeffs, Fq)
 
 
+def _allocations():
+    out = ctypes.c_long()
+    _lib.check(_lib.lib().xca_device_allocations(ctypes.byref(out)))
+    return out.value
+
+
 def _run(ev, fn, G_dev, S_dev, topo, scale):
     t = np.ascontiguousarray(np.asarray(topo, np.int32).reshape(-1, 2))
     ev.zero_device(S_dev, ev.slab)
@@ -63,7 +69,9 @@ def test_noalloc_matches_device_entry_on_two_calls():
     for G, topo, scale in calls:
         ev.to_device(G_dev, ev.pack(G).real)
         ref = _run(ev, "xca_compute_self_energy_device", G_dev, S_dev, topo, scale)
+        before = _allocations()
         got = _run(ev, "xca_compute_self_energy_device_noalloc", G_dev, S_dev, topo, scale)
+        assert _allocations() == before  # the call itself allocated no device memory
         assert max(np.max(np.abs(b)) for b in ref) > 0.0
         assert _node_rel_err(got, ref) <= 1.0, topo
 

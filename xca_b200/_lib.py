@@ -78,6 +78,7 @@ SIGNATURES = {
     "xca_copy_to_host": [P, dp, P, L],
     "xca_synchronize": [P],
     "xca_kernel_launches": [P, lp],
+    "xca_device_allocations": [lp],
     "xca_set_precision_mode": [P, I],
     "xca_set_tuning": [P, I, I],
     "xca_get_tuning": [P, I, ip],

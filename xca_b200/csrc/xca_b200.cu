@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -38,6 +39,9 @@ struct Error : std::runtime_error {
     if (e_ != cudaSuccess) throw Error(XCA_ERR_CUDA, std::string(#x ": ") + cudaGetErrorString(e_)); \
   } while (0)
 
+// Device allocations made by the library's own buffers since load (xca_device_allocations).
+static std::atomic<long> g_device_allocations{0};
+
 template <class T>
 struct DevBuf {
   T *ptr = nullptr;
@@ -49,6 +53,7 @@ struct DevBuf {
     n = 0;
     if (count == 0) return;
     CUDA_CHECK(cudaMalloc(&ptr, count * sizeof(T)));
+    g_device_allocations.fetch_add(1, std::memory_order_relaxed);
     n = count;
   }
   void upload(const std::vector<T> &v, cudaStream_t s) {
@@ -2146,6 +2151,12 @@ int xca_get_precision_mode(xca_ctx *ctx, int *mode) {
   API_END
 }
 
+int xca_device_allocations(long *out) {
+  API_BEGIN
+  *out = g_device_allocations.load(std::memory_order_relaxed);
+  API_END
+}
+
 int xca_kernel_launches(xca_ctx *ctx, long *out) {
   API_BEGIN
   *out = reinterpret_cast<Ctx *>(ctx)->launches;
@@ -2189,9 +2200,16 @@ int xca_compute_self_energy_device_noalloc(xca_ctx *ctx, const double *G_dev, in
   for (int b = 0; b < nb; ++b) zero[b] = mx[b] < 1e-16 ? 1 : 0;
   // host work list, cached per (topology, zero pattern)
   const std::string key = class_key(T, zero);
-  auto itc = c->noalloc_classes.find(key);
-  if (itc == c->noalloc_classes.end()) itc = c->noalloc_classes.emplace(key, build_classes(c, T, zero)).first;
-  const ClassSet *cs = itc->second.get();
+  // the allocating path's cached work list when it has built one (its host vectors only), else a host-only one
+  const ClassSet *cs = nullptr;
+  auto itk = c->class_cache.find(key);
+  if (itk != c->class_cache.end()) {
+    cs = itk->second.get();
+  } else {
+    auto itc = c->noalloc_classes.find(key);
+    if (itc == c->noalloc_classes.end()) itc = c->noalloc_classes.emplace(key, build_classes(c, T, zero)).first;
+    cs = itc->second.get();
+  }
   if (!cs->wide_units.empty())
     throw Error(XCA_ERR_UNSUPPORTED, "xca_compute_self_energy_device_noalloc: block chains wider than the panel kernel's panel are "
                                      "not supported; use xca_compute_self_energy_device");
