@@ -16,11 +16,11 @@ template <int RP>
 int launch_sigma_panel(cudaStream_t s, int nsm, const DevBasis &B, const ClassRec *classes, const WorkUnit *units, int n_units,
                        int *counter, const double *G, const SigmaOut &out);
 
-// Wide-chain Sigma kernel (sigma_wide.cuh) over n_units units with `grid` CTAs, three slabs of `slab`
-// doubles per CTA in scratch.
+// Wide-chain Sigma kernel (sigma_wide.cuh) over n_units units with `grid` CTAs; each CTA's region of scratch
+// is cta_doubles long and holds 3 + (largest symmetry set) slabs of `slab` doubles.
 template <int RP>
 int launch_sigma_wide(cudaStream_t s, int grid, const DevBasis &B, const ClassRec *classes, const WorkUnit *units, int n_units,
-                      int *counter, const double *G, const SigmaOut &out, double *scratch, long slab);
+                      int *counter, const double *G, const SigmaOut &out, double *scratch, long slab, long cta_doubles);
 
 // Usable panel columns of the panel kernels of rank RP.
 template <int RP>

@@ -3,13 +3,13 @@
 // The panel kernel (sigma_panel.cuh) keeps a batch of items in shared memory, which bounds an item's widest
 // state (rows x columns of its T slab) by the panel width.  Chains through large Fock-space blocks (the
 // five-orbital d shell has blocks up to 100 x 100, states of up to 10^4 entries) run here instead: a CTA
-// evaluates one item at a time with its T, X and Y slabs (r x widest state each) in a per-CTA region of
-// global memory, the threads striding over output entries.  The steps are those of
+// evaluates one item at a time with its T, X and Y slabs (r x widest state each) and one slab per
+// zero-vertex operator in a per-CTA region of global memory, the threads striding over output entries.  The steps are those of
 // eval_self_energy_fixed_indices (c++/triqs_xca/block_sparse_backbone.cpp:339-367) in the operation order of
 // the CPU restatement, as in the panel kernel, so each item's contribution is bit-identical to it:
 //   vertex       X(t) = k(t) (F T(t))                   fused multiply-adds over the inner index, then k
 //   edge         corr_edge: K^-1 per column (substitution order of getrs), W, Q / P', (beta K) products
-//   zero vertex  Y(t) = sum_kappa (+-h) (T(t) F_kappa); X(t) += F_mu Y(t), mu in order
+//   zero vertex  T(t) F_kappa once per kappa, then Y(t) = sum_kappa (+-h) (T(t) F_kappa); X(t) += F_mu Y(t)
 //   prefactor    T *= scale; the 1e-16 guard on max |T|; accumulation (atomics, or the ordered slots).
 #pragma once
 #include "sigma_kernel.cuh"
@@ -30,7 +30,8 @@ template <int RP>
 __global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, const ClassRec *__restrict__ classes,
                                                                   const WorkUnit *__restrict__ units, int n_units,
                                                                   int *__restrict__ unit_counter, const double *__restrict__ G,
-                                                                  SigmaOut out, double *__restrict__ scratch, long slab) {
+                                                                  SigmaOut out, double *__restrict__ scratch, long slab,
+                                                                  long cta_doubles) {
   extern __shared__ __align__(16) double smem[];
   double *sLU = smem, *sW = sLU + RP * RP + RP, *sBK = sW + RP * RP;
   int *sPerm = reinterpret_cast<int *>(sBK + RP * RP);
@@ -47,7 +48,7 @@ __global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, co
   __shared__ double s_red[WIDE_THREADS / 32];
   __syncthreads();
   const int r = B.r, p = B.p, n = B.n, tid = threadIdx.x, NT = WIDE_THREADS;
-  double *T0 = scratch + (long)blockIdx.x * 3 * slab;
+  double *T0 = scratch + (long)blockIdx.x * cta_doubles;  // T | X | Y | one slab per zero-vertex operator
 
   while (true) {
     if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
@@ -157,21 +158,31 @@ __global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, co
             for (int idx = tid; idx < r * dvp * d0; idx += NT) X[idx] = 0.0;
             __syncthreads();
           }
-          for (int mu = 0; mu < qs; ++mu) {
-            const int om = B.set_to_orb[pk * n + mu];
-            const int per = dv * d0;
+          // T(t) F_kappa for every kappa once (the same fused multiply-adds as forming it per mu)
+          const int per = dv * d0;
+          double *TK = T0 + 3 * slab;
+          for (int kap = 0; kap < qs; ++kap) {
+            const double *Fk0 = B.ops + ok_off + (size_t)kap * d1 * d0;
+            double *tk = TK + (long)kap * slab;
             for (int idx = tid; idx < r * per; idx += NT) {
               const int t = idx / per, e2 = idx - t * per, x = e2 / d0, z = e2 - x * d0;
-              const double *Tx = T + (long)t * dv * d1 + x * d1;
+              const double *Tx = T + (long)t * dv * d1 + x * d1, *Fk = Fk0 + z;
+              double tf = 0.0;
+              for (int y = 0; y < d1; ++y) tf = fmad(Tx[y], Fk[y * d0], tf);
+              tk[idx] = tf;
+            }
+          }
+          __syncthreads();
+          for (int mu = 0; mu < qs; ++mu) {
+            const int om = B.set_to_orb[pk * n + mu];
+            for (int idx = tid; idx < r * per; idx += NT) {
+              const int t = idx / per;
               double a = 0.0;
               for (int kap = 0; kap < qs; ++kap) {
                 const int ok = B.set_to_orb[pk * n + kap];
                 const double h = fwd ? B.hval[((size_t)t * n + om) * n + ok] : B.hrefl[((size_t)t * n + ok) * n + om];
                 if (h == 0.0) continue;
-                const double *Fk = B.ops + ok_off + (size_t)kap * d1 * d0 + z;
-                double tf = 0.0;
-                for (int y = 0; y < d1; ++y) tf = fmad(Tx[y], Fk[y * d0], tf);
-                a = fmad(mul(hs, h), tf, a);
+                a = fmad(mul(hs, h), TK[(long)kap * slab + idx], a);
               }
               Y[idx] = a;
             }

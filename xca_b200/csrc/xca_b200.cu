@@ -699,12 +699,15 @@ static void launch_wide_units(Ctx *c, const DevBasis &B, const ClassRec *d_class
                               const double *G_dev, const SigmaOut &out) {
   if (n_units == 0) return;
   const int grid = std::max(1, std::min(c->wide_ctas_per_sm * c->nsm, n_units));
-  c->d_wide_scratch.resize((size_t)grid * 3 * std::max(slab, 1L));
+  long qmax = 1;
+  for (long q : c->ssizes) qmax = std::max(qmax, q);
+  const long cta_doubles = (3 + qmax) * std::max(slab, 1L);
+  c->d_wide_scratch.resize((size_t)grid * cta_doubles);
   c->d_wide_counter.resize(1);
   switch (c->RP) {
-    case 32: c->launches += launch_sigma_wide<32>(c->stream, grid, B, d_classes, d_units, n_units, c->d_wide_counter.ptr, G_dev, out, c->d_wide_scratch.ptr, slab); break;
-    case 48: c->launches += launch_sigma_wide<48>(c->stream, grid, B, d_classes, d_units, n_units, c->d_wide_counter.ptr, G_dev, out, c->d_wide_scratch.ptr, slab); break;
-    default: c->launches += launch_sigma_wide<64>(c->stream, grid, B, d_classes, d_units, n_units, c->d_wide_counter.ptr, G_dev, out, c->d_wide_scratch.ptr, slab); break;
+    case 32: c->launches += launch_sigma_wide<32>(c->stream, grid, B, d_classes, d_units, n_units, c->d_wide_counter.ptr, G_dev, out, c->d_wide_scratch.ptr, slab, cta_doubles); break;
+    case 48: c->launches += launch_sigma_wide<48>(c->stream, grid, B, d_classes, d_units, n_units, c->d_wide_counter.ptr, G_dev, out, c->d_wide_scratch.ptr, slab, cta_doubles); break;
+    default: c->launches += launch_sigma_wide<64>(c->stream, grid, B, d_classes, d_units, n_units, c->d_wide_counter.ptr, G_dev, out, c->d_wide_scratch.ptr, slab, cta_doubles); break;
   }
 }
 
