@@ -1,15 +1,17 @@
 """Generates tests/golden/topologies.json by importing the reference's own pure-Python diagram
 enumerator (python/triqs_xca/diag.py of TRIQS/xca), which needs only numpy.
 
-Run in the build container, where the reference is mounted:
-    python tests/golden/make_topologies.py /root/reference
+Run where a checkout of the reference is available, giving its root directory:
+    python tests/golden/make_topologies.py <path to the TRIQS/xca checkout>
 """
 import importlib.util
 import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_topologies.py <path to the TRIQS/xca checkout>")
+ref = sys.argv[1]
 spec = importlib.util.spec_from_file_location("ref_diag", os.path.join(ref, "python", "triqs_xca", "diag.py"))
 mod = importlib.util.module_from_spec(spec)
 spec.loader.exec_module(mod)

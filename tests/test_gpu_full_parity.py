@@ -198,3 +198,33 @@ def test_t2g_nca_solve_ordered_vs_oracle():
     assert _max_diff(S.G, G) <= 1e-10
     assert abs(S.eta - eta) <= 1e-10
     assert float(np.max(np.abs(S.G_tau - g))) <= 1e-10
+
+
+@pytest.mark.parametrize("mode", ["fp64_ordered", "fp64"])
+def test_zero_block_filtered_in_kernel(mode):
+    # the device-resident call leaves the zero-block test (max |G_b| < 1e-16 drops the path,
+    # find_path_self_energy) to the kernels; the host call tests on the host: both must give the oracle's Sigma
+    from xca_b200.block_sparse import BlockOpSymQuartet, DiagramEvaluator
+    d = O.Dlr(40.0, 1e-8)
+    m = models.kanamori_2orb(d.rf, d.it, 4.0, 40.0, 1e-8)
+    Fq = BlockOpSymQuartet(m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks, m.dims)
+    ev = DiagramEvaluator.from_arrays(4.0, 40.0, 1e-8, d.rf, d.it, m.hyb_poles, m.hyb_coeffs, Fq)
+    ora = O.Evaluator(d, 4.0, m.hyb_poles, m.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
+    ev.precision_mode = mode
+    G = models.seeded_G(m, 2)
+    G[3] = np.zeros_like(G[3])
+    G[5] = 1e-17 * G[5]
+    for topo in ([[0, 2], [1, 3]], [[0, 3], [1, 4], [2, 5]]):
+        t = np.array(topo, np.int32)
+        host = np.concatenate([s.real.ravel() for s in ev.compute_self_energy(G, t)])
+        dev = _device_topology(ev, G, t)
+        ref = np.concatenate([s.real.ravel() for s in (ora.compute_self_energy_ordered(G, t) if mode == "fp64_ordered"
+                                                       else ora.compute_self_energy(G, t))])
+        # blocks the host call zeroes (below 1e-16) may hold round-off in the device-resident result
+        if mode == "fp64_ordered":
+            assert np.array_equal(host, ref)
+            nz = np.abs(ref) > 0
+            assert np.array_equal(dev[nz], ref[nz])
+        else:
+            assert _per_node_rel(ev, host, ref) <= TOL_FAST_PER_NODE
+            assert _per_node_rel(ev, dev, ref) <= TOL_FAST_PER_NODE

@@ -54,7 +54,18 @@ struct DevBasis {
   const double *tab;    // edge tables: per block b at tab_off[b], per signature [fc (r d^2) | W fc (r d^2)]
   const long *tab_off;
   int nsig;             // signatures per block: 1 + 2p (+ 4p^2 when two K factors can meet on an edge)
+  const double *gmax;   // nullptr, or per block max |G_b| of this call's G: the kernels then drop the work units
+                        // whose block path meets a block below 1e-16 (the work list was built without that test)
 };
+
+// Does the block path of a class meet a zero block of G (max |G_b| < 1e-16, find_path_self_energy,
+// c++/triqs_xca/block_sparse_backbone.cpp:248-262)?  Only when the work list was built without the test.
+__device__ __forceinline__ bool path_meets_zero_block(const DevBasis &B, const int *ind_path, int m) {
+  if (B.gmax == nullptr) return false;
+  bool z = false;
+  for (int v = 0; v < 2 * m - 1; ++v) z |= B.gmax[ind_path[v]] < 1e-16;
+  return z;
+}
 
 struct ClassRec {
   int m, vct0, fbmask, b_out, pk;
@@ -115,6 +126,43 @@ struct DysonBasis {
 // D = A B + C on one 8 x 8 x 4 tile (a: A[g][q], b: B[q][g], c/d: C[g][2q], C[g][2q + 1], g = lane / 4, q = lane % 4).
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
   asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};" : "+d"(d0), "+d"(d1) : "d"(a), "d"(b));
+}
+
+// Batched small matrix products on the FP64 tensor cores, shared by the warps of a CTA:
+// for every batch entry e < nbatch, C_e[m][n] = sum_{k < K} A_e(m, k) B_e(k, n) for m < M, n < N, each entry
+// one chain of fused multiply-adds over k ascending from zero (an m8n8k4 MMA computes its tile as four
+// correctly rounded fused multiply-adds in ascending k), handed to epi(e, m, n, value).  Warps take 8 x 8
+// output tiles in turn (a warp index `warp` of `nwarps`); out-of-range rows, columns and k read as zero,
+// which adds exactly zero to the chain.  The accessors a(e, m, k) and b(e, k, n) read the operands.
+template <class FA, class FB, class FE>
+__device__ __forceinline__ void warp_gemm_dmma(int nbatch, int M, int N, int K, FA a, FB b, FE epi, int warp, int nwarps) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  const int mt = (M + 7) >> 3, nt = (N + 7) >> 3;
+  const long ntiles = (long)nbatch * mt * nt;
+  for (long tile = warp; tile < ntiles; tile += nwarps) {
+    const int e = (int)(tile / (mt * nt));
+    const int rem = (int)(tile - (long)e * mt * nt);
+    const int m0 = (rem / nt) * 8, n0 = (rem - (rem / nt) * nt) * 8;
+    const int ma = m0 + g, nb = n0 + g;
+    double c0 = 0.0, c1 = 0.0;
+    // the next k-group's fragments are loaded before the current MMA issues
+    double an = (ma < M && q < K) ? a(e, ma, q) : 0.0;
+    double bn = (q < K && nb < N) ? b(e, q, nb) : 0.0;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const double av = an, bv = bn;
+      const int k = k0 + 4 + q;
+      if (k0 + 4 < K) {
+        an = (ma < M && k < K) ? a(e, ma, k) : 0.0;
+        bn = (k < K && nb < N) ? b(e, k, nb) : 0.0;
+      }
+      dmma(c0, c1, av, bv);
+    }
+    const int nc = n0 + 2 * q;
+    if (ma < M) {
+      if (nc < N) epi(e, ma, nc, c0);
+      if (nc + 1 < N) epi(e, ma, nc + 1, c1);
+    }
+  }
 }
 
 // Arithmetic of the plain FP64 path: the fused multiply-adds and the separately rounded products and

@@ -634,6 +634,13 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
     const int dout = C.bdims[2 * m];
     const int cap = C.batch;
     const int nops = 4 * m - 3;
+    if (path_meets_zero_block(B, C.ind_path, m)) {
+      // the reference drops this path: no items (an ordered-mode slot still receives its zeros)
+      if (out.slots)
+        for (int idx = tid; idx < r * dout * d0; idx += NT) out.slots[out.slot_off[u] + idx] = 0.0;
+      __syncthreads();
+      continue;
+    }
 
     for (int first = 0; first < wu.count; first += cap) {
       const int nbi = min(cap, wu.count - first);

@@ -8,6 +8,8 @@
 // eval_self_energy_fixed_indices (c++/triqs_xca/block_sparse_backbone.cpp:339-367) in the operation order of
 // the CPU restatement, as in the panel kernel, so each item's contribution is bit-identical to it:
 //   vertex       X(t) = k(t) (F T(t))                   fused multiply-adds over the inner index, then k
+// The block products (vertex, zero-vertex operator products, the edge's Q and P') run on the FP64 tensor
+// cores (warp_gemm_dmma), whose chains are those of the scalar loops; the r x r DLR steps per column.
 //   edge         corr_edge: K^-1 per column (substitution order of getrs), W, Q / P', (beta K) products
 //   zero vertex  T(t) F_kappa once per kappa, then Y(t) = sum_kappa (+-h) (T(t) F_kappa); X(t) += F_mu Y(t)
 //   prefactor    T *= scale; the 1e-16 guard on max |T|; accumulation (atomics, or the ordered slots).
@@ -27,7 +29,7 @@ __host__ __device__ constexpr size_t wide_smem_bytes() {
 }
 
 template <int RP>
-__global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, const ClassRec *__restrict__ classes,
+__global__ void __launch_bounds__(WIDE_THREADS, RP <= 32 ? 2 : 1) sigma_wide_kernel(DevBasis B, const ClassRec *__restrict__ classes,
                                                                   const WorkUnit *__restrict__ units, int n_units,
                                                                   int *__restrict__ unit_counter, const double *__restrict__ G,
                                                                   SigmaOut out, double *__restrict__ scratch, long slab,
@@ -47,7 +49,7 @@ __global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, co
   __shared__ double s_scale;
   __shared__ double s_red[WIDE_THREADS / 32];
   __syncthreads();
-  const int r = B.r, p = B.p, n = B.n, tid = threadIdx.x, NT = WIDE_THREADS;
+  const int r = B.r, p = B.p, n = B.n, tid = threadIdx.x, NT = WIDE_THREADS, warp = tid >> 5, NWARPS = NT / 32;
   double *T0 = scratch + (long)blockIdx.x * cta_doubles;  // T | X | Y | one slab per zero-vertex operator
 
   while (true) {
@@ -65,6 +67,12 @@ __global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, co
     const ClassRec &C = s_cls;
     const int m = C.m, vct0 = C.vct0, d0 = C.bdims[0], d1 = C.bdims[1], dout = C.bdims[2 * m];
     const int nops = 4 * m - 3, pre = 2 * (vct0 - 1);
+    if (path_meets_zero_block(B, C.ind_path, m)) {
+      if (out.slots)
+        for (int idx = tid; idx < r * dout * d0; idx += NT) out.slots[out.slot_off[u] + idx] = 0.0;
+      __syncthreads();
+      continue;
+    }
 
     for (int it = 0; it < wu.count; ++it) {
       // ---- pole tuple (Backbone::set_pole_inds, backbone.cpp:86-150), prefactor and signs
@@ -118,14 +126,13 @@ __global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, co
             kt = (ks < 0 ? B.kitm : B.kitp) + l;
           }
           const int per = dvp * ncol;
-          for (int idx = tid; idx < r * per; idx += NT) {
-            const int t = idx / per, e = idx - t * per, x = e / ncol, z = e - x * ncol;
-            const double *Fx = F + x * dv, *Tt = T + (long)t * dv * ncol + z;
-            double a = 0.0;
-            for (int y = 0; y < dv; ++y) a = fmad(Fx[y], Tt[y * ncol], a);
-            if (kt) a = mul(a, kt[(size_t)t * p]);
-            X[idx] = a;
-          }
+          const double *Tc = T;
+          double *Xc = X;
+          warp_gemm_dmma(
+              r, dvp, ncol, dv, [&](int, int x, int y) { return F[x * dv + y]; },
+              [&](int t, int y, int z) { return Tc[(long)t * dv * ncol + y * ncol + z]; },
+              [&](int t, int x, int z, double a) { Xc[(long)t * per + x * ncol + z] = kt ? mul(a, kt[(size_t)t * p]) : a; }, warp,
+              NWARPS);
           __syncthreads();
           double *tmp = T; T = X; X = tmp;
         } else if (kind == 1) {
@@ -161,16 +168,12 @@ __global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, co
           // T(t) F_kappa for every kappa once (the same fused multiply-adds as forming it per mu)
           const int per = dv * d0;
           double *TK = T0 + 3 * slab;
-          for (int kap = 0; kap < qs; ++kap) {
-            const double *Fk0 = B.ops + ok_off + (size_t)kap * d1 * d0;
-            double *tk = TK + (long)kap * slab;
-            for (int idx = tid; idx < r * per; idx += NT) {
-              const int t = idx / per, e2 = idx - t * per, x = e2 / d0, z = e2 - x * d0;
-              const double *Tx = T + (long)t * dv * d1 + x * d1, *Fk = Fk0 + z;
-              double tf = 0.0;
-              for (int y = 0; y < d1; ++y) tf = fmad(Tx[y], Fk[y * d0], tf);
-              tk[idx] = tf;
-            }
+          {
+            const double *Tc = T, *Fk0 = B.ops + ok_off;
+            warp_gemm_dmma(
+                qs * r, dv, d0, d1, [&](int e, int x, int y) { return Tc[(long)(e % r) * dv * d1 + x * d1 + y]; },
+                [&](int e, int y, int z) { return Fk0[(size_t)(e / r) * d1 * d0 + y * d0 + z]; },
+                [&](int e, int x, int z, double a) { TK[(long)(e / r) * slab + (long)(e % r) * per + x * d0 + z] = a; }, warp, NWARPS);
           }
           __syncthreads();
           for (int mu = 0; mu < qs; ++mu) {
@@ -189,13 +192,16 @@ __global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, co
             __syncthreads();
             const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
             const int per2 = dvp * d0;
-            for (int idx = tid; idx < r * per2; idx += NT) {
-              const int t = idx / per2, e2 = idx - t * per2, x = e2 / d0, z = e2 - x * d0;
-              const double *Fx = Fm + x * dv, *Yt = Y + (long)t * dv * d0 + z;
-              double a = 0.0;
-              for (int y = 0; y < dv; ++y) a = fmad(Fx[y], Yt[y * d0], a);
-              X[idx] = add(mu == 0 ? 0.0 : X[idx], a);
-            }
+            const double *Yc = Y;
+            double *Xc = X;
+            warp_gemm_dmma(
+                r, dvp, d0, dv, [&](int, int x, int y) { return Fm[x * dv + y]; },
+                [&](int t, int y, int z) { return Yc[(long)t * dv * d0 + y * d0 + z]; },
+                [&](int t, int x, int z, double a) {
+                  double *o = Xc + (long)t * per2 + x * d0 + z;
+                  *o = add(mu == 0 ? 0.0 : *o, a);
+                },
+                warp, NWARPS);
             __syncthreads();
           }
           double *tmp = T; T = X; X = tmp;

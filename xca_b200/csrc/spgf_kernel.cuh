@@ -153,7 +153,16 @@ __device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, 
   }
   item_sync<CTA>();
   const double *fc = tb, *fw = tb + (long)r * dd;
-  // (b) Q_l (into Y)
+  // (b) Q_l (into Y); the CTA form of a left edge runs the products on the FP64 tensor cores (the same
+  // chains: k' = 2y takes f gt, k' = 2y + 1 takes Wf g)
+  if constexpr (CTA && LEFT) {
+    const double *fc0 = tb, *fw0 = tb + (long)r * dd, *Tc = T, *Xc = X;
+    warp_gemm_dmma(
+        r, rows, cols, 2 * d,
+        [&](int l, int x, int k) { return ((k & 1) ? fw0 : fc0)[(long)l * dd + x * d + (k >> 1)]; },
+        [&](int l, int k, int z) { return ((k & 1) ? Tc : Xc)[(long)l * dc + (k >> 1) * cols + z]; },
+        [&](int l, int x, int z, double a) { Y[(long)l * dc + x * cols + z] = a; }, lane >> 5, nt >> 5);
+  } else
   for (int idx = lane; idx < r * dc; idx += nt) {
     const int l = idx / dc, rem = idx - l * dc, x = rem / cols, z = rem - x * cols;
     double a = 0.0;
@@ -178,6 +187,13 @@ __device__ __forceinline__ void corr_edge(const DevBasis &B, const double *sLU, 
   }
   item_sync<CTA>();
   // (d) P'_l = K(0, om_l) (f_l g_l) (into Y)
+  if constexpr (CTA && LEFT) {
+    const double *fc0 = tb, *Tc = T;
+    warp_gemm_dmma(
+        r, rows, cols, d, [&](int l, int x, int y) { return fc0[(long)l * dd + x * d + y]; },
+        [&](int l, int y, int z) { return Tc[(long)l * dc + y * cols + z]; },
+        [&](int l, int x, int z, double a) { Y[(long)l * dc + x * cols + z] = mul(B.k0[l], a); }, lane >> 5, nt >> 5);
+  } else
   for (int idx = lane; idx < r * dc; idx += nt) {
     const int l = idx / dc, rem = idx - l * dc, x = rem / cols, z = rem - x * cols;
     double a = 0.0;

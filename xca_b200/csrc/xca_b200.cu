@@ -270,6 +270,7 @@ struct Ctx {
   DevBuf<double> d_xops;                  // one-time correlator: uploaded operator slabs
   DevBuf<long> d_xmu_off, d_xka_off;
   std::map<std::string, std::unique_ptr<ClassSet>> noalloc_classes;  // host-only work lists of the allocation-free call
+  const double *gmax_filter = nullptr;  // set while a device-resident call filters zero blocks in the kernels
   int unit_batches = 4;      // panel batches per work unit (tunable, XCA_TUNE_UNIT_BATCHES)
   int wide_unit_tuples = 4;  // pole tuples per work unit of the wide kernel (XCA_TUNE_WIDE_UNIT_TUPLES)
   int wide_ctas_per_sm = 2;  // CTAs of the wide kernel per SM (XCA_TUNE_WIDE_CTAS_PER_SM)
@@ -303,6 +304,7 @@ struct Ctx {
     B.hval = d_hval.ptr; B.hrefl = d_hrefl.ptr; B.goff = d_goff.ptr; B.dims = d_dims.ptr; B.ops = d_ops.ptr;
     B.F_off = d_F_off.ptr; B.Fd_off = d_Fd_off.ptr; B.Fb_off = d_Fb_off.ptr; B.Fdb_off = d_Fdb_off.ptr;
     B.set_to_orb = d_set_to_orb.ptr;
+    B.gmax = gmax_filter;
     return B;
   }
 };
@@ -598,6 +600,24 @@ static SigmaOut atomic_out(double *Sig_dev, double scale) {
   o.slot_off = nullptr;
   return o;
 }
+
+// Per-block max |G_b| of a device G into d_maxabs, left on the device: the Sigma kernels drop the paths
+// through zero blocks themselves, so a device-resident call needs no host round trip.  The work list is
+// the one of the all-nonzero pattern.
+static const double *block_max_async(Ctx *c, const double *G_dev) {
+  c->d_maxabs.resize(c->nb);
+  block_maxabs_kernel<<<c->nb, 256, 0, c->stream>>>(G_dev, c->d_goff.ptr, c->d_dims.ptr, c->r, c->nb, c->d_maxabs.ptr);
+  c->launches++;
+  CUDA_CHECK(cudaGetLastError());
+  return c->d_maxabs.ptr;
+}
+
+// Clears the context's zero-block filter when a device-resident call leaves (also on errors).
+struct GmaxFilter {
+  Ctx *c;
+  GmaxFilter(Ctx *ctx, const double *gmax) : c(ctx) { c->gmax_filter = gmax; }
+  ~GmaxFilter() { c->gmax_filter = nullptr; }
+};
 
 static std::vector<int> zero_flags_device(Ctx *c, const double *G_dev) {
   c->d_maxabs.resize(c->nb);
@@ -1430,8 +1450,8 @@ int xca_compute_self_energy_device(xca_ctx *ctx, const double *G_dev, int m, con
   if (!c->ready) throw Error(XCA_ERR_INVALID, "evaluator not set up");
   set_device(c);
   Topology T = parse_topology(m, topology);
-  auto zero = zero_flags_device(c, G_dev);
-  ClassSet *cs = get_classes(c, T, zero);
+  GmaxFilter filter(c, block_max_async(c, G_dev));
+  ClassSet *cs = get_classes(c, T, std::vector<int>(c->nb, 0));
   int nsig = prepare_tables(c, G_dev, m);
   launch_sigma(c, cs, G_dev, Sigma_dev, scale, nsig);
   API_END
@@ -1447,8 +1467,8 @@ int xca_compute_self_energy_device_shard(xca_ctx *ctx, const double *G_dev, int 
     throw Error(XCA_ERR_UNSUPPORTED, "the ordered summation mode evaluates whole topologies on one device (n_shards must be 1)");
   set_device(c);
   Topology T = parse_topology(m, topology);
-  auto zero = zero_flags_device(c, G_dev);
-  ClassSet *cs = get_classes(c, T, zero);
+  GmaxFilter filter(c, block_max_async(c, G_dev));
+  ClassSet *cs = get_classes(c, T, std::vector<int>(c->nb, 0));
   int nsig = prepare_tables(c, G_dev, m);
   if (n_shards == 1) {
     launch_sigma(c, cs, G_dev, Sigma_dev, scale, nsig);
