@@ -43,6 +43,10 @@ def parse():
                     help="instead of the Sigma metric: a Poisson stream of whole self-consistent solves through the solve server")
     ap.add_argument("--serving-requests", type=int, default=64)
     ap.add_argument("--no-serving", action="store_true", help="skip the served-solves measurement of the default line")
+    ap.add_argument("--dshell", action="store_true",
+                    help="instead of the Sigma metric: OCA Sigma of the five-orbital d shell (wide-chain kernel)")
+    ap.add_argument("--dshell-stride", type=int, default=1,
+                    help="with --dshell: evaluate every n-th flat index only (a small case, e.g. for a kernel profile)")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--no-variants", action="store_true", help="skip the compressed-hybridization variant")
     return ap.parse_args()
@@ -168,11 +172,12 @@ def cpu_baseline_object(seconds):
             "cpu_model": name, "host_cpus": usable, "sample_wall_s": wall}
 
 
-def run_serving(args):
+def run_serving(args, batched=False):
     """Served solves/s and p50 / p99 time to converged solve for a mixed request stream: Poisson arrivals
     (mean gap 5 ms, numpy default_rng(2)); each request draws a single-orbital Anderson (orders 1-3) or a
     two-orbital Kanamori model (orders 1-2), beta in {10, 20, 50, 100}, Lambda = 10 beta, eps = 1e-10,
-    U ~ U(1, 6), tolerance 1e-8; up to 8 solves run concurrently, each with its own context and stream."""
+    U ~ U(1, 6), tolerance 1e-8; up to 8 solves run concurrently, each with its own context and stream,
+    in worker threads or (``batched``) in lock step with one Sigma launch per iteration for all of them."""
     from xca_b200.serving import SolveServer, synthetic_request
     rng = np.random.default_rng(2)
     n = args.serving_requests
@@ -184,7 +189,7 @@ def run_serving(args):
         U = float(rng.uniform(1.0, 6.0))
         order = int(rng.integers(1, 4)) if kind == "anderson" else int(rng.integers(1, 3))
         reqs.append(synthetic_request(kind, beta, U, order, tag=(kind, beta, order)))
-    srv = SolveServer(max_concurrent=8)
+    srv = SolveServer(max_concurrent=8, batched=batched)
     for kind, order in (("anderson", 3), ("kanamori", 2)):  # warm-up: module load and first-use set-up
         srv.submit(synthetic_request(kind, 10.0, 2.0, order)).result()
     t0 = time.perf_counter()
@@ -203,6 +208,7 @@ def run_serving(args):
     out = {"metric": "served solves/s (FP64 plain, mixed stream)", "value": n / (t1 - t0), "unit": "solves/s", "n_gpus": 1,
            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
            "config": {"workload": "poisson_stream", "requests": n, "mean_gap_ms": 5.0, "max_concurrent": 8,
+                      "mode": "lock step, one batched Sigma launch per iteration" if batched else "worker threads",
                       "models": "anderson orders 1-3, kanamori_2orb orders 1-2", "beta": [10, 20, 50, 100], "tol": 1e-8},
            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
            "mean_iterations": float(np.mean([r.n_iter for r in res])),
@@ -250,6 +256,57 @@ def compressed_variant(m, G, device):
             "sigma_rel_change_vs_dlr_poles": diff, "ms_per_step": res["compressed"][0]}
 
 
+def run_dshell(args):
+    """OCA Sigma evaluations per second of the five-orbital d shell (10 spin-orbitals, N = 4..6: 672 states in
+    16 (N_up, N_dn) blocks up to 100 x 100; Slater F0 = 4, J = 0.7, F4 / F2 = 0.625; beta = 20, Lambda = 200,
+    eps = 1e-8, r = 31; diagonal Bethe hybridization on the DLR poles; seeded G from default_rng(0)).  Every
+    chain is wider than a shared-memory panel, so the wide-chain kernel does the work.  One step is the
+    device-resident evaluation of the OCA topology over every flat index, or with --dshell-stride n over every
+    n-th flat index (through the host API's flat-index list)."""
+    from xca_b200 import models
+    from xca_b200.block_sparse import BlockOpSymQuartet, DiagramEvaluator
+    from xca_b200.pycppdlr import ImTimeOps, build_dlr_rf
+    lam, eps, beta = 200.0, 1e-8, 20.0
+    rf = build_dlr_rf(lam, eps)
+    it = ImTimeOps(lam, rf).get_itnodes()
+    m = models.dshell_5orb(rf, it, beta, lam, eps)
+    G = models.seeded_G(m, 0)
+    Fq = BlockOpSymQuartet(m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks, m.dims)
+    ev = DiagramEvaluator.from_arrays(beta, lam, eps, rf, it, m.hyb_poles, m.hyb_coeffs, Fq)
+    topo = np.array([[0, 2], [1, 3]], np.int32)
+    flops, items = ev.self_energy_flops(G, topo)
+    stride = max(1, args.dshell_stride)
+    if stride > 1:
+        fix = np.arange(0, ev.get_num_self_energy_backbones(topo), stride)
+
+        def step():
+            ev.compute_self_energy(G, topo, f_ix=fix)
+        frac = len(fix) / ev.get_num_self_energy_backbones(topo)
+    else:
+        bg, bs = ev.device_buffer(30, ev.slab), ev.device_buffer(31, ev.slab)
+        ev.to_device(bg, ev.pack(G).real)
+
+        def step():
+            ev.zero_device(bs, ev.slab)
+            ev.compute_self_energy_device(bg, topo, 1.0, bs)
+        frac = 1.0
+    for _ in range(args.warmup):
+        step()
+    ms = []
+    for _ in range(args.steps):
+        ev.flush_l2(256 << 20)
+        ev.event_record(0)
+        step()
+        ev.event_record(1)
+        ms.append(ev.event_elapsed(0, 1))
+    t = float(np.median(ms))
+    return {"metric": "d-shell OCA Sigma(tau) evals/s (FP64 plain)", "value": 1000.0 / t / frac, "unit": "evals/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "dshell_5orb_beta20_L200_eps1e-8_OCA", "r": int(len(rf)),
+                                            "flat_index_stride": stride, "l2": "flushed (256 MB write) before each step"},
+            "items_full": int(items), "tflops": flops * frac / (t * 1e-3) / 1e12}
+
+
 def run_reference(args, rank):
     """--impl reference: the CPU restatement of the reference's path (oracle) on the host cores.  One step is
     a bounded random sample of the benchmark evaluation; its time is extrapolated to the full evaluation."""
@@ -287,9 +344,14 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank)
         return
+    if args.dshell:
+        if rank == 0:
+            print(json.dumps(run_dshell(args)), flush=True)
+        return
     if args.serving:
         if rank == 0:
             print(json.dumps(run_serving(args)), flush=True)
+            print(json.dumps(run_serving(args, batched=True)), flush=True)
         return
     import torch
     dist = None
@@ -395,7 +457,7 @@ def main():
         variants = {"compressed_hybridization": compressed_variant(m, G, local)}
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
-        serving = run_serving(args)
+        serving = {"threads": run_serving(args), "batched": run_serving(args, batched=True)}
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": t_step, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",

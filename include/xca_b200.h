@@ -131,6 +131,17 @@ int xca_compute_self_energy(xca_ctx *ctx, const double *G, int m, const int *top
 int xca_compute_self_energy_device(xca_ctx *ctx, const double *G_dev, int m, const int *topology, double scale,
                                    double *Sigma_dev);
 
+/* Job-batched compute_self_energy_device (no counterpart in the reference, whose evaluator serves one solve
+ * per process): job j adds scales[j] * Sigma(topology j, order orders[j]) of the evaluator ctxs[j] on its
+ * device G_devs[j] into Sigma_devs[j].  The jobs' panel work units run in ONE persistent launch on ctxs[0]'s
+ * stream, so the iterations of many small solves share the device without a launch each; chains too wide
+ * for a panel follow on their own context's stream.  topologies is n_jobs x 6 ints (the first 2 m of each
+ * used).  Every context must be set up on the same device with the same padded DLR rank and the
+ * XCA_PREC_FP64 mode (else XCA_ERR_INVALID / XCA_ERR_UNSUPPORTED); the jobs of one context share one G.
+ * Each context's stream is ordered after the batch; the call does not wait for the device. */
+int xca_compute_self_energy_device_batch(int n_jobs, xca_ctx *const *ctxs, const double *const *G_devs, const int *orders,
+                                         const int *topologies, const double *scales, double *const *Sigma_devs);
+
 /* One shard of compute_self_energy_device: the work units u of the topology with u % n_shards == shard
  * (units are runs of pole tuples of one path class).  Summing the shards of every rank (an all-reduce)
  * gives the full result; replaces the flat-index scatter of python/triqs_xca/block_sparse_solver.py:29-33

@@ -20,7 +20,8 @@ def _close(a, b, tol=1e-10):
     assert np.max(np.abs(a.G_tau - b.G_tau)) < tol
 
 
-def test_result_same_alone_and_in_mix():
+@pytest.mark.parametrize("batched", [False, True])
+def test_result_same_alone_and_in_mix(batched):
     probe = synthetic_request("anderson", 10.0, 2.5, 2, tag="probe")
     others = [synthetic_request("kanamori", 10.0, 4.0, 2, tag="k2"),
               synthetic_request("anderson", 20.0, 3.0, 3, tag="a3"),
@@ -29,7 +30,7 @@ def test_result_same_alone_and_in_mix():
     srv = SolveServer(max_concurrent=1)
     alone = srv.submit(probe).result()
     srv.shutdown()
-    srv = SolveServer(max_concurrent=4)
+    srv = SolveServer(max_concurrent=4, batched=batched)
     futs = [srv.submit(r) for r in others[:2]] + [srv.submit(probe)] + [srv.submit(r) for r in others[2:]]
     results = [f.result() for f in futs]
     srv.shutdown()

@@ -59,6 +59,7 @@ SIGNATURES = {
     "xca_compute_self_energy": [P, dp, I, ip, lp, L, dp],
     "xca_compute_self_energy_device": [P, P, I, ip, D, P],
     "xca_compute_self_energy_device_shard": [P, P, I, ip, D, P, I, I],
+    "xca_compute_self_energy_device_batch": [I, ctypes.POINTER(P), ctypes.POINTER(P), ip, ip, dp, ctypes.POINTER(P)],
     "xca_compute_self_energy_device_noalloc": [P, P, I, ip, D, P],
     "xca_compute_single_ptcle_gf": [P, dp, I, ip, lp, L, dp],
     "xca_compute_single_ptcle_gf_device": [P, P, I, ip, D, P],

@@ -276,6 +276,12 @@ class DiagramEvaluator:
         return complex(out[0], out[1])
 
     @property
+    def padded_rank(self):
+        """Register-column width the Sigma kernels are compiled for: the DLR rank rounded up to 32, 48 or 64
+        (evaluators batched into one launch share it)."""
+        return 32 if self.r <= 32 else (48 if self.r <= 48 else 64)
+
+    @property
     def precision_mode(self):
         """'fp64' (items summed with atomics) or 'fp64_ordered' (fixed summation order, reproducible bit for bit)."""
         out = ctypes.c_int()
@@ -356,6 +362,30 @@ class DiagramEvaluator:
         t, m = self._topo(topology)
         _lib.check(_lib.lib().xca_compute_self_energy_device(self._ctx, ctypes.c_void_p(G_dev), m, _lib.as_ip(t), float(scale),
                                                              ctypes.c_void_p(Sigma_dev)))
+
+    @staticmethod
+    def compute_self_energy_device_batch(jobs):
+        """Job-batched compute_self_energy_device: jobs is a list of (evaluator, G_dev, topology, scale,
+        Sigma_dev); every job adds scale * Sigma(topology) of its evaluator into its Sigma_dev, the panel work of
+        all jobs in one launch on the first evaluator's stream (every evaluator's stream is ordered after it).
+        The evaluators share a device and a padded DLR rank and sum with atomics (precision 'fp64'); the jobs
+        of one evaluator share its G."""
+        n = len(jobs)
+        if n == 0:
+            return
+        P = ctypes.c_void_p
+        ctxs = (P * n)(*[j[0]._ctx for j in jobs])
+        Gs = (P * n)(*[j[1] for j in jobs])
+        Ss = (P * n)(*[j[4] for j in jobs])
+        orders = np.zeros(n, np.int32)
+        topo = np.zeros((n, 6), np.int32)
+        for k, j in enumerate(jobs):
+            t, m = DiagramEvaluator._topo(j[2])
+            orders[k] = m
+            topo[k, :2 * m] = t.ravel()
+        scales = np.ascontiguousarray([float(j[3]) for j in jobs], dtype=np.float64)
+        _lib.check(_lib.lib().xca_compute_self_energy_device_batch(n, ctxs, Gs, _lib.as_ip(orders), _lib.as_ip(topo),
+                                                                   _lib.as_dp(scales), Ss))
 
     def compute_self_energy_device_shard(self, G_dev, topology, scale, Sigma_dev, shard, n_shards):
         t, m = self._topo(topology)

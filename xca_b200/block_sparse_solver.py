@@ -87,60 +87,98 @@ class BlockSparseSolver:
     def _download(self, key):
         return [x.astype(np.complex128) for x in self.d.unpack(self.d.to_host(self._buf[key], self.d.slab))]
 
-    def _sigma_device(self, max_order):
+    def sigma_jobs(self, max_order):
+        """Zeroes the device Sigma and returns the iteration's Sigma evaluations as jobs (evaluator, G, topology,
+        scale, Sigma) of DiagramEvaluator.compute_self_energy_device_batch: every connected topology of orders
+        1..max_order with the reference's signs (block_sparse_solver.py:597-640)."""
         d = self.d
         d.zero_device(self._buf["S"], d.slab)
+        jobs = []
         for order in range(1, max_order + 1):
             for sign, topo in diag.all_connected_pairings(order):
                 # (-1)^order * parity * (-1)^(order+1): the order loop's and the topology loop's signs
                 fac = (-1) ** order * sign * (-1) ** (order + 1)
-                d.compute_self_energy_device(self._buf["G"], topo, float(fac), self._buf["S"])
+                jobs.append((d, self._buf["G"], topo, float(fac), self._buf["S"]))
+        return jobs
 
-    def solve(self, max_order, tol=1e-4, maxiter=10, mix=1.0, hyb_tol=None, hyb_comp=False, normalization="classic",
-              spgf_max_order=None, verbose=None):
-        """BlockSparseSolver.solve (block_sparse_solver.py:240-355) with the 'classic' normalisation."""
+    def _sigma_device(self, max_order):
+        jobs = self.sigma_jobs(max_order)
+        if self.precision == "fp64":
+            # every topology in one launch over the shared edge tables of the highest order
+            DiagramEvaluator.compute_self_energy_device_batch(jobs)
+        else:
+            # the fixed summation order: one ordered evaluation per topology, accumulated in topology order
+            for _, G, topo, fac, S in jobs:
+                self.d.compute_self_energy_device(G, topo, fac, S)
+
+    def begin(self, max_order, tol=1e-4, hyb_tol=None, hyb_comp=False, normalization="classic", spgf_max_order=None):
+        """The set-up of solve (block_sparse_solver.py:240-300): hybridization fit, evaluator, G on the device."""
         if normalization not in NORMALIZATIONS:
             raise NotImplementedError(f"normalization {normalization!r} is not available on the device path "
                                       f"(available: {', '.join(NORMALIZATIONS)})")
         self.normalization = normalization
-        verbose = self.verbose if verbose is None else verbose
         self.max_order = max_order
         self.spgf_max_order = spgf_max_order if spgf_max_order is not None else max_order
         # compression is skipped for NCA, whose backbones use no pole representation (block_sparse_solver.py:289)
         self.hyb_tol = hyb_tol if hyb_tol is not None else 0.1 * tol
         self.fit_hybridization(tol=self.hyb_tol, compression=hyb_comp and max_order > 1)
         self.init_diagram_evaluator()
-        d = self.d
         self._upload("G", self.G)
-        it = 0
-        t0 = time.perf_counter()
-        for it in range(1, maxiter + 1):
-            self._sigma_device(max_order)
-            if normalization in ("ode+classic", "ode+root"):
-                self.solve_ppsc_chempot_adiabatic_ode(tol=100 * self.eps)
-            if normalization in ("root", "ode+root"):
-                self.solve_ppsc_chempot_newton(xtol=10 * self.eps)
+
+    def launch_dyson(self):
+        """The Dyson solve of an iteration whose Sigma is on the device, for the 'classic' normalisation
+        (queued on the evaluator's stream)."""
+        self.d.dyson_solve_device(self._buf["S"], self.eta, self._buf["Gn"], hermitize=True)
+
+    def end_iteration(self, it, tol, mix, verbose=False, dyson_launched=False):
+        """The rest of one iteration after its Sigma (block_sparse_solver.py:300-345): eta, Dyson solve,
+        normalisation, diff_G; mixes G unless converged.  Returns True when diff_G < tol."""
+        d = self.d
+        normalization = self.normalization
+        if normalization in ("ode+classic", "ode+root"):
+            self.solve_ppsc_chempot_adiabatic_ode(tol=100 * self.eps)
+        if normalization in ("root", "ode+root"):
+            self.solve_ppsc_chempot_newton(xtol=10 * self.eps)
+        if not dyson_launched:
             d.dyson_solve_device(self._buf["S"], self.eta, self._buf["Gn"], hermitize=True)
-            if normalization in ("classic", "ode+classic"):
-                Z, deta = d.normalize_device(self._buf["Gn"])
-                self.eta += deta
-            else:
-                Z = -d.trace_device(self._buf["Gn"]).real
-            self.diff_G = d.max_abs_diff_device(self._buf["Gn"], self._buf["G"])
-            if verbose:
-                print(f"iter = {it}, diff_G = {self.diff_G:2.2E}, Z = {Z:+2.6E}, eta = {self.eta:2.2E}")
-            if self.diff_G < tol:
-                break
-            d.axpby_device(mix, self._buf["Gn"], 1.0 - mix, self._buf["G"])
-        d.synchronize()
-        self.timings["solve_loop_s"] = time.perf_counter() - t0
+        if normalization in ("classic", "ode+classic"):
+            Z, deta = d.normalize_device(self._buf["Gn"])
+            self.eta += deta
+        else:
+            Z = -d.trace_device(self._buf["Gn"]).real
+        self.diff_G = d.max_abs_diff_device(self._buf["Gn"], self._buf["G"])
         self.n_ppsc_iter = it
+        if verbose:
+            print(f"iter = {it}, diff_G = {self.diff_G:2.2E}, Z = {Z:+2.6E}, eta = {self.eta:2.2E}")
+        if self.diff_G < tol:
+            return True
+        d.axpby_device(mix, self._buf["Gn"], 1.0 - mix, self._buf["G"])
+        return False
+
+    def finish(self):
+        """The end of solve: G and Sigma back to the host, the single-particle Green's function."""
+        self.d.synchronize()
         self.G = self._download("G")
         self.Sigma = self._download("S")
         self.G_tau = None
         if self.spgf_max_order > 0:
             self.G_tau = self.eval_single_particle_greens_function(self.G, self.spgf_max_order)
         return self
+
+    def solve(self, max_order, tol=1e-4, maxiter=10, mix=1.0, hyb_tol=None, hyb_comp=False, normalization="classic",
+              spgf_max_order=None, verbose=None):
+        """BlockSparseSolver.solve (block_sparse_solver.py:240-355)."""
+        verbose = self.verbose if verbose is None else verbose
+        self.begin(max_order, tol, hyb_tol, hyb_comp, normalization, spgf_max_order)
+        t0 = time.perf_counter()
+        self.n_ppsc_iter = 0
+        for it in range(1, maxiter + 1):
+            self._sigma_device(max_order)
+            if self.end_iteration(it, tol, mix, verbose):
+                break
+        self.d.synchronize()
+        self.timings["solve_loop_s"] = time.perf_counter() - t0
+        return self.finish()
 
     # -- eta from Z(eta) = 1 ('root' / 'ode' normalizations, block_sparse_solver.py:744-1030).  G_alpha solves the
     # Dyson equation with alpha * Sigma (the current Sigma on the device) at eta; every Dyson solve, convolution

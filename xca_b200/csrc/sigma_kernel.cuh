@@ -84,6 +84,7 @@ struct WorkUnit {
   int cls;
   int first;
   int count;
+  int job = 0;  // job index of a job-batched launch (0 otherwise)
 };
 
 // Where a Sigma launch puts its result.  Fast mode (slots == nullptr): every batch adds scale * (its sum)
@@ -95,6 +96,15 @@ struct SigmaOut {
   double scale;
   double *slots;
   const long *slot_off;
+};
+
+// One job of a job-batched Sigma launch: a solve's basis, model and edge tables (B), the path classes of
+// one topology, the solve's G and where the topology's Sigma goes (fast summation: Sigma += scale * ...).
+struct SigmaJob {
+  DevBasis B;
+  const ClassRec *classes;
+  const double *G;
+  SigmaOut out;
 };
 
 // Per-item state of a batch, kept in shared memory.

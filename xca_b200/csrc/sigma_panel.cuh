@@ -595,24 +595,246 @@ __device__ __forceinline__ void zv_outer_pass(const double *Fm, const double *Y,
   }
 }
 
+// One work unit (a run of pole tuples of one path class, staged in shared memory as C) on the CTA's panels:
+// batches of `C.batch` items (see the file comment).  Shared by the single-job and the job-batched kernels.
+template <int RP>
+__device__ __forceinline__ void panel_unit(const DevBasis &B, const ClassRec &C, const WorkUnit &wu, int u, const double *__restrict__ G,
+                                           const SigmaOut &out, const double *sLU, const double *sW, const double *sBK,
+                                           double *PA, ItemState *ist, const int *sPerm, unsigned long long *s_max) {
+  constexpr int NC = PanelCfg<RP>::LDP, NT = PANEL_THREADS;  // NC: panel row stride
+  double *PB = PA + RP * NC, *PC = PB + RP * NC;
+  const int r = B.r, p = B.p, n = B.n, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m = C.m, vct0 = C.vct0;
+  const int d0 = C.bdims[0], d1 = C.bdims[1];
+  const int dout = C.bdims[2 * m];
+  const int cap = C.batch;
+  const int nops = 4 * m - 3;
+  if (path_meets_zero_block(B, C.ind_path, m)) {
+    // the reference drops this path: no items (an ordered-mode slot still receives its zeros)
+    if (out.slots)
+      for (int idx = tid; idx < r * dout * d0; idx += NT) out.slots[out.slot_off[u] + idx] = 0.0;
+    __syncthreads();
+    return;
+  }
+
+  for (int first = 0; first < wu.count; first += cap) {
+    const int nbi = min(cap, wu.count - first);
+    // ---- decode the pole tuples (Backbone::set_pole_inds, backbone.cpp:86-150)
+    if (tid < nbi) {
+      ItemState &S = ist[tid];
+      int q = wu.first + first + tid;
+      for (int i = 0; i < MAXM; ++i) { S.lpole[i] = 0; S.caseA[i] = 0; }
+      for (int i = 1; i < m; ++i) {
+        S.lpole[i] = q % p;
+        q /= p;
+      }
+      double pf = 1.0;
+      int psign = 1;
+      for (int i = 1; i < m; ++i) {
+        const int fwd = (C.fbmask >> i) & 1;
+        const double w = B.polesb[S.lpole[i]];
+        S.caseA[i] = fwd ? (w <= 0.0) : (w >= 0.0);
+        if (!fwd) psign = -psign;
+        const int row = S.caseA[i] ? (fwd ? 1 : 0) : (fwd ? 0 : 1);
+        const int ex = S.caseA[i] ? 1 : C.lb[i] - C.la[i] - 1;
+        if (ex != 0) pf = mul(pf, B.kpow[((size_t)row * p + S.lpole[i]) * (MAXE + 1) + ex]);
+      }
+      int dsign = (m % 2 == 0) ? -1 : 1;
+      if (!(C.fbmask & 1)) dsign = -dsign;
+      S.scale = mul(pf, (double)(psign * dsign));
+      s_max[tid] = 0ull;
+    }
+    double *T = PA, *X = PB, *Y = PC;
+    // T := G[ind_path[0]] (d1 x d1) for every item
+    {
+      const double *g = G + B.goff[C.ind_path[0]];
+      const int dc = d1 * d1, nc = nbi * dc, tpc = NT / nc, c = tid % nc, t0 = tid / nc;
+      if (t0 < tpc) {
+        const int e = c % dc;
+        for (int t = t0; t < r; t += tpc) T[t * NC + c] = g[t * dc + e];
+      }
+    }
+    __syncthreads();
+
+    // op order: for v < vct0: vertex v, edge v; zero vertex; for v > vct0: edge v - 1, vertex v
+    const int pre = 2 * (vct0 - 1);
+    auto op_kind = [&](int o) -> int {
+      if (o < pre) return (o & 1) ? 1 : 0;
+      if (o == pre) return 2;
+      return ((o - pre - 1) & 1) ? 0 : 1;
+    };
+    for (int op = 0; op < nops; ++op) {
+      int v;
+      const int kind = op_kind(op);
+      if (op < pre) v = 1 + op / 2;
+      else if (op == pre) v = vct0;
+      else v = vct0 + 1 + (op - pre - 1) / 2;
+      const int ncol = v < vct0 ? d1 : d0;
+      // a vertex feeding an edge writes its rows in pivot order (the order the substitution works in)
+      const int *rowpos = (op + 1 < nops && op_kind(op + 1) == 1) ? sPerm + RP : nullptr;
+
+      if (kind == 0) {
+        // ---- vertex v: T(t) <- k(t) F T(t)  (multiply_left_vertex)
+        const int line = C.vline[v];
+        const int b = C.ind_path[v - 1];
+        const int dv = C.bdims[v], dvp = C.bdims[v + 1];
+        const int s = C.vset[v], qo = C.vqo[v];
+        // operator base of this vertex (uniform); the pole-dependent part and the K factor are per item
+        const int vk = C.vkind[v];
+        const long vbase = vk == 0 ? B.F_off[s * B.nb + b] : vk == 1 ? B.Fd_off[s * B.nb + b]
+                         : vk == 2 ? B.Fb_off[s * B.nb + b] : B.Fdb_off[s * B.nb + b];
+        int ks = 0;
+        if (line > 0) {
+          const int fwd = (C.fbmask >> line) & 1;
+          ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
+        }
+        const VertexOp vo{vbase, qo, line, ks, vk >= 2};
+        switch (dv) {
+          case 1: vertex_pass<RP, 1>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+          case 2: vertex_pass<RP, 2>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+          case 3: vertex_pass<RP, 3>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+          case 4: vertex_pass<RP, 4>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+          default: vertex_pass<RP, 0>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
+        }
+        __syncthreads();
+        double *tmp = T; T = X; X = tmp;
+      } else if (kind == 1) {
+        // ---- edge e: T <- conv(G_b prod K, T)  (integrate_left_edge, time-ordered convolution)
+        const int e = v < vct0 ? v : v - 1;
+        const int b = C.ind_path[e];
+        const int d = C.bdims[e + 1];
+        const int dd = d * d, dc = d * ncol, nc = nbi * dc;
+        if (tid < nbi) {
+          ItemState &S = ist[tid];
+          int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
+          for (int i = 1; i < m; ++i)
+            if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
+              sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
+              lp[nf] = S.lpole[i];
+              nf++;
+            }
+          long sig = 0;
+          if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
+          if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
+          S.taboff = B.tab_off[b] + sig * 2 * r * dd;
+        }
+        // (a) gc = K^-1 T (in place), then Gt = W gc (into X)
+        panel_trsm_mma<RP>(sLU, T, r, nc, tid, warp, lane);
+        panel_mma<RP, false>(sW, T, nullptr, X, r, nc, nullptr, warp, lane);
+        __syncthreads();
+        // (b) per row l (one warp per row; Q and P' of row l read only row l of gc and Gt):
+        //     Q_l = Ft_l gc_l + fc_l Gt_l (into Y) and P'_l = K(0, om_l) (fc_l gc_l) (over Gt, into X)
+        switch (d) {
+          case 1: qp_pass<RP, 1>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
+          case 2: qp_pass<RP, 2>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
+          case 3: qp_pass<RP, 3>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
+          case 4: qp_pass<RP, 4>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
+          default: qp_pass<RP, 0>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
+        }
+        __syncthreads();
+        // (c) h = fma(t_i, (beta K) P', (beta K) Q) (into T; gc is no longer needed)
+        panel_mma<RP, true>(sBK, Y, X, T, r, nc, B.tabs, warp, lane);
+        __syncthreads();
+      } else {
+        // ---- zero vertex (multiply_left_vertex_and_right_zero_vertex)
+        const int b_mu = C.ind_path[v - 1];
+        const int dv = C.bdims[v], dvp = C.bdims[v + 1];
+        const bool fwd = C.fbmask & 1;
+        const int pk = C.pk;
+        const long ok_off = fwd ? B.F_off[pk * B.nb + C.b_out] : B.Fd_off[pk * B.nb + C.b_out];
+        const long om_off = fwd ? B.Fd_off[pk * B.nb + b_mu] : B.F_off[pk * B.nb + b_mu];
+        const double hs = fwd ? 1.0 : -1.0;
+        int qs = 0;
+        for (int i = 0; i < n; ++i)
+          if (B.set_to_orb[pk * n + i] >= 0) qs = i + 1;
+        if (qs == 0) {  // no operator pair: the zero vertex is zero
+          const int nco = nbi * dvp * d0, tpo = NT / nco, co = tid % nco, to0 = tid / nco;
+          if (to0 < tpo)
+            for (int t = to0; t < r; t += tpo) X[(rowpos ? rowpos[t] : t) * NC + co] = 0.0;
+          __syncthreads();
+        }
+        for (int mu = 0; mu < qs; ++mu) {
+          const int om = B.set_to_orb[pk * n + mu];
+          switch (d1) {
+            case 1: zv_inner_pass<RP, 1>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
+            case 2: zv_inner_pass<RP, 2>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
+            case 3: zv_inner_pass<RP, 3>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
+            case 4: zv_inner_pass<RP, 4>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
+            default: zv_inner_pass<RP, 0>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
+          }
+          __syncthreads();
+          const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
+          switch (dv) {
+            case 1: zv_outer_pass<RP, 1>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
+            case 2: zv_outer_pass<RP, 2>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
+            case 3: zv_outer_pass<RP, 3>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
+            case 4: zv_outer_pass<RP, 4>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
+            default: zv_outer_pass<RP, 0>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
+          }
+          __syncthreads();
+        }
+        double *tmp = T; T = X; X = tmp;
+      }
+    }
+    // ---- prefactor and signs, the |T| > 1e-16 guard, accumulation
+    const int dco = dout * d0, nc = nbi * dco;
+    {
+      const int tpc = NT / nc, c = tid % nc, t0 = tid / nc;
+      if (t0 < tpc) {
+        const int j = c / dco;
+        const double sc = ist[j].scale;
+        double mx = 0.0;
+        for (int t = t0; t < r; t += tpc) mx = fmax(mx, fabs(mul(T[t * NC + c], sc)));
+        atomicMax(&s_max[j], (unsigned long long)__double_as_longlong(mx));  // non-negative doubles order as integers
+      }
+    }
+    __syncthreads();
+    if (out.slots) {
+      // ordered mode: the unit's running sum continues over its batches (a thread keeps the same
+      // entries from batch to batch, so it reads back only what it wrote)
+      double *dst = out.slots + out.slot_off[u];
+      for (int idx = tid; idx < r * dco; idx += NT) {
+        const int t = idx / dco, ee = idx - t * dco;
+        double a = first == 0 ? 0.0 : dst[idx];
+        for (int j = 0; j < nbi; ++j)
+          if (__longlong_as_double((long long)s_max[j]) > 1e-16) a = add(a, mul(T[t * NC + j * dco + ee], ist[j].scale));
+        dst[idx] = a;
+      }
+    } else {
+      double *dst = out.Sigma + B.goff[C.b_out];
+      for (int idx = tid; idx < r * dco; idx += NT) {
+        const int t = idx / dco, ee = idx - t * dco;
+        double a = 0.0;
+        bool keep_any = false;
+        for (int j = 0; j < nbi; ++j)
+          if (__longlong_as_double((long long)s_max[j]) > 1e-16) {
+            a = add(a, mul(T[t * NC + j * dco + ee], ist[j].scale));
+            keep_any = true;
+          }
+        if (keep_any) atomicAdd(dst + idx, mul(out.scale, a));
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // Dynamic shared memory: see panel_smem_doubles.
 template <int RP>
 __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis B, const ClassRec *__restrict__ classes,
                                                                         const WorkUnit *__restrict__ units, int n_units,
                                                                         int *__restrict__ unit_counter, const double *__restrict__ G,
                                                                         SigmaOut out) {
-  constexpr int NC = PanelCfg<RP>::LDP, NT = PANEL_THREADS;  // NC: panel row stride
+  constexpr int NT = PANEL_THREADS;
   extern __shared__ __align__(16) double smem[];
   double *sLU, *sW, *sBK, *PA;
   ItemState *ist;
   int *sPerm;
   panel_layout<RP>(smem, sLU, sW, sBK, PA, ist, sPerm);
-  double *PB = PA + RP * NC, *PC = PB + RP * NC;
   __shared__ int s_unit;
   __shared__ ClassRec s_cls;
   __shared__ unsigned long long s_max[PANEL_BMAX];
   stage_basis<RP>(B, sLU, sW, sBK, sPerm);
-  const int r = B.r, p = B.p, n = B.n, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x;
 
   while (true) {
     if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
@@ -628,219 +850,61 @@ __global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_kernel(DevBasis 
       for (int i = tid; i < (int)(sizeof(ClassRec) / sizeof(int)); i += NT) reinterpret_cast<int *>(&s_cls)[i] = src[i];
     }
     __syncthreads();
-    const ClassRec &C = s_cls;
-    const int m = C.m, vct0 = C.vct0;
-    const int d0 = C.bdims[0], d1 = C.bdims[1];
-    const int dout = C.bdims[2 * m];
-    const int cap = C.batch;
-    const int nops = 4 * m - 3;
-    if (path_meets_zero_block(B, C.ind_path, m)) {
-      // the reference drops this path: no items (an ordered-mode slot still receives its zeros)
-      if (out.slots)
-        for (int idx = tid; idx < r * dout * d0; idx += NT) out.slots[out.slot_off[u] + idx] = 0.0;
+    panel_unit<RP>(B, s_cls, wu, u, G, out, sLU, sW, sBK, PA, ist, sPerm, s_max);
+  }
+}
+
+// Job-batched form: every work unit names its job (a solve's basis, model and edge tables, a topology's
+// path classes, its G and its output).  The CTA stages a job's descriptor, and its DLR matrices when they
+// differ from the staged ones, as the units change job (the host lists the units job by job), then runs the
+// unit exactly as the single-job kernel does.  Fast (atomic) summation only.
+template <int RP>
+__global__ void __launch_bounds__(PANEL_THREADS, 1) sigma_panel_batch_kernel(const SigmaJob *__restrict__ jobs,
+                                                                              const WorkUnit *__restrict__ units, int n_units,
+                                                                              int *__restrict__ unit_counter) {
+  constexpr int NT = PANEL_THREADS;
+  extern __shared__ __align__(16) double smem[];
+  double *sLU, *sW, *sBK, *PA;
+  ItemState *ist;
+  int *sPerm;
+  panel_layout<RP>(smem, sLU, sW, sBK, PA, ist, sPerm);
+  __shared__ int s_unit, s_job_id;
+  __shared__ const double *s_staged;
+  __shared__ SigmaJob s_job;
+  __shared__ ClassRec s_cls;
+  __shared__ unsigned long long s_max[PANEL_BMAX];
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    s_job_id = -1;
+    s_staged = nullptr;
+  }
+  __syncthreads();
+  static_assert(sizeof(SigmaJob) % sizeof(int) == 0, "job descriptor copied as ints");
+
+  while (true) {
+    if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
+    __syncthreads();
+    const int u = s_unit;
+    __syncthreads();
+    if (u >= n_units) break;
+    const WorkUnit wu = units[u];
+    if (wu.job != s_job_id) {
+      const int *src = reinterpret_cast<const int *>(jobs + wu.job);
+      for (int i = tid; i < (int)(sizeof(SigmaJob) / sizeof(int)); i += NT) reinterpret_cast<int *>(&s_job)[i] = src[i];
       __syncthreads();
-      continue;
+      if (s_job.B.LUp != s_staged) stage_basis<RP>(s_job.B, sLU, sW, sBK, sPerm);
+      __syncthreads();
+      if (tid == 0) {
+        s_job_id = wu.job;
+        s_staged = s_job.B.LUp;
+      }
     }
-
-    for (int first = 0; first < wu.count; first += cap) {
-      const int nbi = min(cap, wu.count - first);
-      // ---- decode the pole tuples (Backbone::set_pole_inds, backbone.cpp:86-150)
-      if (tid < nbi) {
-        ItemState &S = ist[tid];
-        int q = wu.first + first + tid;
-        for (int i = 0; i < MAXM; ++i) { S.lpole[i] = 0; S.caseA[i] = 0; }
-        for (int i = 1; i < m; ++i) {
-          S.lpole[i] = q % p;
-          q /= p;
-        }
-        double pf = 1.0;
-        int psign = 1;
-        for (int i = 1; i < m; ++i) {
-          const int fwd = (C.fbmask >> i) & 1;
-          const double w = B.polesb[S.lpole[i]];
-          S.caseA[i] = fwd ? (w <= 0.0) : (w >= 0.0);
-          if (!fwd) psign = -psign;
-          const int row = S.caseA[i] ? (fwd ? 1 : 0) : (fwd ? 0 : 1);
-          const int ex = S.caseA[i] ? 1 : C.lb[i] - C.la[i] - 1;
-          if (ex != 0) pf = mul(pf, B.kpow[((size_t)row * p + S.lpole[i]) * (MAXE + 1) + ex]);
-        }
-        int dsign = (m % 2 == 0) ? -1 : 1;
-        if (!(C.fbmask & 1)) dsign = -dsign;
-        S.scale = mul(pf, (double)(psign * dsign));
-        s_max[tid] = 0ull;
-      }
-      double *T = PA, *X = PB, *Y = PC;
-      // T := G[ind_path[0]] (d1 x d1) for every item
-      {
-        const double *g = G + B.goff[C.ind_path[0]];
-        const int dc = d1 * d1, nc = nbi * dc, tpc = NT / nc, c = tid % nc, t0 = tid / nc;
-        if (t0 < tpc) {
-          const int e = c % dc;
-          for (int t = t0; t < r; t += tpc) T[t * NC + c] = g[t * dc + e];
-        }
-      }
-      __syncthreads();
-
-      // op order: for v < vct0: vertex v, edge v; zero vertex; for v > vct0: edge v - 1, vertex v
-      const int pre = 2 * (vct0 - 1);
-      auto op_kind = [&](int o) -> int {
-        if (o < pre) return (o & 1) ? 1 : 0;
-        if (o == pre) return 2;
-        return ((o - pre - 1) & 1) ? 0 : 1;
-      };
-      for (int op = 0; op < nops; ++op) {
-        int v;
-        const int kind = op_kind(op);
-        if (op < pre) v = 1 + op / 2;
-        else if (op == pre) v = vct0;
-        else v = vct0 + 1 + (op - pre - 1) / 2;
-        const int ncol = v < vct0 ? d1 : d0;
-        // a vertex feeding an edge writes its rows in pivot order (the order the substitution works in)
-        const int *rowpos = (op + 1 < nops && op_kind(op + 1) == 1) ? sPerm + RP : nullptr;
-
-        if (kind == 0) {
-          // ---- vertex v: T(t) <- k(t) F T(t)  (multiply_left_vertex)
-          const int line = C.vline[v];
-          const int b = C.ind_path[v - 1];
-          const int dv = C.bdims[v], dvp = C.bdims[v + 1];
-          const int s = C.vset[v], qo = C.vqo[v];
-          // operator base of this vertex (uniform); the pole-dependent part and the K factor are per item
-          const int vk = C.vkind[v];
-          const long vbase = vk == 0 ? B.F_off[s * B.nb + b] : vk == 1 ? B.Fd_off[s * B.nb + b]
-                           : vk == 2 ? B.Fb_off[s * B.nb + b] : B.Fdb_off[s * B.nb + b];
-          int ks = 0;
-          if (line > 0) {
-            const int fwd = (C.fbmask >> line) & 1;
-            ks = (v == C.la[line]) ? (fwd ? -1 : 1) : (fwd ? 1 : -1);
-          }
-          const VertexOp vo{vbase, qo, line, ks, vk >= 2};
-          switch (dv) {
-            case 1: vertex_pass<RP, 1>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
-            case 2: vertex_pass<RP, 2>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
-            case 3: vertex_pass<RP, 3>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
-            case 4: vertex_pass<RP, 4>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
-            default: vertex_pass<RP, 0>(B, vo, ist, T, X, rowpos, r, dv, dvp, ncol, nbi, tid); break;
-          }
-          __syncthreads();
-          double *tmp = T; T = X; X = tmp;
-        } else if (kind == 1) {
-          // ---- edge e: T <- conv(G_b prod K, T)  (integrate_left_edge, time-ordered convolution)
-          const int e = v < vct0 ? v : v - 1;
-          const int b = C.ind_path[e];
-          const int d = C.bdims[e + 1];
-          const int dd = d * d, dc = d * ncol, nc = nbi * dc;
-          if (tid < nbi) {
-            ItemState &S = ist[tid];
-            int nf = 0, sg[2] = {0, 0}, lp[2] = {0, 0};
-            for (int i = 1; i < m; ++i)
-              if (!S.caseA[i] && e >= C.la[i] && e < C.lb[i]) {
-                sg[nf] = ((C.fbmask >> i) & 1) ? 0 : 1;
-                lp[nf] = S.lpole[i];
-                nf++;
-              }
-            long sig = 0;
-            if (nf == 1) sig = 1 + (long)sg[0] * p + lp[0];
-            if (nf == 2) sig = 1 + 2L * p + ((long)sg[0] * p + lp[0]) * 2 * p + (long)sg[1] * p + lp[1];
-            S.taboff = B.tab_off[b] + sig * 2 * r * dd;
-          }
-          // (a) gc = K^-1 T (in place), then Gt = W gc (into X)
-          panel_trsm_mma<RP>(sLU, T, r, nc, tid, warp, lane);
-          panel_mma<RP, false>(sW, T, nullptr, X, r, nc, nullptr, warp, lane);
-          __syncthreads();
-          // (b) per row l (one warp per row; Q and P' of row l read only row l of gc and Gt):
-          //     Q_l = Ft_l gc_l + fc_l Gt_l (into Y) and P'_l = K(0, om_l) (fc_l gc_l) (over Gt, into X)
-          switch (d) {
-            case 1: qp_pass<RP, 1>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
-            case 2: qp_pass<RP, 2>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
-            case 3: qp_pass<RP, 3>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
-            case 4: qp_pass<RP, 4>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
-            default: qp_pass<RP, 0>(B, ist, T, X, Y, r, d, ncol, nc, warp, lane); break;
-          }
-          __syncthreads();
-          // (c) h = fma(t_i, (beta K) P', (beta K) Q) (into T; gc is no longer needed)
-          panel_mma<RP, true>(sBK, Y, X, T, r, nc, B.tabs, warp, lane);
-          __syncthreads();
-        } else {
-          // ---- zero vertex (multiply_left_vertex_and_right_zero_vertex)
-          const int b_mu = C.ind_path[v - 1];
-          const int dv = C.bdims[v], dvp = C.bdims[v + 1];
-          const bool fwd = C.fbmask & 1;
-          const int pk = C.pk;
-          const long ok_off = fwd ? B.F_off[pk * B.nb + C.b_out] : B.Fd_off[pk * B.nb + C.b_out];
-          const long om_off = fwd ? B.Fd_off[pk * B.nb + b_mu] : B.F_off[pk * B.nb + b_mu];
-          const double hs = fwd ? 1.0 : -1.0;
-          int qs = 0;
-          for (int i = 0; i < n; ++i)
-            if (B.set_to_orb[pk * n + i] >= 0) qs = i + 1;
-          if (qs == 0) {  // no operator pair: the zero vertex is zero
-            const int nco = nbi * dvp * d0, tpo = NT / nco, co = tid % nco, to0 = tid / nco;
-            if (to0 < tpo)
-              for (int t = to0; t < r; t += tpo) X[(rowpos ? rowpos[t] : t) * NC + co] = 0.0;
-            __syncthreads();
-          }
-          for (int mu = 0; mu < qs; ++mu) {
-            const int om = B.set_to_orb[pk * n + mu];
-            switch (d1) {
-              case 1: zv_inner_pass<RP, 1>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
-              case 2: zv_inner_pass<RP, 2>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
-              case 3: zv_inner_pass<RP, 3>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
-              case 4: zv_inner_pass<RP, 4>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
-              default: zv_inner_pass<RP, 0>(B, T, Y, r, pk, qs, om, fwd, hs, ok_off, d0, d1, dv, nbi, tid); break;
-            }
-            __syncthreads();
-            const double *Fm = B.ops + om_off + (size_t)mu * dvp * dv;
-            switch (dv) {
-              case 1: zv_outer_pass<RP, 1>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
-              case 2: zv_outer_pass<RP, 2>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
-              case 3: zv_outer_pass<RP, 3>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
-              case 4: zv_outer_pass<RP, 4>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
-              default: zv_outer_pass<RP, 0>(Fm, Y, X, rowpos, r, d0, dv, dvp, nbi, tid, mu == 0); break;
-            }
-            __syncthreads();
-          }
-          double *tmp = T; T = X; X = tmp;
-        }
-      }
-      // ---- prefactor and signs, the |T| > 1e-16 guard, accumulation
-      const int dco = dout * d0, nc = nbi * dco;
-      {
-        const int tpc = NT / nc, c = tid % nc, t0 = tid / nc;
-        if (t0 < tpc) {
-          const int j = c / dco;
-          const double sc = ist[j].scale;
-          double mx = 0.0;
-          for (int t = t0; t < r; t += tpc) mx = fmax(mx, fabs(mul(T[t * NC + c], sc)));
-          atomicMax(&s_max[j], (unsigned long long)__double_as_longlong(mx));  // non-negative doubles order as integers
-        }
-      }
-      __syncthreads();
-      if (out.slots) {
-        // ordered mode: the unit's running sum continues over its batches (a thread keeps the same
-        // entries from batch to batch, so it reads back only what it wrote)
-        double *dst = out.slots + out.slot_off[u];
-        for (int idx = tid; idx < r * dco; idx += NT) {
-          const int t = idx / dco, ee = idx - t * dco;
-          double a = first == 0 ? 0.0 : dst[idx];
-          for (int j = 0; j < nbi; ++j)
-            if (__longlong_as_double((long long)s_max[j]) > 1e-16) a = add(a, mul(T[t * NC + j * dco + ee], ist[j].scale));
-          dst[idx] = a;
-        }
-      } else {
-        double *dst = out.Sigma + B.goff[C.b_out];
-        for (int idx = tid; idx < r * dco; idx += NT) {
-          const int t = idx / dco, ee = idx - t * dco;
-          double a = 0.0;
-          bool keep_any = false;
-          for (int j = 0; j < nbi; ++j)
-            if (__longlong_as_double((long long)s_max[j]) > 1e-16) {
-              a = add(a, mul(T[t * NC + j * dco + ee], ist[j].scale));
-              keep_any = true;
-            }
-          if (keep_any) atomicAdd(dst + idx, mul(out.scale, a));
-        }
-      }
-      __syncthreads();
+    {
+      const int *src = reinterpret_cast<const int *>(s_job.classes + wu.cls);
+      for (int i = tid; i < (int)(sizeof(ClassRec) / sizeof(int)); i += NT) reinterpret_cast<int *>(&s_cls)[i] = src[i];
     }
+    __syncthreads();
+    panel_unit<RP>(s_job.B, s_cls, wu, u, s_job.G, s_job.out, sLU, sW, sBK, PA, ist, sPerm, s_max);
   }
 }
 

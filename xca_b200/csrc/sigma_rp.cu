@@ -46,6 +46,19 @@ int launch_sigma_panel(cudaStream_t s, int nsm, const DevBasis &B, const ClassRe
   return 1;
 }
 
+template <int RP>
+int launch_sigma_panel_batch(cudaStream_t s, int nsm, const SigmaJob *jobs, const WorkUnit *units, int n_units, int *counter) {
+  const size_t smem = panel_smem_doubles<RP>() * sizeof(double);
+  check(cudaFuncSetAttribute(sigma_panel_batch_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+        "sigma_panel_batch_kernel attributes");
+  check(cudaMemsetAsync(counter, 0, sizeof(int), s), "unit counter reset");
+  const int grid = std::max(1, std::min(nsm, n_units));
+  sigma_panel_batch_kernel<RP><<<grid, PANEL_THREADS, smem, s>>>(jobs, units, n_units, counter);
+  check(cudaGetLastError(), "sigma_panel_batch_kernel");
+  return 1;
+}
+
+template int launch_sigma_panel_batch<XCA_RP>(cudaStream_t, int, const SigmaJob *, const WorkUnit *, int, int *);
 template int panel_width<XCA_RP>();
 template int launch_edge_tables<XCA_RP>(cudaStream_t, int, const DevBasis &, const double *, const int2 *, int);
 template int launch_sigma_panel<XCA_RP>(cudaStream_t, int, const DevBasis &, const ClassRec *, const WorkUnit *, int, int *,

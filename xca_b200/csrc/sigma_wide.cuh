@@ -29,7 +29,7 @@ __host__ __device__ constexpr size_t wide_smem_bytes() {
 }
 
 template <int RP>
-__global__ void __launch_bounds__(WIDE_THREADS, RP <= 32 ? 2 : 1) sigma_wide_kernel(DevBasis B, const ClassRec *__restrict__ classes,
+__global__ void __launch_bounds__(WIDE_THREADS) sigma_wide_kernel(DevBasis B, const ClassRec *__restrict__ classes,
                                                                   const WorkUnit *__restrict__ units, int n_units,
                                                                   int *__restrict__ unit_counter, const double *__restrict__ G,
                                                                   SigmaOut out, double *__restrict__ scratch, long slab,

@@ -271,6 +271,13 @@ struct Ctx {
   DevBuf<long> d_xmu_off, d_xka_off;
   std::map<std::string, std::unique_ptr<ClassSet>> noalloc_classes;  // host-only work lists of the allocation-free call
   const double *gmax_filter = nullptr;  // set while a device-resident call filters zero blocks in the kernels
+  // job-batched Sigma launches led by this context: descriptors and units (host copies outlive the uploads)
+  std::vector<SigmaJob> h_batch_jobs;
+  std::vector<WorkUnit> h_batch_units;
+  DevBuf<SigmaJob> d_batch_jobs;
+  DevBuf<WorkUnit> d_batch_units;
+  DevBuf<int> d_batch_counter;
+  cudaEvent_t ev_batch = nullptr;  // orders this context's stream against a batch led by another context
   int unit_batches = 4;      // panel batches per work unit (tunable, XCA_TUNE_UNIT_BATCHES)
   int wide_unit_tuples = 4;  // pole tuples per work unit of the wide kernel (XCA_TUNE_WIDE_UNIT_TUPLES)
   int wide_ctas_per_sm = 2;  // CTAs of the wide kernel per SM (XCA_TUNE_WIDE_CTAS_PER_SM)
@@ -1234,6 +1241,7 @@ int xca_ctx_destroy(xca_ctx *ctx) {
   for (auto &e : c->prof_events) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   for (auto &e : c->user_events)
     if (e) cudaEventDestroy(e);
+  if (c->ev_batch) cudaEventDestroy(c->ev_batch);
   cudaStream_t s = c->stream;
   delete c;
   if (s) cudaStreamDestroy(s);
@@ -1454,6 +1462,98 @@ int xca_compute_self_energy_device(xca_ctx *ctx, const double *G_dev, int m, con
   ClassSet *cs = get_classes(c, T, std::vector<int>(c->nb, 0));
   int nsig = prepare_tables(c, G_dev, m);
   launch_sigma(c, cs, G_dev, Sigma_dev, scale, nsig);
+  API_END
+}
+
+int xca_compute_self_energy_device_batch(int n_jobs, xca_ctx *const *ctxs, const double *const *G_devs, const int *orders,
+                                         const int *topologies, const double *scales, double *const *Sigma_devs) {
+  API_BEGIN
+  if (n_jobs < 1) throw Error(XCA_ERR_INVALID, "compute_self_energy_device_batch: no jobs");
+  auto *c0 = reinterpret_cast<Ctx *>(ctxs[0]);
+  for (int j = 0; j < n_jobs; ++j) {
+    auto *c = reinterpret_cast<Ctx *>(ctxs[j]);
+    if (!c || !c->ready) throw Error(XCA_ERR_INVALID, "compute_self_energy_device_batch: evaluator not set up");
+    if (c->device != c0->device || c->RP != c0->RP)
+      throw Error(XCA_ERR_INVALID, "compute_self_energy_device_batch: the jobs' contexts must share the device and the padded DLR rank");
+    if (c->precision != XCA_PREC_FP64)
+      throw Error(XCA_ERR_UNSUPPORTED, "compute_self_energy_device_batch: the batched launch sums with atomics (XCA_PREC_FP64)");
+  }
+  set_device(c0);
+  // one preparation per context: its G's block norms (left on the device) and its edge tables in the layout
+  // of the highest order among its jobs
+  struct Prep {
+    Ctx *c;
+    const double *G;
+    int maxm;
+    int nsig;
+    const double *gmax;
+  };
+  std::vector<Prep> preps;
+  std::vector<int> prep_of(n_jobs);
+  std::vector<ClassSet *> sets(n_jobs);
+  for (int j = 0; j < n_jobs; ++j) {
+    auto *c = reinterpret_cast<Ctx *>(ctxs[j]);
+    size_t k = 0;
+    while (k < preps.size() && preps[k].c != c) ++k;
+    if (k == preps.size()) preps.push_back(Prep{c, G_devs[j], orders[j], 0, nullptr});
+    if (preps[k].G != G_devs[j])
+      throw Error(XCA_ERR_INVALID, "compute_self_energy_device_batch: the jobs of one context must share its G");
+    preps[k].maxm = std::max(preps[k].maxm, orders[j]);
+    prep_of[j] = (int)k;
+    set_device(c);
+    sets[j] = get_classes(c, parse_topology(orders[j], topologies + 6 * j), std::vector<int>(c->nb, 0));
+  }
+  for (Prep &pr : preps) {
+    Ctx *c = pr.c;
+    pr.gmax = block_max_async(c, pr.G);
+    pr.nsig = prepare_tables(c, pr.G, pr.maxm);
+    if (c != c0) {
+      if (!c->ev_batch) CUDA_CHECK(cudaEventCreateWithFlags(&c->ev_batch, cudaEventDisableTiming));
+      CUDA_CHECK(cudaEventRecord(c->ev_batch, c->stream));
+      CUDA_CHECK(cudaStreamWaitEvent(c0->stream, c->ev_batch, 0));
+    }
+  }
+  // the jobs' descriptors and their panel units, job by job, in one launch on the leading context's stream
+  c0->h_batch_jobs.resize(n_jobs);
+  c0->h_batch_units.clear();
+  for (int j = 0; j < n_jobs; ++j) {
+    const Prep &pr = preps[prep_of[j]];
+    SigmaJob &J = c0->h_batch_jobs[j];
+    J.B = pr.c->basis(pr.nsig);
+    J.B.gmax = pr.gmax;
+    J.classes = sets[j]->d_classes.ptr;
+    J.G = pr.G;
+    J.out = atomic_out(Sigma_devs[j], scales[j]);
+    for (WorkUnit w : sets[j]->units) {
+      w.job = j;
+      c0->h_batch_units.push_back(w);
+    }
+  }
+  if (!c0->h_batch_units.empty()) {
+    c0->d_batch_jobs.upload(c0->h_batch_jobs, c0->stream);
+    c0->d_batch_units.upload(c0->h_batch_units, c0->stream);
+    c0->d_batch_counter.resize(1);
+    const int nu = (int)c0->h_batch_units.size();
+    switch (c0->RP) {
+      case 32: c0->launches += launch_sigma_panel_batch<32>(c0->stream, c0->nsm, c0->d_batch_jobs.ptr, c0->d_batch_units.ptr, nu, c0->d_batch_counter.ptr); break;
+      case 48: c0->launches += launch_sigma_panel_batch<48>(c0->stream, c0->nsm, c0->d_batch_jobs.ptr, c0->d_batch_units.ptr, nu, c0->d_batch_counter.ptr); break;
+      default: c0->launches += launch_sigma_panel_batch<64>(c0->stream, c0->nsm, c0->d_batch_jobs.ptr, c0->d_batch_units.ptr, nu, c0->d_batch_counter.ptr); break;
+    }
+  }
+  // chains too wide for a panel: the wide kernel of the job's context, after the batch
+  if (!c0->ev_batch) CUDA_CHECK(cudaEventCreateWithFlags(&c0->ev_batch, cudaEventDisableTiming));
+  CUDA_CHECK(cudaEventRecord(c0->ev_batch, c0->stream));
+  for (const Prep &pr : preps)
+    if (pr.c != c0) CUDA_CHECK(cudaStreamWaitEvent(pr.c->stream, c0->ev_batch, 0));
+  for (int j = 0; j < n_jobs; ++j) {
+    ClassSet *cs = sets[j];
+    if (cs->wide_units.empty()) continue;
+    const Prep &pr = preps[prep_of[j]];
+    set_device(pr.c);
+    GmaxFilter filter(pr.c, pr.gmax);
+    launch_wide_units(pr.c, pr.c->basis(pr.nsig), cs->d_classes.ptr, cs->d_wide_units.ptr, (int)cs->wide_units.size(), cs->wide_slab,
+                      pr.G, atomic_out(Sigma_devs[j], scales[j]));
+  }
   API_END
 }
 

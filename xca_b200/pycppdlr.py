@@ -6,6 +6,7 @@ The node selection runs in the C++ library (host set-up, once per (Lambda, eps))
 """
 
 import ctypes
+import functools
 
 import numpy as np
 
@@ -13,13 +14,30 @@ from . import _lib
 from .models import kernel, rel2abs
 
 
-def build_dlr_rf(lam, eps):
-    """DLR real frequencies for cutoff ``lam`` = beta * w_max and accuracy ``eps`` (ascending)."""
+@functools.lru_cache(maxsize=64)
+def _dlr_rf_cached(lam, eps):
     L = _lib.lib()
     buf = np.zeros(4096)
     r = ctypes.c_int(0)
-    _lib.check(L.xca_dlr_build_rf(float(lam), float(eps), _lib.as_dp(buf), len(buf), ctypes.byref(r)))
-    return buf[: r.value].copy()
+    _lib.check(L.xca_dlr_build_rf(lam, eps, _lib.as_dp(buf), len(buf), ctypes.byref(r)))
+    out = buf[: r.value].copy()
+    out.setflags(write=False)
+    return out
+
+
+def build_dlr_rf(lam, eps):
+    """DLR real frequencies for cutoff ``lam`` = beta * w_max and accuracy ``eps`` (ascending).  The node
+    selection is computed once per (lam, eps) in a process (a served stream repeats them)."""
+    return _dlr_rf_cached(float(lam), float(eps)).copy()
+
+
+@functools.lru_cache(maxsize=64)
+def _dlr_it_cached(lam, rf_bytes):
+    rf = np.frombuffer(rf_bytes, dtype=float).copy()
+    it = np.zeros(len(rf))
+    _lib.check(_lib.lib().xca_dlr_build_it(lam, _lib.as_dp(rf), len(rf), _lib.as_dp(it)))
+    it.setflags(write=False)
+    return it
 
 
 class ImTimeOps:
@@ -33,8 +51,7 @@ class ImTimeOps:
             raise NotImplementedError("symmetrized DLR nodes are not supported")
         self._lam = float(lam)
         self.rf = np.ascontiguousarray(dlr_rf, dtype=float)
-        self.it = np.zeros(len(self.rf))
-        _lib.check(_lib.lib().xca_dlr_build_it(self._lam, _lib.as_dp(self.rf), len(self.rf), _lib.as_dp(self.it)))
+        self.it = _dlr_it_cached(self._lam, self.rf.tobytes()).copy()
 
     def rank(self):
         return len(self.rf)

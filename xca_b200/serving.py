@@ -2,11 +2,20 @@
 
 Requests (a local problem, its hybridization and the solve parameters of BlockSparseSolver.solve,
 ``python/triqs_xca/block_sparse_solver.py:240-355``) arrive at any time.  The server admits a request
-when its device-memory footprint fits into what the running solves leave of the budget, runs every
-admitted solve in its own worker thread with its own evaluator context — its own CUDA stream, its G, Σ
-and Dyson state resident on the device for the whole solve — so that the device work of concurrent
-solves overlaps, and completes a future with the converged result and its timings (queue wait, time to
-converged solve).  Solves never share device state, so a result does not depend on what else runs.
+when its device-memory footprint fits into what the running solves leave of the budget and completes a
+future with the converged result and its timings (queue wait, time to converged solve).  Every admitted
+solve has its own evaluator context — its own CUDA stream, its G, Σ and Dyson state resident on the
+device for the whole solve — so a result does not depend on what else runs (up to the summation order
+of the Σ items).  Two ways to run them:
+
+- threads (``batched=False``): each solve iterates in its own worker thread; the device work of
+  concurrent solves overlaps through their streams;
+- lock step (``batched=True``): one scheduler thread runs an iteration of every live solve at a time,
+  the Σ of all of them (every topology of every solve, grouped by padded DLR rank) in ONE job-batched
+  launch (``DiagramEvaluator.compute_self_energy_device_batch``), then their Dyson solves, then their
+  normalisations and convergence tests.  Set-up (hybridization fit, evaluator) and the final
+  single-particle Green's function run in helper threads beside it; a solve joins the next iteration
+  when its set-up is done and leaves when it converges.
 """
 
 import threading
@@ -16,6 +25,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from .block_sparse import DiagramEvaluator
 from .block_sparse_solver import BlockSparseSolver
 
 
@@ -66,21 +76,41 @@ def footprint_bytes(atom_diag, r, n_poles, max_order=3):
     return 8 * (12 * slab + tables + mats + ops + 6 * slab) + (64 << 20)
 
 
-class SolveServer:
-    """Admits solve requests by device-memory budget and runs up to ``max_concurrent`` at a time."""
+@dataclass
+class _Live:
+    """A solve of the lock-step scheduler."""
+    req: SolveRequest
+    fut: Future
+    t_submit: float
+    t_start: float
+    need: int
+    solver: BlockSparseSolver
+    it: int = 0
 
-    def __init__(self, max_concurrent=8, hbm_budget=48 << 30, device=0):
+
+class SolveServer:
+    """Admits solve requests by device-memory budget and runs up to ``max_concurrent`` at a time, each in
+    its own thread or (``batched``) all in lock step with one Σ launch per iteration."""
+
+    def __init__(self, max_concurrent=8, hbm_budget=48 << 30, device=0, batched=False):
         self.max_concurrent = max_concurrent
         self.budget = int(hbm_budget)
         self.device = device
+        self.batched = bool(batched)
         self._used = 0
         self._running = 0
         self._cv = threading.Condition()
         self._queue = []
         self._threads = []
+        self._arrived = []  # set up, waiting for the next lock-step iteration
         self._closed = False
+        self.iterations = 0  # lock-step iterations run (batched)
         self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
         self._dispatcher.start()
+        self._stepper = None
+        if self.batched:
+            self._stepper = threading.Thread(target=self._step_loop, daemon=True)
+            self._stepper.start()
 
     def submit(self, req: SolveRequest) -> Future:
         fut = Future()
@@ -96,7 +126,9 @@ class SolveServer:
             self._closed = True
             self._cv.notify_all()
         self._dispatcher.join()
-        for t in self._threads:
+        if self._stepper is not None:
+            self._stepper.join()
+        for t in list(self._threads):
             t.join()
 
     def _dispatch(self):
@@ -118,7 +150,7 @@ class SolveServer:
                             self._running += 1
                             break
                     self._cv.wait()
-            th = threading.Thread(target=self._run, args=(req, fut, t_sub, need), daemon=True)
+            th = threading.Thread(target=self._setup if self.batched else self._run, args=(req, fut, t_sub, need), daemon=True)
             self._threads.append(th)
             th.start()
 
@@ -142,10 +174,96 @@ class SolveServer:
         except BaseException as e:  # the future carries the failure to the caller
             fut.set_exception(e)
         finally:
+            self._release(need)
+
+    def _release(self, need):
+        with self._cv:
+            self._used -= need
+            self._running -= 1
+            self._cv.notify_all()
+
+    # ---------------------------------------------------------------- lock step (batched=True)
+    def _setup(self, req, fut, t_sub, need):
+        t_start = time.perf_counter()
+        try:
+            S = BlockSparseSolver(req.atom_diag, req.beta, req.w_max, req.eps, device=self.device)
+            if S.Delta_tau.shape != req.delta_tau.shape:
+                raise ValueError(f"delta_tau has shape {req.delta_tau.shape}, the DLR mesh needs {S.Delta_tau.shape}")
+            S.Delta_tau = np.asarray(req.delta_tau, dtype=np.complex128)
+            S.begin(req.max_order, tol=req.tol)
+            S.d.synchronize()
+        except BaseException as e:
+            fut.set_exception(e)
+            self._release(need)
+            return
+        with self._cv:
+            self._arrived.append(_Live(req, fut, t_sub, t_start, need, S))
+            self._cv.notify_all()
+
+    def _step_loop(self):
+        live = []
+        while True:
             with self._cv:
-                self._used -= need
-                self._running -= 1
-                self._cv.notify_all()
+                while not live and not self._arrived:
+                    if self._closed and self._running == 0 and not self._queue:
+                        return
+                    self._cv.wait()
+                live.extend(self._arrived)
+                self._arrived.clear()
+            self._iterate(live)
+            self.iterations += 1
+
+    def _fail(self, live, L, e):
+        live.remove(L)
+        L.solver = None
+        L.fut.set_exception(e)
+        self._release(L.need)
+
+    def _iterate(self, live):
+        """One iteration of every live solve: their Σ in one launch per padded rank, Dyson solves queued on every
+        stream, then normalisation and convergence test per solve; converged solves leave for a finisher."""
+        groups = {}
+        for L in live:
+            groups.setdefault(L.solver.d.padded_rank, []).append(L)
+        for grp in groups.values():
+            try:
+                jobs = []
+                for L in grp:
+                    jobs += L.solver.sigma_jobs(L.req.max_order)
+                DiagramEvaluator.compute_self_energy_device_batch(jobs)
+            except BaseException as e:
+                for L in grp:
+                    self._fail(live, L, e)
+        for L in list(live):
+            try:
+                L.solver.launch_dyson()
+            except BaseException as e:
+                self._fail(live, L, e)
+        for L in list(live):
+            L.it += 1
+            try:
+                done = L.solver.end_iteration(L.it, L.req.tol, L.req.mix, dyson_launched=True) or L.it >= L.req.maxiter
+            except BaseException as e:
+                self._fail(live, L, e)
+                continue
+            if done:
+                live.remove(L)
+                th = threading.Thread(target=self._finish, args=(L,), daemon=True)
+                self._threads.append(th)
+                th.start()
+
+    def _finish(self, L):
+        try:
+            S = L.solver.finish()
+            L.solver = None
+            res = SolveResult(L.req.tag, S.G, S.Sigma, S.eta, S.G_tau, S.n_ppsc_iter, S.diff_G, L.t_submit, L.t_start,
+                              time.perf_counter(), {"footprint_bytes": L.need, "batched": True})
+            del S
+            L.fut.set_result(res)
+        except BaseException as e:
+            L.fut.set_exception(e)
+        finally:
+            self._release(L.need)
 
 
 def synthetic_request(kind, beta, U, order, eps=1e-10, tol=1e-8, maxiter=100, tag=None):
