@@ -65,6 +65,47 @@ struct DevBuf {
   }
 };
 
+// Host-to-device copies of per-call descriptor lists through pinned staging memory: two areas used in turn,
+// each refilled only after its previous copy completed, so a copy never waits for the work queued on the
+// stream before it (a copy from pageable memory may).  An unchanged list is not copied again.
+struct StagedUpload {
+  void *host[2] = {nullptr, nullptr};
+  size_t cap[2] = {0, 0};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+  int next = 0;
+  std::vector<unsigned char> last;  // the bytes of the last copy
+  const void *last_dst = nullptr;
+  void copy(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return;
+    if (dst == last_dst && last.size() == bytes && std::memcmp(last.data(), src, bytes) == 0) return;
+    const int k = next;
+    next ^= 1;
+    if (done[k]) CUDA_CHECK(cudaEventSynchronize(done[k]));
+    else CUDA_CHECK(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+    if (cap[k] < bytes) {
+      if (host[k]) cudaFreeHost(host[k]);
+      host[k] = nullptr;
+      cap[k] = 0;
+      CUDA_CHECK(cudaMallocHost(&host[k], bytes + bytes / 2));
+      cap[k] = bytes + bytes / 2;
+    }
+    std::memcpy(host[k], src, bytes);
+    CUDA_CHECK(cudaMemcpyAsync(dst, host[k], bytes, cudaMemcpyHostToDevice, s));
+    CUDA_CHECK(cudaEventRecord(done[k], s));
+    last.assign(static_cast<const unsigned char *>(src), static_cast<const unsigned char *>(src) + bytes);
+    last_dst = dst;
+  }
+  ~StagedUpload() {
+    for (int k = 0; k < 2; ++k) {
+      if (done[k]) {
+        cudaEventSynchronize(done[k]);
+        cudaEventDestroy(done[k]);
+      }
+      if (host[k]) cudaFreeHost(host[k]);
+    }
+  }
+};
+
 // -------------------------------------------------------------------------------- small kernels
 __global__ void block_maxabs_kernel(const double *G, const long *goff, const int *dims, int r, int nb, double *out) {
   int b = blockIdx.x;
@@ -276,6 +317,7 @@ struct Ctx {
   std::vector<WorkUnit> h_batch_units;
   DevBuf<SigmaJob> d_batch_jobs;
   DevBuf<WorkUnit> d_batch_units;
+  StagedUpload stage_jobs, stage_units;
   DevBuf<int> d_batch_counter;
   cudaEvent_t ev_batch = nullptr;  // orders this context's stream against a batch led by another context
   int unit_batches = 4;      // panel batches per work unit (tunable, XCA_TUNE_UNIT_BATCHES)
@@ -304,6 +346,7 @@ struct Ctx {
 
   DevBasis basis(int nsig) const {
     DevBasis B;
+    std::memset(&B, 0, sizeof B);  // padding too: job descriptors are compared byte for byte
     B.r = r; B.p = p; B.n = n; B.nb = nb; B.nq = nq; B.beta = beta;
     B.LUp = d_LUp.ptr; B.perm = d_perm.ptr; B.pinv = d_pinv.ptr; B.Wp = d_Wp.ptr; B.BKp = d_BKp.ptr; B.tabs = d_tabs.ptr; B.k0 = d_k0.ptr;
     B.tab = d_tab.ptr; B.tab_off = nsig == nsig_alloc ? d_tab_off.ptr : d_tab_off_small.ptr; B.nsig = nsig;
@@ -1519,6 +1562,7 @@ int xca_compute_self_energy_device_batch(int n_jobs, xca_ctx *const *ctxs, const
   for (int j = 0; j < n_jobs; ++j) {
     const Prep &pr = preps[prep_of[j]];
     SigmaJob &J = c0->h_batch_jobs[j];
+    std::memset(&J, 0, sizeof J);
     J.B = pr.c->basis(pr.nsig);
     J.B.gmax = pr.gmax;
     J.classes = sets[j]->d_classes.ptr;
@@ -1530,8 +1574,12 @@ int xca_compute_self_energy_device_batch(int n_jobs, xca_ctx *const *ctxs, const
     }
   }
   if (!c0->h_batch_units.empty()) {
-    c0->d_batch_jobs.upload(c0->h_batch_jobs, c0->stream);
-    c0->d_batch_units.upload(c0->h_batch_units, c0->stream);
+    // device lists with headroom, so that a stream of slightly growing batches does not reallocate each time
+    const size_t nj = c0->h_batch_jobs.size(), nu_ = c0->h_batch_units.size();
+    if (nj > c0->d_batch_jobs.n) c0->d_batch_jobs.resize(nj + nj / 2);
+    if (nu_ > c0->d_batch_units.n) c0->d_batch_units.resize(nu_ + nu_ / 2);
+    c0->stage_jobs.copy(c0->d_batch_jobs.ptr, c0->h_batch_jobs.data(), nj * sizeof(SigmaJob), c0->stream);
+    c0->stage_units.copy(c0->d_batch_units.ptr, c0->h_batch_units.data(), nu_ * sizeof(WorkUnit), c0->stream);
     c0->d_batch_counter.resize(1);
     const int nu = (int)c0->h_batch_units.size();
     switch (c0->RP) {

@@ -8,14 +8,14 @@ solve has its own evaluator context — its own CUDA stream, its G, Σ and Dyson
 device for the whole solve — so a result does not depend on what else runs (up to the summation order
 of the Σ items).  Two ways to run them:
 
-- threads (``batched=False``): each solve iterates in its own worker thread; the device work of
-  concurrent solves overlaps through their streams;
-- lock step (``batched=True``): one scheduler thread runs an iteration of every live solve at a time,
+- lock step (``batched=True``, the default): one scheduler thread runs an iteration of every live solve at a time,
   the Σ of all of them (every topology of every solve, grouped by padded DLR rank) in ONE job-batched
   launch (``DiagramEvaluator.compute_self_energy_device_batch``), then their Dyson solves, then their
   normalisations and convergence tests.  Set-up (hybridization fit, evaluator) and the final
   single-particle Green's function run in helper threads beside it; a solve joins the next iteration
-  when its set-up is done and leaves when it converges.
+  when its set-up is done and leaves when it converges;
+- threads (``batched=False``): each solve iterates in its own worker thread; the device work of
+  concurrent solves overlaps through their streams.
 """
 
 import threading
@@ -92,7 +92,7 @@ class SolveServer:
     """Admits solve requests by device-memory budget and runs up to ``max_concurrent`` at a time, each in
     its own thread or (``batched``) all in lock step with one Σ launch per iteration."""
 
-    def __init__(self, max_concurrent=8, hbm_budget=48 << 30, device=0, batched=False):
+    def __init__(self, max_concurrent=8, hbm_budget=48 << 30, device=0, batched=True):
         self.max_concurrent = max_concurrent
         self.budget = int(hbm_budget)
         self.device = device
