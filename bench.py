@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end host-API measurement (profiling runs)")
     ap.add_argument("--serving", action="store_true",
                     help="instead of the Sigma metric: a Poisson stream of whole self-consistent solves through the solve server")
-    ap.add_argument("--serving-requests", type=int, default=64)
+    ap.add_argument("--serving-requests", type=int, default=256)
     ap.add_argument("--no-serving", action="store_true", help="skip the served-solves measurement of the default line")
     ap.add_argument("--dshell", action="store_true",
                     help="instead of the Sigma metric: OCA Sigma of the five-orbital d shell (wide-chain kernel)")
@@ -174,23 +174,26 @@ def cpu_baseline_object(seconds):
 
 def run_serving(args, batched=False):
     """Served solves/s and p50 / p99 time to converged solve for a mixed request stream: Poisson arrivals
-    (mean gap 5 ms, numpy default_rng(2)); each request draws a single-orbital Anderson (orders 1-3) or a
-    two-orbital Kanamori model (orders 1-2), beta in {10, 20, 50, 100}, Lambda = 10 beta, eps = 1e-10,
-    U ~ U(1, 6), tolerance 1e-8; up to 8 solves run concurrently, each with its own context and stream,
-    in worker threads or (``batched``) in lock step with one Sigma launch per iteration for all of them."""
-    from xca_b200.serving import SolveServer, synthetic_request
+    (mean gap 5 ms, numpy default_rng(2)); each request draws a model family (single-orbital Anderson,
+    two-orbital Kanamori, three-orbital t2g with its 8-pole off-diagonal bath), beta in {10, 20, 50, 100},
+    Lambda = 10 beta, U ~ U(1, 6), an order in {NCA, OCA, TCA} (t2g: NCA, OCA) and tolerance 1e-8, at most
+    100 iterations, the hybridization compressed as the reference's solve does by default.  Up to 8 solves
+    run concurrently, each with its own context and stream, in lock step with one Sigma launch per iteration
+    for all of them (``batched``) or in worker threads."""
+    from xca_b200.serving import SolveServer, STREAM_EPS, synthetic_request
     rng = np.random.default_rng(2)
     n = args.serving_requests
     gaps = rng.exponential(0.005, n)
+    kinds = ("anderson", "kanamori", "t2g")
     reqs = []
     for i in range(n):
-        kind = "anderson" if rng.random() < 0.5 else "kanamori"
+        kind = kinds[int(rng.integers(0, 3))]
         beta = float(rng.choice([10.0, 20.0, 50.0, 100.0]))
         U = float(rng.uniform(1.0, 6.0))
-        order = int(rng.integers(1, 4)) if kind == "anderson" else int(rng.integers(1, 3))
+        order = int(rng.integers(1, 3 if kind == "t2g" else 4))
         reqs.append(synthetic_request(kind, beta, U, order, tag=(kind, beta, order)))
     srv = SolveServer(max_concurrent=8, batched=batched)
-    for kind, order in (("anderson", 3), ("kanamori", 2)):  # warm-up: module load and first-use set-up
+    for kind, order in (("anderson", 3), ("kanamori", 3), ("t2g", 2)):  # warm-up: module load and first-use set-up
         srv.submit(synthetic_request(kind, 10.0, 2.0, order)).result()
     t0 = time.perf_counter()
     futs = []
@@ -209,7 +212,10 @@ def run_serving(args, batched=False):
            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
            "config": {"workload": "poisson_stream", "requests": n, "mean_gap_ms": 5.0, "max_concurrent": 8,
                       "mode": "lock step, one batched Sigma launch per iteration" if batched else "worker threads",
-                      "models": "anderson orders 1-3, kanamori_2orb orders 1-2", "beta": [10, 20, 50, 100], "tol": 1e-8},
+                      "models": "anderson, kanamori_2orb, t2g_3orb (U ~ U(1, 6))", "orders": "1-3; t2g 1-2",
+                      "t2g_tca_excluded": "a t2g TCA solve alone takes 41-172 s (0.45 s per iteration, up to 100 iterations)",
+                      "beta": [10, 20, 50, 100], "lambda": "10 beta", "eps": STREAM_EPS, "tol": 1e-8, "maxiter": 100,
+                      "hyb_comp": True},
            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
            "mean_iterations": float(np.mean([r.n_iter for r in res])),
            "converged": int(sum(r.diff_G < 1e-8 for r in res)), "wall_s": t1 - t0}

@@ -131,7 +131,7 @@ def test_anderson_self_consistent_solve_vs_oracle(max_order):
     delta[:, 0, 0] = dv
     delta[:, 1, 1] = dv
     S.Delta_tau = delta
-    S.solve(max_order=max_order, tol=1e-10, maxiter=60, mix=1.0)
+    S.solve(max_order=max_order, tol=1e-10, maxiter=60, mix=1.0, hyb_comp=False)
 
     d = O.Dlr(lam, eps, rf=S.rf, it=S.it)
     ev = O.Evaluator(d, beta, S.hyb_poles, S.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
@@ -158,7 +158,7 @@ def test_t2g_nca_solve_vs_oracle():
     S = BlockSparseSolver(m.ad, beta, lam / beta, eps)
     rf, it = S.rf, S.it
     S.Delta_tau = np.asarray(models.kernel(it[:, None], rf[None, :]) @ m.hyb_coeffs.reshape(len(rf), -1)).reshape(S.Delta_tau.shape)
-    S.solve(max_order=1, tol=1e-8, maxiter=40, mix=1.0)
+    S.solve(max_order=1, tol=1e-8, maxiter=40, mix=1.0, hyb_comp=False)
     d = O.Dlr(lam, eps, rf=rf, it=it)
     ev = O.Evaluator(d, beta, S.hyb_poles, S.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
     G, Sig, eta, g, n_iter, diff = O.solve(d, ev, beta, m.G0, 1, 1e-8, 40, mix=1.0, spgf_max_order=1)

@@ -149,9 +149,9 @@ def _max_diff(A, B):
 def test_anderson_nca_then_oca_ordered_vs_oracle():
     # the single-orbital Anderson solve as written: NCA to 1e-10, then OCA from the NCA solution
     S, m, d, beta = _anderson_solver("fp64_ordered")
-    S.solve(max_order=1, tol=1e-10, maxiter=60)
+    S.solve(max_order=1, tol=1e-10, maxiter=60, hyb_comp=False)
     n1 = S.n_ppsc_iter
-    S.solve(max_order=2, tol=1e-10, maxiter=60)
+    S.solve(max_order=2, tol=1e-10, maxiter=60, hyb_comp=False)
     ev = _oracle_eval(d, m, S, beta)
     G1, _, e1, _, it1, _ = O.solve(d, ev, beta, m.G0, 1, 1e-10, 60, spgf_max_order=0, ordered=True)
     G, Sig, eta, g, it2, diff = O.solve(d, ev, beta, m.G0, 2, 1e-10, 60, spgf_max_order=2, ordered=True, G_init=G1, eta_init=e1)
@@ -167,7 +167,7 @@ def test_anderson_nca_then_oca_ordered_vs_oracle():
 
 def test_anderson_tca_solve_ordered_vs_oracle():
     S, m, d, beta = _anderson_solver("fp64_ordered")
-    S.solve(max_order=3, tol=1e-10, maxiter=60)
+    S.solve(max_order=3, tol=1e-10, maxiter=60, hyb_comp=False)
     ev = _oracle_eval(d, m, S, beta)
     G, Sig, eta, g, n_iter, diff = O.solve(d, ev, beta, m.G0, 3, 1e-10, 60, spgf_max_order=3, ordered=True)
     print(f"TCA: iterations device {S.n_ppsc_iter}, oracle {n_iter}; |dG| {_max_diff(S.G, G):.2e}, "
@@ -188,7 +188,7 @@ def test_t2g_nca_solve_ordered_vs_oracle():
     S = BlockSparseSolver(m.ad, beta, lam / beta, eps, precision="fp64_ordered")
     rf, it = S.rf, S.it
     S.Delta_tau = np.asarray(models.kernel(it[:, None], rf[None, :]) @ m.hyb_coeffs.reshape(len(rf), -1)).reshape(S.Delta_tau.shape)
-    S.solve(max_order=1, tol=1e-8, maxiter=40)
+    S.solve(max_order=1, tol=1e-8, maxiter=40, hyb_comp=False)
     d = O.Dlr(lam, eps, rf=rf, it=it)
     ev = O.Evaluator(d, beta, S.hyb_poles, S.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
     G, Sig, eta, g, n_iter, diff = O.solve(d, ev, beta, m.G0, 1, 1e-8, 40, spgf_max_order=1, ordered=True)

@@ -38,7 +38,7 @@ def _max_diff(A, B):
 @pytest.mark.parametrize("normalization", ["root", "ode+classic", "ode+root"])
 def test_normalization_variant_vs_oracle(normalization):
     S, m = _solver()
-    S.solve(max_order=2, tol=1e-8, maxiter=40, normalization=normalization)
+    S.solve(max_order=2, tol=1e-8, maxiter=40, normalization=normalization, hyb_comp=False)
     d = O.Dlr(LAM, EPS, rf=S.rf, it=S.it)
     ev = O.Evaluator(d, BETA, S.hyb_poles, S.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
     G, Sig, eta, g, n_iter, diff = O.solve(d, ev, BETA, m.G0, 2, 1e-8, 40, spgf_max_order=2, ordered=True, normalization=normalization,
@@ -59,7 +59,7 @@ def test_normalizations_agree():
     gs = {}
     for normalization in ("classic", "root", "ode+classic", "ode+root"):
         S, _ = _solver("fp64")
-        S.solve(max_order=1, tol=1e-4, maxiter=40, normalization=normalization)
+        S.solve(max_order=1, tol=1e-4, maxiter=40, normalization=normalization, hyb_comp=False)
         assert S.diff_G < 1e-4
         gs[normalization] = S.G_tau
     for k, g in gs.items():
@@ -70,12 +70,12 @@ def test_state_save_load_resume(tmp_path):
     # NCA, save, load into a new solver, then OCA: the same as NCA then OCA without the round trip
     from xca_b200.block_sparse_solver import BlockSparseSolver
     S, _ = _solver()
-    S.solve(max_order=1, tol=1e-10, maxiter=60)
+    S.solve(max_order=1, tol=1e-10, maxiter=60, hyb_comp=False)
     path = str(tmp_path / "state.npz")
     S.save(path)
     R = BlockSparseSolver.load(path)
     assert R == S
-    S.solve(max_order=2, tol=1e-10, maxiter=60)
-    R.solve(max_order=2, tol=1e-10, maxiter=60)
+    S.solve(max_order=2, tol=1e-10, maxiter=60, hyb_comp=False)
+    R.solve(max_order=2, tol=1e-10, maxiter=60, hyb_comp=False)
     assert R.n_ppsc_iter == S.n_ppsc_iter
     assert _max_diff(R.G, S.G) == 0.0 and R.eta == S.eta

@@ -111,7 +111,7 @@ class BlockSparseSolver:
             for _, G, topo, fac, S in jobs:
                 self.d.compute_self_energy_device(G, topo, fac, S)
 
-    def begin(self, max_order, tol=1e-4, hyb_tol=None, hyb_comp=False, normalization="classic", spgf_max_order=None):
+    def begin(self, max_order, tol=1e-4, hyb_tol=None, hyb_comp=True, normalization="classic", spgf_max_order=None):
         """The set-up of solve (block_sparse_solver.py:240-300): hybridization fit, evaluator, G on the device."""
         if normalization not in NORMALIZATIONS:
             raise NotImplementedError(f"normalization {normalization!r} is not available on the device path "
@@ -165,9 +165,10 @@ class BlockSparseSolver:
             self.G_tau = self.eval_single_particle_greens_function(self.G, self.spgf_max_order)
         return self
 
-    def solve(self, max_order, tol=1e-4, maxiter=10, mix=1.0, hyb_tol=None, hyb_comp=False, normalization="classic",
+    def solve(self, max_order, tol=1e-4, maxiter=10, mix=1.0, hyb_tol=None, hyb_comp=True, normalization="classic",
               spgf_max_order=None, verbose=None):
-        """BlockSparseSolver.solve (block_sparse_solver.py:240-355)."""
+        """BlockSparseSolver.solve (block_sparse_solver.py:240-355), with its defaults: the hybridization is
+        compressed to a few poles (hyb_comp=True, tolerance hyb_tol = 0.1 tol) for orders above NCA."""
         verbose = self.verbose if verbose is None else verbose
         self.begin(max_order, tol, hyb_tol, hyb_comp, normalization, spgf_max_order)
         t0 = time.perf_counter()

@@ -201,7 +201,8 @@ def t2g_3orb(rf, it, beta=50.0, lam=500.0, eps=1e-10, U=3.0, J=0.3, seed=1, n_ba
         vv = np.outer(V[k], V[k])
         for s in range(2):
             delta[:, 3 * s:3 * s + 3, 3 * s:3 * s + 3] += kt[:, None, None] * vv[None]
-    return _finish("t2g_3orb", beta, lam, eps, 6, ad, rf, it, delta_vals=delta, extra={"mu": mu, "bath_w": w, "bath_V": V})
+    return _finish("t2g_3orb", beta, lam, eps, 6, ad, rf, it, delta_vals=delta,
+                   extra={"mu": mu, "bath_w": w, "bath_V": V, "delta": delta})
 
 
 def seeded_G(model, seed=0):

@@ -40,6 +40,7 @@ class SolveRequest:
     tol: float = 1e-8
     maxiter: int = 100
     mix: float = 1.0
+    hyb_comp: bool = True        # compress the hybridization to a few poles (the reference's default)
     tag: object = None
 
 
@@ -166,7 +167,7 @@ class SolveServer:
             if S.Delta_tau.shape != req.delta_tau.shape:
                 raise ValueError(f"delta_tau has shape {req.delta_tau.shape}, the DLR mesh needs {S.Delta_tau.shape}")
             S.Delta_tau = np.asarray(req.delta_tau, dtype=np.complex128)
-            S.solve(max_order=req.max_order, tol=req.tol, maxiter=req.maxiter, mix=req.mix)
+            S.solve(max_order=req.max_order, tol=req.tol, maxiter=req.maxiter, mix=req.mix, hyb_comp=req.hyb_comp)
             res = SolveResult(req.tag, S.G, S.Sigma, S.eta, S.G_tau, S.n_ppsc_iter, S.diff_G, t_sub, t_start,
                               time.perf_counter(), {"footprint_bytes": need})
             del S
@@ -190,7 +191,7 @@ class SolveServer:
             if S.Delta_tau.shape != req.delta_tau.shape:
                 raise ValueError(f"delta_tau has shape {req.delta_tau.shape}, the DLR mesh needs {S.Delta_tau.shape}")
             S.Delta_tau = np.asarray(req.delta_tau, dtype=np.complex128)
-            S.begin(req.max_order, tol=req.tol)
+            S.begin(req.max_order, tol=req.tol, hyb_comp=req.hyb_comp)
             S.d.synchronize()
         except BaseException as e:
             fut.set_exception(e)
@@ -266,19 +267,33 @@ class SolveServer:
             self._release(L.need)
 
 
-def synthetic_request(kind, beta, U, order, eps=1e-10, tol=1e-8, maxiter=100, tag=None):
-    """A request of the mixed serving stream: single-orbital Anderson or two-orbital Kanamori (J = U / 8)
-    at half filling with a Bethe hybridization (t = 1), Lambda = 10 beta (w_max = 10)."""
+# DLR accuracy of each model family of the served stream (the accuracy its single-solve configuration uses)
+STREAM_EPS = {"anderson": 1e-10, "kanamori": 1e-12, "t2g": 1e-10}
+
+
+def synthetic_request(kind, beta, U, order, eps=None, tol=1e-8, maxiter=100, tag=None, hyb_comp=True):
+    """A request of the mixed serving stream, Lambda = 10 beta (w_max = 10), at half filling:
+    'anderson': single-orbital Anderson with a Bethe hybridization (t = 1);
+    'kanamori': two-orbital Kanamori (J = U / 8) with a diagonal Bethe hybridization;
+    't2g': three-orbital t2g Kanamori (J = U / 10) with the off-diagonal 8-pole bath of numpy default_rng(1)
+    (poles w_k ~ U(-2, 2), weights V_k V_k^T, V_k ~ N(0, 0.3^2)).  eps defaults to STREAM_EPS[kind]."""
     from . import models
     from .pycppdlr import MeshDLRImTime
+    eps = STREAM_EPS[kind] if eps is None else eps
     mesh = MeshDLRImTime(beta=beta, statistic="Fermion", w_max=10.0, eps=eps)
     rf, it = mesh.dlr_rf, mesh.dlr_it.it
-    if kind == "anderson":
-        m = models.anderson(rf, it, beta, 10.0 * beta, eps, U=U, mu=U / 2)
+    if kind == "t2g":
+        m = models.t2g_3orb(rf, it, beta, 10.0 * beta, eps, U=U, J=U / 10)
+        delta = np.asarray(m.extra["delta"], np.complex128)
     else:
-        m = models.kanamori_diag_bethe(rf, it, 2, beta, 10.0 * beta, eps, U, U / 8, "kanamori_2orb")
-    delta = np.zeros((len(rf), m.n, m.n), np.complex128)
-    dv = models.bethe_delta(beta, it)
-    for i in range(m.n):
-        delta[:, i, i] = dv
-    return SolveRequest(m.ad, beta, 10.0, eps, delta, max_order=order, tol=tol, maxiter=maxiter, tag=tag)
+        if kind == "anderson":
+            m = models.anderson(rf, it, beta, 10.0 * beta, eps, U=U, mu=U / 2)
+        elif kind == "kanamori":
+            m = models.kanamori_diag_bethe(rf, it, 2, beta, 10.0 * beta, eps, U, U / 8, "kanamori_2orb")
+        else:
+            raise ValueError(f"unknown model family {kind!r}")
+        delta = np.zeros((len(rf), m.n, m.n), np.complex128)
+        dv = models.bethe_delta(beta, it)
+        for i in range(m.n):
+            delta[:, i, i] = dv
+    return SolveRequest(m.ad, beta, 10.0, eps, delta, max_order=order, tol=tol, maxiter=maxiter, hyb_comp=hyb_comp, tag=tag)
