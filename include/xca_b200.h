@@ -273,11 +273,15 @@ int xca_get_precision_mode(xca_ctx *ctx, int *mode);
  * the autotuner, xca_b200/autotune.py).  XCA_TUNE_UNIT_BATCHES: panel batches per work unit of the panel
  * kernel (1..64, default 4); XCA_TUNE_WIDE_UNIT_TUPLES: pole tuples per work unit of the wide-chain kernel
  * (1..1024, default 4); XCA_TUNE_WIDE_CTAS_PER_SM: resident CTAs per SM of the wide-chain kernel (1..8,
- * default 2).  The results do not depend on them in XCA_PREC_FP64_ORDERED; in XCA_PREC_FP64 they change only
- * the order of the atomic additions.  Out-of-range values give XCA_ERR_INVALID. */
+ * default 2); XCA_TUNE_DYSON_BLOCKED_MIN_N: the Dyson solve factorises every block with the multi-CTA blocked
+ * LU when the largest system N = r d_b exceeds it, else with one CTA per block (0..2^30; the results are
+ * identical bit for bit either way).  The Sigma results do not depend on them in XCA_PREC_FP64_ORDERED; in
+ * XCA_PREC_FP64 they change only the order of the atomic additions.  Out-of-range values give
+ * XCA_ERR_INVALID. */
 #define XCA_TUNE_UNIT_BATCHES 0
 #define XCA_TUNE_WIDE_UNIT_TUPLES 1
 #define XCA_TUNE_WIDE_CTAS_PER_SM 2
+#define XCA_TUNE_DYSON_BLOCKED_MIN_N 3
 int xca_set_tuning(xca_ctx *ctx, int param, int value);
 int xca_get_tuning(xca_ctx *ctx, int param, int *value);
 

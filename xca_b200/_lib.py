@@ -23,7 +23,7 @@ XCA_ORDERED_UNIT_TUPLES = 64
 PRECISION_MODES = {"fp64": XCA_PREC_FP64, "fp64_ordered": XCA_PREC_FP64_ORDERED}
 
 # launch-shape parameters (xca_set_tuning)
-TUNING = {"unit_batches": 0, "wide_unit_tuples": 1, "wide_ctas_per_sm": 2}
+TUNING = {"unit_batches": 0, "wide_unit_tuples": 1, "wide_ctas_per_sm": 2, "dyson_blocked_min_n": 3}
 
 _lib = None
 

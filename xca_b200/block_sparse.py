@@ -295,7 +295,7 @@ class DiagramEvaluator:
         _lib.check(_lib.lib().xca_set_precision_mode(self._ctx, _lib.PRECISION_MODES[mode]))
 
     def set_tuning(self, **params):
-        """Launch-shape parameters of the Sigma kernels (unit_batches, wide_unit_tuples, wide_ctas_per_sm)."""
+        """Launch-shape parameters (unit_batches, wide_unit_tuples, wide_ctas_per_sm of the Sigma kernels; dyson_blocked_min_n of the Dyson solve)."""
         for k, v in params.items():
             if k not in _lib.TUNING:
                 raise ValueError(f"unknown tuning parameter {k!r} ({sorted(_lib.TUNING)})")

@@ -69,7 +69,7 @@ static int launch_blocked_lu(cudaStream_t s, const DysonBasis &B, int n_max, int
 
 template <int RP>
 int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const double *Sigma, double eta, int hermitize, double *rhs,
-                 double *G, int *status, int n_max, int d_max) {
+                 double *G, int *status, int n_max, int d_max, int blocked_min_n) {
   const size_t sm = (2 * (size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
   if (cudaFuncSetAttribute(dyson_coef_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
     check_launch("dyson_coef_kernel attributes");
@@ -78,7 +78,7 @@ int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const do
   dim3 grid((unsigned)((n_conv_rows + 63) / 64), (unsigned)B.nb);
   dyson_convmat_kernel<RP><<<grid, 64, 0, s>>>(B);
   check_launch("dyson_convmat_kernel");
-  if (n_max > DYSON_BLOCKED_MIN_N) return 2 + launch_blocked_lu(s, B, n_max, d_max, rhs, G, hermitize, status);
+  if (n_max > blocked_min_n) return 2 + launch_blocked_lu(s, B, n_max, d_max, rhs, G, hermitize, status);
   dyson_lu_solve_kernel<<<B.nb, 1024, 0, s>>>(B, rhs, G, hermitize, status);
   check_launch("dyson_lu_solve_kernel");
   return 3;
@@ -135,11 +135,11 @@ int launch_axpby(cudaStream_t s, double alpha, const double *x, double beta, dou
 }
 
 template int launch_dyson<32>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *, int,
-                               int);
+                               int, int);
 template int launch_dyson<48>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *, int,
-                               int);
+                               int, int);
 template int launch_dyson<64>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *, int,
-                               int);
+                               int, int);
 template int launch_convolve_ppsc<32>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);
 template int launch_convolve_ppsc<48>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);
 template int launch_convolve_ppsc<64>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);

@@ -306,7 +306,9 @@ __global__ void __launch_bounds__(128) trace_beta_kernel(DysonBasis B, const dou
   __syncthreads();
   const int r = B.r, d = B.dims[b], dd = d * d;
   const double *g = G + B.goff[b];
-  double s = 0.0;
+  // the thread's partial sum lives in shared memory: a register carried across the loop with the
+  // register-resident solve made the compiler spill the whole vector
+  part[threadIdx.x] = 0.0;
   for (int xx = threadIdx.x; xx < d; xx += blockDim.x) {
     double x[RP];
 #pragma unroll
@@ -319,9 +321,8 @@ __global__ void __launch_bounds__(128) trace_beta_kernel(DysonBasis B, const dou
 #pragma unroll
     for (int l = 0; l < RP; ++l)
       if (l < r) v = add(v, mul(B.k1[l], x[l]));
-    s = add(s, v);
+    part[threadIdx.x] = add(part[threadIdx.x], v);
   }
-  part[threadIdx.x] = s;
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0.0;

@@ -35,12 +35,13 @@ int launch_correlator(cudaStream_t s, int grid, int warps_per_cta, const DevBasi
                       const CorrChain *chains, const CorrTerm *terms, const WorkUnit *units, int n_units, int *counter,
                       const double *G, double *g, double scale, int nmax, double *scratch, long warp_doubles);
 
-// Systems larger than this (N = r d_b) are factorised by the blocked kernels, smaller ones by one CTA each.
+// Default threshold: when the largest system (N = r d_b) exceeds blocked_min_n, every block is factorised by
+// the blocked kernels, else by one CTA each (the results are the same bit for bit).
 constexpr int DYSON_BLOCKED_MIN_N = 512;
 
 template <int RP>
 int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const double *Sigma, double eta, int hermitize, double *rhs,
-                 double *G, int *status, int n_max, int d_max);
+                 double *G, int *status, int n_max, int d_max, int blocked_min_n);
 
 template <int RP>
 int launch_trace_beta(cudaStream_t s, const DysonBasis &B, const double *G, double *out);

@@ -321,6 +321,7 @@ struct Ctx {
   DevBuf<int> d_batch_counter;
   cudaEvent_t ev_batch = nullptr;  // orders this context's stream against a batch led by another context
   int unit_batches = 4;      // panel batches per work unit (tunable, XCA_TUNE_UNIT_BATCHES)
+  int dyson_blocked_min_n = DYSON_BLOCKED_MIN_N;  // blocked Dyson LU above this N (XCA_TUNE_DYSON_BLOCKED_MIN_N)
   int wide_unit_tuples = 4;  // pole tuples per work unit of the wide kernel (XCA_TUNE_WIDE_UNIT_TUPLES)
   int wide_ctas_per_sm = 2;  // CTAs of the wide kernel per SM (XCA_TUNE_WIDE_CTAS_PER_SM)
   int precision = XCA_PREC_FP64;
@@ -1077,9 +1078,12 @@ static void launch_dyson(Ctx *c, const double *Sig_dev, double eta, int hermitiz
   const DysonBasis B = dyson_basis(c);
   const int n_max = c->r * c->nmax, d_max = c->nmax;
   switch (c->RP) {
-    case 32: c->launches += launch_dyson<32>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max); break;
-    case 48: c->launches += launch_dyson<48>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max); break;
-    default: c->launches += launch_dyson<64>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max); break;
+    case 32: c->launches += launch_dyson<32>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max,
+                                                        c->dyson_blocked_min_n); break;
+    case 48: c->launches += launch_dyson<48>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max,
+                                                        c->dyson_blocked_min_n); break;
+    default: c->launches += launch_dyson<64>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max,
+                                                        c->dyson_blocked_min_n); break;
   }
 }
 
@@ -2291,6 +2295,7 @@ int xca_set_tuning(xca_ctx *ctx, int param, int value) {
     case XCA_TUNE_UNIT_BATCHES: slot = &c->unit_batches; hi = 64; break;
     case XCA_TUNE_WIDE_UNIT_TUPLES: slot = &c->wide_unit_tuples; hi = 1024; break;
     case XCA_TUNE_WIDE_CTAS_PER_SM: slot = &c->wide_ctas_per_sm; hi = 8; break;
+    case XCA_TUNE_DYSON_BLOCKED_MIN_N: slot = &c->dyson_blocked_min_n; lo = 0; hi = 1 << 30; break;
     default: throw Error(XCA_ERR_INVALID, "unknown tuning parameter " + std::to_string(param));
   }
   if (value < lo || value > hi)
@@ -2298,8 +2303,10 @@ int xca_set_tuning(xca_ctx *ctx, int param, int value) {
                                      std::to_string(hi) + "]");
   if (*slot != value) {
     *slot = value;
-    c->class_cache.clear();  // work lists are cut with these sizes
-    c->noalloc_classes.clear();
+    if (param != XCA_TUNE_DYSON_BLOCKED_MIN_N) {
+      c->class_cache.clear();  // work lists are cut with these sizes
+      c->noalloc_classes.clear();
+    }
   }
   API_END
 }
@@ -2311,6 +2318,7 @@ int xca_get_tuning(xca_ctx *ctx, int param, int *value) {
     case XCA_TUNE_UNIT_BATCHES: *value = c->unit_batches; break;
     case XCA_TUNE_WIDE_UNIT_TUPLES: *value = c->wide_unit_tuples; break;
     case XCA_TUNE_WIDE_CTAS_PER_SM: *value = c->wide_ctas_per_sm; break;
+    case XCA_TUNE_DYSON_BLOCKED_MIN_N: *value = c->dyson_blocked_min_n; break;
     default: throw Error(XCA_ERR_INVALID, "unknown tuning parameter " + std::to_string(param));
   }
   API_END
