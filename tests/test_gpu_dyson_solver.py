@@ -61,6 +61,34 @@ def test_dyson_backward_error_strong_sigma():
         assert np.max(np.abs(res)) <= 1e-13 * bound, b
 
 
+@pytest.mark.parametrize("kind", ["kanamori", "anderson"])
+def test_dyson_lu_paths_bit_identical(kind):
+    # the three factorisations of the Dyson system -- one CTA with the matrix in shared memory (N <= 160),
+    # one CTA in global memory, the multi-CTA blocked LU -- perform the same operations in the same order:
+    # the solutions agree bit for bit, and with the oracle's solve to 1e-12 (Kanamori N = 168; Anderson N = r, 1 x 1 blocks)
+    from xca_b200.block_sparse import BlockOpSymQuartet, DiagramEvaluator
+    beta, lam, eps = (20.0, 200.0, 1e-12) if kind == "kanamori" else (10.0, 100.0, 1e-10)
+    d = O.Dlr(lam, eps)
+    m = (models.kanamori_2orb if kind == "kanamori" else models.anderson)(d.rf, d.it, beta, lam, eps)
+    Fq = BlockOpSymQuartet(m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks, m.dims)
+    ev = DiagramEvaluator.from_arrays(beta, lam, eps, d.rf, d.it, m.hyb_poles, m.hyb_coeffs, Fq)
+    ev.dyson_setup(m.G0)
+    G = models.seeded_G(m, 2)
+    sig = [0.05 * g for g in G]
+    bs, bg = ev.device_buffer(30, ev.slab), ev.device_buffer(31, ev.slab)
+    ev.to_device(bs, ev.pack(sig).real)
+    outs = {}
+    n_max = d.r * int(max(m.dims))
+    for name, thr in (("one_cta", 1 << 30), ("blocked", 0)):
+        ev.set_tuning(dyson_blocked_min_n=thr)
+        ev.dyson_solve_device(bs, 0.4, bg, hermitize=False)
+        outs[name] = ev.to_host(bg, ev.slab)
+    assert np.array_equal(outs["one_cta"], outs["blocked"]), n_max
+    ref = np.concatenate([d.dyson_solve(beta, g0, s, 0.4).real.ravel() for g0, s in zip(m.G0, sig)])
+    assert _rel(outs["blocked"], ref) < 1e-12
+    print(f"{kind}: N = {n_max}, LU paths identical, |dev - oracle| / max = {_rel(outs['blocked'], ref):.2e}")
+
+
 def test_dyson_zero_sigma_returns_g0():
     from xca_b200.dlr_dyson_ppsc import DysonItPPSC
     from xca_b200.pycppdlr import ImTimeOps, build_dlr_rf

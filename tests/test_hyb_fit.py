@@ -45,3 +45,23 @@ def test_bethe_compression(tol):
     assert np.max(np.abs(poles)) < 2.0 + 1e-6
     # off-diagonal residues stay zero (spin-diagonal input)
     assert np.max(np.abs(coeffs[:, 0, 1])) < 1e-12
+
+
+def test_fit_cache_returns_the_same_fit():
+    # served solves that share a bath share its fit: the cached call returns exactly the uncached result,
+    # as fresh arrays, and a changed input (another tolerance, another Delta) is fitted anew
+    beta, lam, eps = 10.0, 100.0, 1e-10
+    rf, it = _basis(lam, eps)
+    dv = models.bethe_delta(beta, it)
+    delta = np.zeros((len(it), 2, 2))
+    delta[:, 0, 0] = dv
+    delta[:, 1, 1] = dv
+    ref = hyb_fit.compress_hybridization(rf, it, beta, delta, 1e-9)
+    a = hyb_fit.compress_hybridization_cached(rf, it, beta, delta, 1e-9)
+    b = hyb_fit.compress_hybridization_cached(rf, it, beta, delta, 1e-9)
+    for x in (a, b):
+        assert np.array_equal(x[0], ref[0]) and np.array_equal(x[1], ref[1]) and x[2] == ref[2]
+    a[0][0] += 1.0  # the caller's copy, not the cache's
+    assert np.array_equal(hyb_fit.compress_hybridization_cached(rf, it, beta, delta, 1e-9)[0], ref[0])
+    c = hyb_fit.compress_hybridization_cached(rf, it, beta, 0.5 * delta, 1e-9)
+    assert not np.array_equal(c[1], ref[1])

@@ -20,7 +20,7 @@ import numpy as np
 from . import diag
 from .atom_diag import atomic_pseudo_particle_greens_function
 from .block_sparse import BlockOpSymQuartet, DiagramEvaluator
-from .hyb_fit import compress_hybridization
+from .hyb_fit import compress_hybridization_cached
 from .models import dlr_fit_hybridization, rel2abs
 from .pycppdlr import MeshDLRImTime
 
@@ -63,7 +63,8 @@ class BlockSparseSolver:
         if compression:
             if tol is None or tol <= 0:
                 raise ValueError("tol must be provided and positive when compression is enabled")
-            self.hyb_poles, self.hyb_coeffs, self.hyb_fit_error = compress_hybridization(self.rf, self.it, self.beta, self.Delta_tau, tol)
+            self.hyb_poles, self.hyb_coeffs, self.hyb_fit_error = compress_hybridization_cached(self.rf, self.it, self.beta,
+                                                                                                self.Delta_tau, tol)
         else:
             self.hyb_poles, self.hyb_coeffs = dlr_fit_hybridization(self.rf, self.it, self.beta, self.Delta_tau)
             self.hyb_fit_error = self.eps

@@ -79,7 +79,15 @@ int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const do
   dyson_convmat_kernel<RP><<<grid, 64, 0, s>>>(B);
   check_launch("dyson_convmat_kernel");
   if (n_max > blocked_min_n) return 2 + launch_blocked_lu(s, B, n_max, d_max, rhs, G, hermitize, status);
-  dyson_lu_solve_kernel<<<B.nb, 1024, 0, s>>>(B, rhs, G, hermitize, status);
+  // the largest block's matrix (row stride N + 1) and right-hand sides in shared memory when they fit
+  const size_t lu_smem = ((size_t)n_max * (n_max + 1) + (size_t)n_max * d_max) * sizeof(double);
+  if (n_max <= DYSON_SMEM_MAX_N && lu_smem <= DYSON_SMEM_MAX_BYTES) {
+    if (cudaFuncSetAttribute(dyson_lu_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_smem) != cudaSuccess)
+      check_launch("dyson_lu_solve_kernel attributes");
+    dyson_lu_solve_kernel<true><<<B.nb, 1024, lu_smem, s>>>(B, rhs, G, hermitize, status);
+  } else {
+    dyson_lu_solve_kernel<false><<<B.nb, 1024, 0, s>>>(B, rhs, G, hermitize, status);
+  }
   check_launch("dyson_lu_solve_kernel");
   return 3;
 }

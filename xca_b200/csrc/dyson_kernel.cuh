@@ -143,7 +143,8 @@ __global__ void __launch_bounds__(256) dyson_coef_kernel(DysonBasis B, const dou
 // Rows of the system matrix I + M, one thread per (block, i, x, y) row vector of A (convmat_inplace,
 // cppdlr; call site dlr_dyson_ppsc.hpp:149), in the operation order of the CPU restatement:
 //   A[i][k](x,y) = (beta K_ik) (ft_k + (t_i K_k(0)) f_k) + sum_{l != k, ascending} [((beta K_il) K_k(0)) / (om_k - om_l)] f_l
-// then M[(i,x), (i',y)] = (A K^-1)[i'] through K^T z = a.  grid.y = block, 64 threads per CTA.
+// (the bracketed weights come from the basis's table convw), then M[(i,x), (i',y)] = (A K^-1)[i'] through
+// K^T z = a.  grid.y = block, 64 threads per CTA.
 template <int RP>
 __global__ void __launch_bounds__(64) dyson_convmat_kernel(DysonBasis B) {
   __shared__ double sf[RP * 64];
@@ -165,12 +166,12 @@ __global__ void __launch_bounds__(64) dyson_convmat_kernel(DysonBasis B) {
   for (int k = 0; k < RP; ++k) {
     double acc = 0.0;
     if (k < r) {
-      const double k0k = B.k0[k], rfk = B.rf[k];
+      const double k0k = B.k0[k];
       acc = mul(B.BKp[k * RP + i], add(ft[(long)k * dd + xy], mul(mul(ti, k0k), sf[k * 64 + threadIdx.x])));
+      const double *wk = B.convw + (long)k * RP * RP + i;
       for (int l = 0; l < r; ++l) {
         if (l == k) continue;
-        const double wl = __ddiv_rn(mul(B.BKp[l * RP + i], k0k), __dsub_rn(rfk, B.rf[l]));
-        acc = add(acc, mul(wl, sf[l * 64 + threadIdx.x]));
+        acc = add(acc, mul(wk[(long)l * RP], sf[l * 64 + threadIdx.x]));
       }
     }
     a[k] = acc;
@@ -198,8 +199,13 @@ __device__ __forceinline__ void argmax_combine(double &v, int &ix, double v2, in
 // solve with the d right-hand-side columns G0 (rows (t, i), columns j: the packed slab layout), row
 // interchanges, unit-lower forward and upper backward substitution, and the (optional) hermitization
 // G(t) <- (G(t) + G(t)^T) / 2 into G_out.  rhs is the block's scratch copy of G0.
+// SMEM: the matrix (row stride N + 1, against bank conflicts on column accesses) and the right-hand sides
+// are copied into dynamic shared memory first (systems up to DYSON_SMEM_MAX_N), so that every elimination
+// step works at shared-memory latency; the operations and their order are the same either way.
+template <bool SMEM>
 __global__ void __launch_bounds__(1024) dyson_lu_solve_kernel(DysonBasis B, double *__restrict__ rhs, double *__restrict__ G_out,
                                                               int hermitize, int *__restrict__ status) {
+  extern __shared__ __align__(16) double smA[];
   __shared__ double red_v[32];
   __shared__ int red_i[32];
   __shared__ int s_piv;
@@ -207,17 +213,27 @@ __global__ void __launch_bounds__(1024) dyson_lu_solve_kernel(DysonBasis B, doub
   if (b >= B.nb) return;
   const int r = B.r, d = B.dims[b], dd = d * d;
   const int N = r * d;
+  const long lda = SMEM ? N + 1 : N;
   double *A = B.mats + B.moff[b];
   double *x = rhs + B.goff[b];
   const double *g0 = B.g0 + B.goff[b];
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  if (SMEM) {
+    for (long e = tid; e < (long)N * N; e += nt) {
+      const long i = e / N, j = e - i * N;
+      smA[i * lda + j] = A[e];
+    }
+    A = smA;
+    x = smA + (long)N * lda;
+  }
   for (long e = tid; e < (long)N * d; e += nt) x[e] = g0[e];
+  if (SMEM) __syncthreads();
   bool singular = false;
   for (int k = 0; k < N; ++k) {
     // pivot search in column k, rows k..N-1
     double bv = -1.0;
     int bi = N;
-    for (int i = k + tid; i < N; i += nt) argmax_combine(bv, bi, fabs(A[(long)i * N + k]), i);
+    for (int i = k + tid; i < N; i += nt) argmax_combine(bv, bi, fabs(A[(long)i * lda + k]), i);
     for (int o = 16; o > 0; o >>= 1) {
       double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
       int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
@@ -240,9 +256,9 @@ __global__ void __launch_bounds__(1024) dyson_lu_solve_kernel(DysonBasis B, doub
     if (p >= N) { singular = true; break; }  // only when the column is NaN
     if (p != k) {
       for (int j = tid; j < N; j += nt) {
-        const double t = A[(long)k * N + j];
-        A[(long)k * N + j] = A[(long)p * N + j];
-        A[(long)p * N + j] = t;
+        const double t = A[(long)k * lda + j];
+        A[(long)k * lda + j] = A[(long)p * lda + j];
+        A[(long)p * lda + j] = t;
       }
       for (int j = tid; j < d; j += nt) {
         const double t = x[(long)k * d + j];
@@ -251,14 +267,14 @@ __global__ void __launch_bounds__(1024) dyson_lu_solve_kernel(DysonBasis B, doub
       }
     }
     __syncthreads();
-    const double piv = A[(long)k * N + k];
+    const double piv = A[(long)k * lda + k];
     if (piv == 0.0) { singular = true; break; }
-    for (int i = k + 1 + tid; i < N; i += nt) A[(long)i * N + k] = __ddiv_rn(A[(long)i * N + k], piv);
+    for (int i = k + 1 + tid; i < N; i += nt) A[(long)i * lda + k] = __ddiv_rn(A[(long)i * lda + k], piv);
     __syncthreads();
     const int m = N - k - 1;
     for (long e = tid; e < (long)m * m; e += nt) {
       const int i = k + 1 + (int)(e / m), j = k + 1 + (int)(e - (e / m) * m);
-      A[(long)i * N + j] = __dsub_rn(A[(long)i * N + j], mul(A[(long)i * N + k], A[(long)k * N + j]));
+      A[(long)i * lda + j] = __dsub_rn(A[(long)i * lda + j], mul(A[(long)i * lda + k], A[(long)k * lda + j]));
     }
     __syncthreads();
   }
@@ -271,17 +287,17 @@ __global__ void __launch_bounds__(1024) dyson_lu_solve_kernel(DysonBasis B, doub
     const int m = N - k - 1;
     for (int e = tid; e < m * d; e += nt) {
       const int i = k + 1 + e / d, j = e - (e / d) * d;
-      x[(long)i * d + j] = fmad(-A[(long)i * N + k], x[(long)k * d + j], x[(long)i * d + j]);
+      x[(long)i * d + j] = fmad(-A[(long)i * lda + k], x[(long)k * d + j], x[(long)i * d + j]);
     }
     __syncthreads();
   }
   // backward substitution with the upper factor
   for (int k = N - 1; k >= 0; --k) {
-    for (int j = tid; j < d; j += nt) x[(long)k * d + j] = __ddiv_rn(x[(long)k * d + j], A[(long)k * N + k]);
+    for (int j = tid; j < d; j += nt) x[(long)k * d + j] = __ddiv_rn(x[(long)k * d + j], A[(long)k * lda + k]);
     __syncthreads();
     for (int e = tid; e < k * d; e += nt) {
       const int i = e / d, j = e - i * d;
-      x[(long)i * d + j] = fmad(-A[(long)i * N + k], x[(long)k * d + j], x[(long)i * d + j]);
+      x[(long)i * d + j] = fmad(-A[(long)i * lda + k], x[(long)k * d + j], x[(long)i * d + j]);
     }
     __syncthreads();
   }

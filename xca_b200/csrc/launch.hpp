@@ -37,7 +37,10 @@ int launch_correlator(cudaStream_t s, int grid, int warps_per_cta, const DevBasi
 
 // Default threshold: when the largest system (N = r d_b) exceeds blocked_min_n, every block is factorised by
 // the blocked kernels, else by one CTA each (the results are the same bit for bit).
-constexpr int DYSON_BLOCKED_MIN_N = 512;
+constexpr int DYSON_BLOCKED_MIN_N = 192;
+// One-CTA systems whose matrix and right-hand sides fit these bounds are factorised in shared memory.
+constexpr int DYSON_SMEM_MAX_N = 192;
+constexpr size_t DYSON_SMEM_MAX_BYTES = 220 * 1024;
 
 template <int RP>
 int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const double *Sigma, double eta, int hermitize, double *rhs,

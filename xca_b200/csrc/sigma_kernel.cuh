@@ -131,6 +131,7 @@ struct DysonBasis {
   const double *g0, *g0c, *g0t;  // packed slabs: G0 values, K^-1 G0, W K^-1 G0
   double *work;
   double *mats;
+  const double *convw;           // RP^3: ((beta K_il) K_k(0)) / (om_k - om_l) at (k RP + l) RP + i
 };
 
 // D = A B + C on one 8 x 8 x 4 tile (a: A[g][q], b: B[q][g], c/d: C[g][2q], C[g][2q + 1], g = lane / 4, q = lane % 4).

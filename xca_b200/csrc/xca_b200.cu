@@ -297,6 +297,7 @@ struct Ctx {
   DevBuf<double> d_tabs, d_k0, d_kitp, d_kitm, d_kpow, d_polesb, d_hval, d_hrefl, d_ops;
   DevBuf<int> d_dims, d_set_to_orb, d_perm, d_pinv;
   DevBuf<double> d_LUp, d_Wp, d_BKp, d_tab;
+  DevBuf<double> d_convw;  // RP^3: divided weights of the Dyson convolution-matrix rows
   DevBuf<long> d_tab_off;
   DevBuf<long> d_goff, d_F_off, d_Fd_off, d_Fb_off, d_Fdb_off;
   DevBuf<int> d_counter;
@@ -445,6 +446,16 @@ static void setup_basis(Ctx *c, double beta, double lambda, double eps, int r, c
   c->corr_cache.clear();
   c->d_tabs.upload(c->tabs, s); c->d_k0.upload(c->k0, s); c->d_k1.upload(c->k1, s); c->d_rf.upload(c->rf, s);
   c->d_dims.upload(c->dims, s); c->d_goff.upload(c->goff, s);
+  // divided weights of the Dyson convolution-matrix rows, w(k, l, i) = ((beta K_il) K_k(0)) / (om_k - om_l) for
+  // l != k (the kernel's terms, each operation correctly rounded as there), formed once per basis
+  std::vector<double> convw((size_t)RP * RP * RP, 0.0);
+  for (int k = 0; k < r; ++k)
+    for (int l = 0; l < r; ++l) {
+      if (l == k) continue;
+      const double den = c->rf[k] - c->rf[l];
+      for (int i = 0; i < r; ++i) convw[((size_t)k * RP + l) * RP + i] = (c->BKp[(size_t)l * RP + i] * c->k0[k]) / den;
+    }
+  c->d_convw.upload(convw, s);
   c->basis_ready = true;
 }
 
@@ -1060,7 +1071,7 @@ static DysonBasis dyson_basis(Ctx *c) {
   B.tabs = c->d_tabs.ptr; B.k0 = c->d_k0.ptr; B.k1 = c->d_k1.ptr; B.rf = c->d_rf.ptr;
   B.goff = c->d_goff.ptr; B.dims = c->d_dims.ptr; B.woff = c->d_woff.ptr; B.moff = c->d_moff.ptr;
   B.g0 = c->d_g0.ptr; B.g0c = c->d_g0c.ptr; B.g0t = c->d_g0t.ptr;
-  B.work = c->d_dwork.ptr; B.mats = c->d_mats.ptr;
+  B.work = c->d_dwork.ptr; B.mats = c->d_mats.ptr; B.convw = c->d_convw.ptr;
   return B;
 }
 

@@ -12,6 +12,10 @@ imaginary-time error is below the tolerance (``adapol_depr/fit_utils_xca.py:190-
 run once per solve like the reference's.
 """
 
+import hashlib
+import threading
+from collections import OrderedDict
+
 import numpy as np
 import scipy.linalg
 import scipy.optimize
@@ -133,3 +137,31 @@ def compress_hybridization(rf, it, beta, delta_tau, tol, max_poles=50):
     x, W, err = best
     order = np.argsort(x)
     return x[order] / beta, np.asarray(W[order], dtype=np.complex128), err
+
+
+_FITS = OrderedDict()
+_FITS_LOCK = threading.Lock()
+FIT_CACHE_SIZE = 64
+
+
+def compress_hybridization_cached(rf, it, beta, delta_tau, tol, max_poles=50):
+    """compress_hybridization, its result kept per exact input (DLR nodes, beta, the values of Delta, tol,
+    max_poles; at most FIT_CACHE_SIZE fits, least recently used dropped): the fit is a deterministic function
+    of these, so solves that share a bath -- the requests of a served stream at one beta -- share it."""
+    h = hashlib.sha1()
+    for a in (rf, it, delta_tau):
+        h.update(np.ascontiguousarray(a).tobytes())
+    h.update(np.array([beta, tol, max_poles], np.float64).tobytes())
+    key = h.hexdigest()
+    with _FITS_LOCK:
+        hit = _FITS.get(key)
+        if hit is not None:
+            _FITS.move_to_end(key)
+    if hit is None:
+        hit = compress_hybridization(rf, it, beta, delta_tau, tol, max_poles)
+        with _FITS_LOCK:
+            _FITS[key] = hit
+            while len(_FITS) > FIT_CACHE_SIZE:
+                _FITS.popitem(last=False)
+    poles, coeffs, err = hit
+    return poles.copy(), coeffs.copy(), err
