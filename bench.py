@@ -222,19 +222,30 @@ def run_serving(args, batched=False):
     return out
 
 
-def compressed_variant(m, G, device):
-    """The same evaluation with the Bethe hybridization compressed to a few poles inside the band
+def _per_node_rel(ev, a, b):
+    """max over tau nodes of max |a - b| / max |b| at that node (all blocks)."""
+    num, den, off = np.zeros(ev.r), np.zeros(ev.r), 0
+    for d in ev.dims:
+        sz = ev.r * d * d
+        num = np.maximum(num, np.max(np.abs(a[off:off + sz] - b[off:off + sz]).reshape(ev.r, -1), axis=1))
+        den = np.maximum(den, np.max(np.abs(b[off:off + sz]).reshape(ev.r, -1), axis=1))
+        off += sz
+    return float(np.max(num / np.maximum(den, 1e-300)))
+
+
+def precision_variants(m, G, device):
+    """The same evaluation (1) with the Bethe hybridization compressed to a few poles inside the band
     (fit_hybridization(compression=True), xca_b200.hyb_fit, tolerance 1e-10) in place of one pole per DLR
-    frequency: evals/s and the change of Sigma (the DLR-pole evaluation amplifies input rounding, see the
-    conditioning test)."""
+    frequency, and (2) with FP32 block products (the mixed form's bulk arithmetic, evaluator mode 'fp32'), for
+    both pole sets: evals/s and the change of Sigma against FP64 (per tau node, relative to the node's largest
+    entry).  (3) The mixed solve against the FP64 one: the same model from its atomic G0, TCA with the
+    compressed hybridization, to 1e-10: time, iterations and the difference of the converged G(tau)."""
     import torch
-    from xca_b200 import hyb_fit
+    from xca_b200 import hyb_fit, models
     from xca_b200.block_sparse import BlockOpSymQuartet, DiagramEvaluator
+    from xca_b200.block_sparse_solver import BlockSparseSolver
     from xca_b200.distributed import self_energy_sharded
-    dv = m.extra.get("delta_diag")
-    if dv is None:
-        from xca_b200 import models
-        dv = models.bethe_delta(m.beta, m.it)
+    dv = models.bethe_delta(m.beta, m.it)
     delta = np.zeros((m.r, m.n, m.n))
     for i in range(m.n):
         delta[:, i, i] = dv
@@ -247,19 +258,46 @@ def compressed_variant(m, G, device):
         G_t = torch.tensor(np.concatenate([g.real.ravel() for g in G]), dtype=torch.float64, device=dev)
         S_t = torch.zeros(ev.slab, dtype=torch.float64, device=dev)
         terms = topologies()
-        for _ in range(2):
-            self_energy_sharded(ev, G_t.data_ptr(), S_t.data_ptr(), terms, 0, 1)
-        ms = []
-        for _ in range(3):
-            ev.flush_l2(256 << 20)
-            ev.event_record(0)
-            self_energy_sharded(ev, G_t.data_ptr(), S_t.data_ptr(), terms, 0, 1)
-            ev.event_record(1)
-            ms.append(ev.event_elapsed(0, 1))
-        res[name] = (float(np.median(ms)), S_t.cpu().numpy())
-    diff = float(np.max(np.abs(res["compressed"][1] - res["dlr"][1])) / np.max(np.abs(res["dlr"][1])))
-    return {"value": 1000.0 / res["compressed"][0], "unit": UNIT, "poles": int(len(poles)), "fit_error": float(err),
-            "sigma_rel_change_vs_dlr_poles": diff, "ms_per_step": res["compressed"][0]}
+        for mode in ("fp64", "fp32"):
+            ev.precision_mode = mode
+            for _ in range(2):
+                self_energy_sharded(ev, G_t.data_ptr(), S_t.data_ptr(), terms, 0, 1)
+            ms = []
+            for _ in range(3):
+                ev.flush_l2(256 << 20)
+                ev.event_record(0)
+                self_energy_sharded(ev, G_t.data_ptr(), S_t.data_ptr(), terms, 0, 1)
+                ev.event_record(1)
+                ms.append(ev.event_elapsed(0, 1))
+            res[(name, mode)] = (float(np.median(ms)), S_t.cpu().numpy())
+        res[name] = ev
+    ref = res[("dlr", "fp64")][1]
+    diff = float(np.max(np.abs(res[("compressed", "fp64")][1] - ref)) / np.max(np.abs(ref)))
+    out = {"compressed_hybridization": {"value": 1000.0 / res[("compressed", "fp64")][0], "unit": UNIT, "poles": int(len(poles)),
+                                        "fit_error": float(err), "sigma_rel_change_vs_dlr_poles": diff,
+                                        "ms_per_step": res[("compressed", "fp64")][0]}}
+    mixed = {}
+    for name in ("dlr", "compressed"):
+        t32, s32 = res[(name, "fp32")]
+        t64, s64 = res[(name, "fp64")]
+        mixed[f"fp32_sigma_{name}_poles"] = {"value": 1000.0 / t32, "unit": UNIT, "ms_per_step": t32, "fp64_ms_per_step": t64,
+                                             "per_node_rel_err_vs_fp64": _per_node_rel(res[name], s32, s64),
+                                             "input": "seeded G (default_rng(0))"}
+    solves = {}
+    for precision in ("fp64", "mixed"):
+        S = BlockSparseSolver(m.ad, m.beta, m.lam / m.beta, m.eps, device=device, precision=precision)
+        S.Delta_tau = delta.astype(np.complex128)
+        S.solve(max_order=3, tol=1e-10, maxiter=60, hyb_comp=True, hyb_tol=1e-11)
+        solves[precision] = S
+    a, b = solves["mixed"], solves["fp64"]
+    mixed["solve"] = {"model": "kanamori_2orb TCA from G0, compressed hybridization", "tol": 1e-10,
+                      "fp64_solve_loop_s": b.timings["solve_loop_s"], "mixed_solve_loop_s": a.timings["solve_loop_s"],
+                      "fp64_iterations": int(b.n_ppsc_iter), "mixed_fp32_iterations": int(a.n_fp32_iter),
+                      "mixed_fp64_iterations": int(a.n_ppsc_iter - a.n_fp32_iter),
+                      "max_abs_diff_G_tau_vs_fp64": float(np.max(np.abs(a.G_tau - b.G_tau))),
+                      "max_abs_diff_G_vs_fp64": max(float(np.max(np.abs(x - y))) for x, y in zip(a.G, b.G))}
+    out["mixed"] = mixed
+    return out
 
 
 def run_dshell(args):
@@ -460,7 +498,7 @@ def main():
         cpu = cpu_baseline_object(args.cpu_seconds)
     variants = None
     if rank == 0 and world == 1 and not args.no_variants:
-        variants = {"compressed_hybridization": compressed_variant(m, G, local)}
+        variants = precision_variants(m, G, local)
     serving = None
     if rank == 0 and world == 1 and not args.no_serving:
         serving = {"batched": run_serving(args, batched=True), "threads": run_serving(args, batched=False)}

@@ -34,6 +34,7 @@ extern "C" {
 /* Precision / summation modes of the Sigma evaluation (xca_set_precision_mode). */
 #define XCA_PREC_FP64 0          /* FP64, items summed into Sigma with atomics (fastest; order varies run to run) */
 #define XCA_PREC_FP64_ORDERED 1  /* FP64, fixed summation order: reproducible bit for bit from run to run */
+#define XCA_PREC_FP32 2          /* FP32 block products on the CUDA cores, FP64 prefactors and atomic accumulation */
 
 /* Pole tuples per work unit in XCA_PREC_FP64_ORDERED (part of the definition of its summation order). */
 #define XCA_ORDERED_UNIT_TUPLES 64
@@ -263,9 +264,14 @@ int xca_synchronize(xca_ctx *ctx);
  * block, path classes in enumeration order (directions, orbital tuple, symmetry set), within a class runs
  * of XCA_ORDERED_UNIT_TUPLES pole tuples in order, within a run the items in order, each partial sum
  * starting from zero; for a flat-index list (xca_compute_self_energy with f_ix) the items in list order.
+ * XCA_PREC_FP32: the bulk arithmetic of the mixed-precision form — path classes that fit a shared-memory
+ * panel evaluate their block products and DLR steps in FP32 (prefactors and the accumulation into Sigma
+ * stay FP64); wider chains stay FP64.  Accurate to FP32 rounding for NCA topologies only: the DLR
+ * convolution of every edge (K^-1 with cond ~ 1/eps, cancelling Hilbert-type sums) loses all FP32 digits,
+ * so a mixed solve uses it for NCA warm-up iterations and runs the full order in FP64.
  * Applies to xca_compute_self_energy, xca_compute_self_energy_device and the single-shard
- * xca_compute_self_energy_device_shard (n_shards > 1 gives XCA_ERR_UNSUPPORTED); the allocation-free
- * variant always uses XCA_PREC_FP64.  Unknown modes give XCA_ERR_UNSUPPORTED. */
+ * xca_compute_self_energy_device_shard (n_shards > 1 gives XCA_ERR_UNSUPPORTED in XCA_PREC_FP64_ORDERED); the
+ * allocation-free variant always uses XCA_PREC_FP64.  Unknown modes give XCA_ERR_UNSUPPORTED. */
 int xca_set_precision_mode(xca_ctx *ctx, int mode);
 int xca_get_precision_mode(xca_ctx *ctx, int *mode);
 

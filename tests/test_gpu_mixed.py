@@ -1,0 +1,121 @@
+"""The mixed-precision form: FP32 block products for Sigma (evaluator mode 'fp32') and the 'mixed' solve.
+
+Measured first (test_fp32_sigma_error_vs_eps): the FP32 Sigma of the NCA diagram, which has no DLR
+convolution, is within FP32 rounding of the FP64 one (1e-7); every higher diagram passes through the
+closed-form DLR convolution of an edge -- K^-1 with cond ~ 1/eps, then sums over W_lk = K(0, om_k) /
+(om_k - om_l) that cancel -- and its FP32 error grows with 1/eps from 1e-1 at eps = 1e-3 to far beyond 1
+at the accuracies in use.  So the 'mixed' solve confines FP32 to the NCA diagram: FP32 NCA iterations
+to 1e-5, then the full order in FP64 until convergence.  Stated bound: after convergence, G(tau), G and
+eta within 1e-8 of the FP64 oracle's solve (cfg0's Anderson model with DLR poles and with compressed poles,
+cfg2's t2g model at NCA; its OCA solve diverges under the classic normalisation in FP64 as well).
+"""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from xca_b200 import models
+
+pytestmark = pytest.mark.gpu
+
+TOL_MIXED = 1e-8
+
+
+def _per_node_rel(ev, a, b):
+    r = ev.r
+    num, den, off = np.zeros(r), np.zeros(r), 0
+    for d in ev.dims:
+        sz = r * d * d
+        num = np.maximum(num, np.max(np.abs(a[off:off + sz] - b[off:off + sz]).reshape(r, -1), axis=1))
+        den = np.maximum(den, np.max(np.abs(b[off:off + sz]).reshape(r, -1), axis=1))
+        off += sz
+    return float(np.max(num / np.maximum(den, 1e-300)))
+
+
+def _sigma_both(ev, G, topos):
+    bg, bs = ev.device_buffer(30, ev.slab), ev.device_buffer(31, ev.slab)
+    ev.to_device(bg, ev.pack(G).real)
+    out = {}
+    for mode in ("fp64", "fp32"):
+        ev.precision_mode = mode
+        ev.zero_device(bs, ev.slab)
+        for sign, t in topos:
+            ev.compute_self_energy_device(bg, t, float(sign), bs)
+        out[mode] = ev.to_host(bs, ev.slab)
+    ev.precision_mode = "fp64"
+    return out
+
+
+def test_fp32_sigma_error_vs_eps():
+    # Anderson (beta = 10, Lambda = 40) from the atomic G0, one Sigma per order in FP64 and in FP32
+    from xca_b200.block_sparse import BlockOpSymQuartet, DiagramEvaluator
+    from xca_b200.distributed import sigma_terms
+    beta, lam = 10.0, 40.0
+    err = {}
+    for eps in (1e-3, 1e-6, 1e-10):
+        d = O.Dlr(lam, eps)
+        m = models.anderson(d.rf, d.it, beta, lam, eps)
+        Fq = BlockOpSymQuartet(m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks, m.dims)
+        ev = DiagramEvaluator.from_arrays(beta, lam, eps, d.rf, d.it, m.hyb_poles, m.hyb_coeffs, Fq)
+        for order in (1, 2, 3):
+            res = _sigma_both(ev, m.G0, [(fac, t) for o, t, fac in sigma_terms(order) if o == order])
+            err[(eps, order)] = _per_node_rel(ev, res["fp32"], res["fp64"])
+    print("FP32 Sigma vs FP64, per-node relative error: "
+          + ", ".join(f"eps {k[0]:.0e} order {k[1]}: {v:.1e}" for k, v in err.items()))
+    for eps in (1e-3, 1e-6, 1e-10):
+        assert err[(eps, 1)] < 1e-6  # NCA: FP32 rounding
+    # OCA / TCA: the edge's error grows with the conditioning of the DLR basis
+    assert err[(1e-10, 2)] > 100 * err[(1e-3, 2)] and err[(1e-10, 3)] > 100 * err[(1e-3, 3)]
+
+
+def _anderson(precision, beta=10.0, lam=100.0, eps=1e-10):
+    from xca_b200.block_sparse_solver import BlockSparseSolver
+    from xca_b200.pycppdlr import MeshDLRImTime
+    mesh = MeshDLRImTime(beta=beta, statistic="Fermion", w_max=lam / beta, eps=eps)
+    m = models.anderson(mesh.dlr_rf, mesh.dlr_it.it, beta, lam, eps)
+    S = BlockSparseSolver(m.ad, beta, lam / beta, eps, precision=precision)
+    delta = np.zeros((S.r, 2, 2), np.complex128)
+    dv = models.bethe_delta(beta, S.it)
+    delta[:, 0, 0] = dv
+    delta[:, 1, 1] = dv
+    S.Delta_tau = delta
+    return S, m
+
+
+def _vs_oracle(S, m, order, tol, maxiter=60):
+    d = O.Dlr(S.beta * S.w_max, S.eps, rf=S.rf, it=S.it)
+    ev = O.Evaluator(d, S.beta, S.hyb_poles, S.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
+    G, Sig, eta, g, n_iter, diff = O.solve(d, ev, S.beta, m.G0, order, tol, maxiter, spgf_max_order=order)
+    dG = max(float(np.max(np.abs(a - b))) for a, b in zip(S.G, G))
+    dg = float(np.max(np.abs(S.G_tau - g)))
+    return dG, dg, abs(S.eta - eta), n_iter
+
+
+@pytest.mark.parametrize("order,comp", [(2, False), (2, True), (3, True)])
+def test_mixed_solve_anderson_vs_oracle(order, comp):
+    # the single-orbital Anderson solve (beta = 10, Lambda = 100): FP32 NCA iterations, then the full order in
+    # FP64 to tol = 1e-10; G(tau), G and eta within 1e-8 of the FP64 oracle's solve on the same poles
+    S, m = _anderson("mixed")
+    S.solve(max_order=order, tol=1e-10, maxiter=60, hyb_comp=comp, hyb_tol=1e-11)
+    dG, dg, de, n_ora = _vs_oracle(S, m, order, 1e-10)
+    print(f"Anderson order {order}, {'compressed' if comp else 'DLR'} poles ({len(S.hyb_poles)}): {S.n_fp32_iter} FP32 + "
+          f"{S.n_ppsc_iter - S.n_fp32_iter} FP64 iterations (oracle {n_ora}); |dG(tau)| {dg:.1e}, |dG| {dG:.1e}, |deta| {de:.1e}")
+    assert S.diff_G < 1e-10
+    assert S.n_fp32_iter >= 1
+    assert dg <= TOL_MIXED and dG <= TOL_MIXED and de <= TOL_MIXED
+
+
+def test_mixed_solve_t2g_nca_vs_oracle():
+    from xca_b200.block_sparse_solver import BlockSparseSolver
+    from xca_b200.pycppdlr import MeshDLRImTime
+    beta, lam, eps = 50.0, 500.0, 1e-10
+    mesh = MeshDLRImTime(beta=beta, statistic="Fermion", w_max=lam / beta, eps=eps)
+    m = models.t2g_3orb(mesh.dlr_rf, mesh.dlr_it.it, beta, lam, eps)
+    S = BlockSparseSolver(m.ad, beta, lam / beta, eps, precision="mixed")
+    S.Delta_tau = np.asarray(m.extra["delta"], np.complex128)
+    S.solve(max_order=1, tol=1e-9, maxiter=150)
+    dG, dg, de, n_ora = _vs_oracle(S, m, 1, 1e-9, maxiter=150)
+    print(f"t2g NCA: {S.n_fp32_iter} FP32 + {S.n_ppsc_iter - S.n_fp32_iter} FP64 iterations (oracle {n_ora}); "
+          f"|dG(tau)| {dg:.1e}, |dG| {dG:.1e}, |deta| {de:.1e}")
+    assert S.diff_G < 1e-9
+    assert dg <= TOL_MIXED and dG <= TOL_MIXED and de <= TOL_MIXED

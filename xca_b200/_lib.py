@@ -19,8 +19,9 @@ XCA_ERR_UNSUPPORTED = 4
 # precision / summation modes (xca_set_precision_mode)
 XCA_PREC_FP64 = 0
 XCA_PREC_FP64_ORDERED = 1
+XCA_PREC_FP32 = 2
 XCA_ORDERED_UNIT_TUPLES = 64
-PRECISION_MODES = {"fp64": XCA_PREC_FP64, "fp64_ordered": XCA_PREC_FP64_ORDERED}
+PRECISION_MODES = {"fp64": XCA_PREC_FP64, "fp64_ordered": XCA_PREC_FP64_ORDERED, "fp32": XCA_PREC_FP32}
 
 # launch-shape parameters (xca_set_tuning)
 TUNING = {"unit_batches": 0, "wide_unit_tuples": 1, "wide_ctas_per_sm": 2, "dyson_blocked_min_n": 3}

@@ -31,11 +31,19 @@ NORMALIZATIONS = ("classic", "root", "ode+classic", "ode+root")
 
 
 class BlockSparseSolver:
-    def __init__(self, atom_diag, beta, w_max, eps, device=0, verbose=False, precision="fp64"):
-        """``precision``: the evaluator's precision mode, 'fp64' (items summed with atomics) or
-        'fp64_ordered' (fixed summation order: the solve is reproducible bit for bit)."""
+    def __init__(self, atom_diag, beta, w_max, eps, device=0, verbose=False, precision="fp64", mixed_tol=1e-5):
+        """``precision``: 'fp64' (Sigma items summed with atomics), 'fp64_ordered' (fixed summation order: the
+        solve is reproducible bit for bit) or 'mixed': the early iterations evaluate the NCA Sigma only, with
+        FP32 block products (the evaluator's 'fp32' mode), until diff_G falls below ``mixed_tol`` or makes no
+        new low for three iterations; then the full order in FP64 until convergence, which is only accepted in that phase.  FP32
+        is confined to NCA because every higher diagram passes through the DLR convolution of an edge, whose
+        closed form (K^-1 with cond ~ 1/eps, then sums over W_lk = K(0, om_k) / (om_k - om_l) that cancel)
+        loses all FP32 digits.  The Dyson solve, the normalisation and G(tau) are FP64 throughout."""
+        if precision not in ("fp64", "fp64_ordered", "mixed"):
+            raise ValueError(f"precision must be 'fp64', 'fp64_ordered' or 'mixed', got {precision!r}")
         self.ad = atom_diag
         self.precision = precision
+        self.mixed_tol = float(mixed_tol)
         self.beta = float(beta)
         self.w_max = float(w_max)
         self.eps = float(eps)
@@ -73,7 +81,7 @@ class BlockSparseSolver:
     def init_diagram_evaluator(self):
         self.d = DiagramEvaluator.from_arrays(self.beta, self.beta * self.w_max, self.eps, self.rf, self.it, self.hyb_poles,
                                               self.hyb_coeffs, self.Fq, device=self.device)
-        self.d.precision_mode = self.precision
+        self.d.precision_mode = "fp32" if self.precision == "mixed" else self.precision
         self.d.dyson_setup(self.G0)
         self._buf = {k: self.d.device_buffer(slot, self.d.slab) for k, slot in _SLOTS.items()}
 
@@ -104,11 +112,12 @@ class BlockSparseSolver:
 
     def _sigma_device(self, max_order):
         jobs = self.sigma_jobs(max_order)
-        if self.precision == "fp64":
+        if self.d.precision_mode == "fp64":
             # every topology in one launch over the shared edge tables of the highest order
             DiagramEvaluator.compute_self_energy_device_batch(jobs)
         else:
-            # the fixed summation order: one ordered evaluation per topology, accumulated in topology order
+            # the fixed summation order (one ordered evaluation per topology, accumulated in topology order), or
+            # the FP32 products of a mixed solve's early iterations
             for _, G, topo, fac, S in jobs:
                 self.d.compute_self_energy_device(G, topo, fac, S)
 
@@ -131,9 +140,10 @@ class BlockSparseSolver:
         (queued on the evaluator's stream)."""
         self.d.dyson_solve_device(self._buf["S"], self.eta, self._buf["Gn"], hermitize=True)
 
-    def end_iteration(self, it, tol, mix, verbose=False, dyson_launched=False):
+    def end_iteration(self, it, tol, mix, verbose=False, dyson_launched=False, accept=True):
         """The rest of one iteration after its Sigma (block_sparse_solver.py:300-345): eta, Dyson solve,
-        normalisation, diff_G; mixes G unless converged.  Returns True when diff_G < tol."""
+        normalisation, diff_G; mixes G unless converged.  Returns True when diff_G < tol (never with
+        ``accept`` False, as in the FP32 phase of a mixed solve)."""
         d = self.d
         normalization = self.normalization
         if normalization in ("ode+classic", "ode+root"):
@@ -151,7 +161,7 @@ class BlockSparseSolver:
         self.n_ppsc_iter = it
         if verbose:
             print(f"iter = {it}, diff_G = {self.diff_G:2.2E}, Z = {Z:+2.6E}, eta = {self.eta:2.2E}")
-        if self.diff_G < tol:
+        if accept and self.diff_G < tol:
             return True
         d.axpby_device(mix, self._buf["Gn"], 1.0 - mix, self._buf["G"])
         return False
@@ -174,9 +184,23 @@ class BlockSparseSolver:
         self.begin(max_order, tol, hyb_tol, hyb_comp, normalization, spgf_max_order)
         t0 = time.perf_counter()
         self.n_ppsc_iter = 0
+        self.n_fp32_iter = 0
+        fp32_phase = self.precision == "mixed"
+        best, stalled = np.inf, 0
         for it in range(1, maxiter + 1):
-            self._sigma_device(max_order)
-            if self.end_iteration(it, tol, mix, verbose):
+            self._sigma_device(1 if fp32_phase else max_order)
+            done = self.end_iteration(it, tol, mix, verbose, accept=not fp32_phase)
+            if fp32_phase:
+                self.n_fp32_iter += 1
+                if self.diff_G < best:
+                    best, stalled = self.diff_G, 0
+                else:
+                    stalled += 1
+                # below mixed_tol, three iterations without a new best, or not finite: the full order in FP64
+                if self.diff_G < self.mixed_tol or stalled >= 3 or not np.isfinite(self.diff_G):
+                    fp32_phase = False
+                    self.d.precision_mode = "fp64"
+            if done:
                 break
         self.d.synchronize()
         self.timings["solve_loop_s"] = time.perf_counter() - t0
@@ -240,7 +264,7 @@ class BlockSparseSolver:
     # the device evaluator; h5 is not available here, so the state goes to a numpy .npz archive
     _STATE_ARRAYS = ("G", "Sigma", "G0", "Delta_tau", "hyb_poles", "hyb_coeffs", "G_tau")
     _STATE_SCALARS = ("beta", "w_max", "eps", "eta", "eta0", "n_ppsc_iter", "diff_G", "max_order", "spgf_max_order", "precision",
-                      "normalization", "verbose", "hyb_tol", "hyb_fit_error", "hyb_compression")
+                      "normalization", "verbose", "hyb_tol", "hyb_fit_error", "hyb_compression", "mixed_tol", "n_fp32_iter")
 
     def __reduce_to_dict__(self):
         out = {"atom_diag": self.ad.to_dict()}

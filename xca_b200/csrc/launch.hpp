@@ -20,6 +20,11 @@ int launch_sigma_panel(cudaStream_t s, int nsm, const DevBasis &B, const ClassRe
 template <int RP>
 int launch_sigma_panel_batch(cudaStream_t s, int nsm, const SigmaJob *jobs, const WorkUnit *units, int n_units, int *counter);
 
+// FP32 Sigma kernel (sigma_f32.cuh) over the panel classes' units: fast (atomic) output into FP64 Sigma.
+template <int RP>
+int launch_sigma_f32(cudaStream_t s, int nsm, const DevBasis &B, const ClassRec *classes, const WorkUnit *units, int n_units, int *counter,
+                     const double *G, const SigmaOut &out);
+
 // Wide-chain Sigma kernel (sigma_wide.cuh) over n_units units with `grid` CTAs; each CTA's region of scratch
 // is cta_doubles long and holds 3 + (largest symmetry set) slabs of `slab` doubles.
 template <int RP>

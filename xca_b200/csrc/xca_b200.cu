@@ -836,9 +836,19 @@ static void launch_sigma(Ctx *c, ClassSet *cs, const double *G_dev, double *Sig_
     launch_sigma_plan(c, cs->classes, cs->d_classes.ptr, ordered_plan(c, cs), G_dev, Sig_dev, scale, nsig);
   } else {
     c->d_counter.resize(1);
-    if (!cs->units.empty())
+    if (!cs->units.empty() && c->precision == XCA_PREC_FP32) {
+      const DevBasis B = c->basis(nsig);
+      const int nu = (int)cs->units.size();
+      const SigmaOut o = atomic_out(Sig_dev, scale);
+      switch (c->RP) {
+        case 32: c->launches += launch_sigma_f32<32>(c->stream, c->nsm, B, cs->d_classes.ptr, cs->d_units.ptr, nu, c->d_counter.ptr, G_dev, o); break;
+        case 48: c->launches += launch_sigma_f32<48>(c->stream, c->nsm, B, cs->d_classes.ptr, cs->d_units.ptr, nu, c->d_counter.ptr, G_dev, o); break;
+        default: c->launches += launch_sigma_f32<64>(c->stream, c->nsm, B, cs->d_classes.ptr, cs->d_units.ptr, nu, c->d_counter.ptr, G_dev, o); break;
+      }
+    } else if (!cs->units.empty()) {
       launch_sigma_units(c, c->basis(nsig), cs->d_classes.ptr, cs->d_units.ptr, (int)cs->units.size(), c->d_counter.ptr, G_dev,
                          atomic_out(Sig_dev, scale));
+    }
     launch_wide_units(c, c->basis(nsig), cs->d_classes.ptr, cs->d_wide_units.ptr, (int)cs->wide_units.size(), cs->wide_slab, G_dev,
                       atomic_out(Sig_dev, scale));
   }
@@ -2291,7 +2301,7 @@ int xca_synchronize(xca_ctx *ctx) {
 int xca_set_precision_mode(xca_ctx *ctx, int mode) {
   API_BEGIN
   auto *c = reinterpret_cast<Ctx *>(ctx);
-  if (mode != XCA_PREC_FP64 && mode != XCA_PREC_FP64_ORDERED)
+  if (mode != XCA_PREC_FP64 && mode != XCA_PREC_FP64_ORDERED && mode != XCA_PREC_FP32)
     throw Error(XCA_ERR_UNSUPPORTED, "precision mode " + std::to_string(mode) + " is not available");
   c->precision = mode;
   API_END
