@@ -199,3 +199,39 @@ def test_t2g_nca_solve_vs_oracle():
     for a, b in zip(S.G, G):
         assert np.max(np.abs(a - b)) < 1e-7
     assert np.max(np.abs(S.G_tau - g)) < 1e-7
+
+
+def test_dyson_concurrent_contexts_of_different_sizes():
+    # two contexts in two threads solve Dyson systems of different sizes at the same time, both with the
+    # matrix in shared memory: every launch must find the kernel's shared-memory limit above its own size
+    # (the limit is the kernel's, not the context's), and each result must equal its solve alone
+    import threading
+    from xca_b200.block_sparse import BlockOpSymQuartet, DiagramEvaluator
+    cases = []
+    for builder, beta, lam, eps in ((models.anderson, 10.0, 100.0, 1e-10), (models.kanamori_2orb, 4.0, 40.0, 1e-8)):
+        d = O.Dlr(lam, eps)
+        m = builder(d.rf, d.it, beta, lam, eps)
+        Fq = BlockOpSymQuartet(m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks, m.dims)
+        ev = DiagramEvaluator.from_arrays(beta, lam, eps, d.rf, d.it, m.hyb_poles, m.hyb_coeffs, Fq)
+        ev.dyson_setup(m.G0)
+        bs, bg = ev.device_buffer(30, ev.slab), ev.device_buffer(31, ev.slab)
+        ev.to_device(bs, ev.pack([0.05 * g for g in models.seeded_G(m, 4)]).real)
+        ev.dyson_solve_device(bs, 0.3, bg)
+        cases.append((ev, bs, bg, ev.to_host(bg, ev.slab), d.r * int(max(m.dims))))
+    assert cases[0][4] != cases[1][4] and max(c[4] for c in cases) <= 160
+    errors = []
+
+    def work(ev, bs, bg, ref, _n):
+        try:
+            for _ in range(300):
+                ev.dyson_solve_device(bs, 0.3, bg)
+            assert np.array_equal(ev.to_host(bg, ev.slab), ref)
+        except BaseException as e:  # reported to the main thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=c) for c in cases]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors

@@ -113,9 +113,11 @@ def test_mixed_solve_t2g_nca_vs_oracle():
     m = models.t2g_3orb(mesh.dlr_rf, mesh.dlr_it.it, beta, lam, eps)
     S = BlockSparseSolver(m.ad, beta, lam / beta, eps, precision="mixed")
     S.Delta_tau = np.asarray(m.extra["delta"], np.complex128)
-    S.solve(max_order=1, tol=1e-9, maxiter=150)
-    dG, dg, de, n_ora = _vs_oracle(S, m, 1, 1e-9, maxiter=150)
+    # tol 3e-9, below the stated bound (two solves that each stop at diff < tol differ by up to a few tol), and
+    # above where this model's NCA iteration stalls (1.2e-9, the oracle's as well)
+    S.solve(max_order=1, tol=3e-9, maxiter=150)
+    dG, dg, de, n_ora = _vs_oracle(S, m, 1, 3e-9, maxiter=150)
     print(f"t2g NCA: {S.n_fp32_iter} FP32 + {S.n_ppsc_iter - S.n_fp32_iter} FP64 iterations (oracle {n_ora}); "
           f"|dG(tau)| {dg:.1e}, |dG| {dG:.1e}, |deta| {de:.1e}")
-    assert S.diff_G < 1e-9
+    assert S.diff_G < 3e-9
     assert dg <= TOL_MIXED and dG <= TOL_MIXED and de <= TOL_MIXED

@@ -82,7 +82,10 @@ int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const do
   // the largest block's matrix (row stride N + 1) and right-hand sides in shared memory when they fit
   const size_t lu_smem = ((size_t)n_max * (n_max + 1) + (size_t)n_max * d_max) * sizeof(double);
   if (n_max <= DYSON_SMEM_MAX_N && lu_smem <= DYSON_SMEM_MAX_BYTES) {
-    if (cudaFuncSetAttribute(dyson_lu_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_smem) != cudaSuccess)
+    // the attribute is the function's, shared by every context and thread: always the same bound, so that a
+    // concurrent launch with a larger system is never left below its own size
+    if (cudaFuncSetAttribute(dyson_lu_solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DYSON_SMEM_MAX_BYTES) !=
+        cudaSuccess)
       check_launch("dyson_lu_solve_kernel attributes");
     dyson_lu_solve_kernel<true><<<B.nb, 1024, lu_smem, s>>>(B, rhs, G, hermitize, status);
   } else {
