@@ -92,6 +92,11 @@ int xca_dyson_setup(xca_ctx *ctx, const double *G0);
  * Host packed complex slabs in and out.  A singular system matrix gives XCA_ERR_RUNTIME. */
 int xca_dyson_solve(xca_ctx *ctx, const double *Sigma, double eta, int hermitize, double *G_out);
 
+/* dyson_it_ppsc::solve_with_op(sig, eta, op) (dlr_dyson_ppsc.hpp:188-216): the same solve with G0(t) op added to
+ * the source term, (I - G0 * (Sigma + eta + op)) G = G0 in the reference's operation order (convolution, + eta
+ * G0, + G0(t) op, negation).  op: one d_b x d_b complex matrix per block, packed in block order (real data). */
+int xca_dyson_solve_with_op(xca_ctx *ctx, const double *Sigma, double eta, const double *op, int hermitize, double *G_out);
+
 /* Same on device-resident real slabs, asynchronous on the context's stream; a singular system is
  * reported by the next xca_normalize_device or xca_dyson_solve. */
 int xca_dyson_solve_device(xca_ctx *ctx, const double *Sigma_dev, double eta, int hermitize, double *G_dev);

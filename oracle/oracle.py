@@ -47,6 +47,7 @@ def lib():
         L.ora_convolve.argtypes = [P, D, I, I, I, dp, dp, I, dp]
         L.ora_convmat.argtypes = [P, D, I, dp, I, dp]
         L.ora_dyson_solve.argtypes = [P, D, I, dp, dp, D, dp]
+        L.ora_dyson_solve_op.argtypes = [P, D, I, dp, dp, D, dp, dp]
         L.ora_eval_new.restype = P
         L.ora_eval_new.argtypes = [P, D, I, dp, dp, I, lp, I, ip, ip, dp, ip, dp]
         L.ora_eval_free.argtypes = [P]
@@ -145,13 +146,19 @@ class Dlr:
         _check(lib().ora_convmat(self._h, beta, n, _dp(fc), int(bool(time_order)), _dp(out)))
         return out
 
-    def dyson_solve(self, beta, g0, sig, eta):
-        """``dyson_it_ppsc(beta, itops, g0).solve(sig, eta)`` (``c++/triqs_xca/dlr_dyson_ppsc.hpp:135-168``)."""
+    def dyson_solve(self, beta, g0, sig, eta, op=None):
+        """``dyson_it_ppsc(beta, itops, g0).solve(sig, eta)`` (``c++/triqs_xca/dlr_dyson_ppsc.hpp:135-168``), or with
+        ``op`` (n x n) ``solve_with_op(sig, eta, op)`` (``dlr_dyson_ppsc.hpp:188-216``)."""
         g0 = _c(g0)
         sig = _c(sig)
         n = g0.shape[1]
         out = np.empty_like(g0)
-        _check(lib().ora_dyson_solve(self._h, beta, n, _dp(g0), _dp(sig), float(eta), _dp(out)))
+        if op is None:
+            _check(lib().ora_dyson_solve(self._h, beta, n, _dp(g0), _dp(sig), float(eta), _dp(out)))
+        else:
+            o = _c(op)
+            assert o.shape == (n, n)
+            _check(lib().ora_dyson_solve_op(self._h, beta, n, _dp(g0), _dp(sig), float(eta), _dp(o), _dp(out)))
         return out
 
 

@@ -857,18 +857,32 @@ int ora_convmat(void *d, double beta, int n, const double *fc, int time_order, d
   return 0;
 }
 
-// dyson_it_ppsc(beta, itops, g0).solve(sig, eta)  dlr_dyson_ppsc.hpp:91-168
-int ora_dyson_solve(void *dv, double beta, int n, const double *g0_, const double *sig_, double eta, double *g_out) {
+// dyson_it_ppsc(beta, itops, g0).solve(sig, eta)  dlr_dyson_ppsc.hpp:91-168; with op (n x n, may be null),
+// solve_with_op(sig, eta, op)  dlr_dyson_ppsc.hpp:188-216: ggs += eta g0, then ggs(k) += g0(k) op, then negated
+int ora_dyson_solve_op(void *dv, double beta, int n, const double *g0_, const double *sig_, double eta, const double *op_,
+                       double *g_out) {
   try {
     const Dlr &D = *(Dlr *)dv;
     int r = D.r;
     size_t sz = (size_t)r * n * n;
-    const cd *g0 = (const cd *)g0_, *sig = (const cd *)sig_;
+    const cd *g0 = (const cd *)g0_, *sig = (const cd *)sig_, *op = (const cd *)op_;
     std::vector<cd> g0c(sz), sigc(sz), ggs(sz), ggsc(sz);
     D.vals2coefs(g0, (long)n * n, g0c.data());
     D.vals2coefs(sig, (long)n * n, sigc.data());
     D.convolve(beta, n, n, n, g0c.data(), sigc.data(), true, ggs.data());
-    for (size_t x = 0; x < sz; ++x) ggs[x] = -(ggs[x] + eta * g0[x]);
+    if (op == nullptr) {
+      for (size_t x = 0; x < sz; ++x) ggs[x] = -(ggs[x] + eta * g0[x]);
+    } else {
+      for (size_t x = 0; x < sz; ++x) ggs[x] = ggs[x] + eta * g0[x];
+      for (int k = 0; k < r; ++k)
+        for (int a = 0; a < n; ++a)
+          for (int c = 0; c < n; ++c) {
+            cd s = 0.0;
+            for (int b = 0; b < n; ++b) s += g0[((size_t)k * n + a) * n + b] * op[(size_t)b * n + c];
+            ggs[((size_t)k * n + a) * n + c] += s;
+          }
+      for (size_t x = 0; x < sz; ++x) ggs[x] = -ggs[x];
+    }
     D.vals2coefs(ggs.data(), (long)n * n, ggsc.data());
     long N = (long)r * n;
     std::vector<cd> M((size_t)N * N);
@@ -881,6 +895,10 @@ int ora_dyson_solve(void *dv, double beta, int n, const double *g0_, const doubl
     std::copy(rhs.begin(), rhs.end(), (cd *)g_out);
     return 0;
   } catch (std::exception &e) { g_err = e.what(); return 1; }
+}
+
+int ora_dyson_solve(void *dv, double beta, int n, const double *g0_, const double *sig_, double eta, double *g_out) {
+  return ora_dyson_solve_op(dv, beta, n, g0_, sig_, eta, nullptr, g_out);
 }
 
 // DiagramEvaluator TRIQS-free constructor (bsb.cpp:63-85) plus BlockOpSymQuartet (block_sparse.cpp:496-577)

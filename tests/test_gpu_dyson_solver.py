@@ -235,3 +235,26 @@ def test_dyson_concurrent_contexts_of_different_sizes():
     for t in threads:
         t.join()
     assert not errors, errors
+
+
+def test_dyson_solve_with_op_vs_oracle():
+    # solve_with_op(sig, eta, op) (dlr_dyson_ppsc.hpp:188-216): the source term gains G0(t) op; per Kanamori block
+    # against the oracle's restatement (1e-12), and with op = 0 equal to solve() bit for bit
+    from xca_b200.dlr_dyson_ppsc import DysonItPPSC
+    from xca_b200.pycppdlr import ImTimeOps, build_dlr_rf
+    beta, lam, eps = 20.0, 200.0, 1e-12
+    itops = ImTimeOps(lam, build_dlr_rf(lam, eps))
+    d = O.Dlr(lam, eps, rf=itops.get_rfnodes(), it=itops.get_itnodes())
+    m = models.kanamori_2orb(d.rf, d.it, beta, lam, eps)
+    ora = O.Evaluator(d, beta, m.hyb_poles, m.hyb_coeffs, m.dims, m.labels, m.F_index, m.F_blocks, m.Fd_index, m.Fd_blocks)
+    Sig = [-s for s in ora.compute_self_energy(m.G0, np.array([[0, 1]], np.int32))]
+    rng = np.random.default_rng(5)
+    for b, g0 in enumerate(m.G0):
+        n = g0.shape[1]
+        a = rng.normal(0.0, 0.3, (n, n))
+        op = a + a.T
+        solver = DysonItPPSC(beta, itops, g0)
+        dev = solver.solve_with_op(Sig[b], 0.4, op)
+        ref = d.dyson_solve(beta, g0, Sig[b], 0.4, op=op)
+        assert _rel(dev, ref) < 1e-12, b
+        assert np.array_equal(solver.solve_with_op(Sig[b], 0.4, np.zeros((n, n))), solver.solve(Sig[b], 0.4)), b

@@ -49,6 +49,7 @@ SIGNATURES = {
     "xca_basis_setup": [P, D, D, D, I, dp, dp, I, ip],
     "xca_dyson_setup": [P, dp],
     "xca_dyson_solve": [P, dp, D, I, dp],
+    "xca_dyson_solve_with_op": [P, dp, D, dp, I, dp],
     "xca_dyson_solve_device": [P, P, D, I, P],
     "xca_trace": [P, dp, dp],
     "xca_trace_device": [P, P, dp],

@@ -69,11 +69,11 @@ static int launch_blocked_lu(cudaStream_t s, const DysonBasis &B, int n_max, int
 
 template <int RP>
 int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const double *Sigma, double eta, int hermitize, double *rhs,
-                 double *G, int *status, int n_max, int d_max, int blocked_min_n) {
+                 double *G, int *status, int n_max, int d_max, int blocked_min_n, const double *op) {
   const size_t sm = (2 * (size_t)RP * RP + RP + (RP + 1) / 2) * sizeof(double);
   if (cudaFuncSetAttribute(dyson_coef_kernel<RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
     check_launch("dyson_coef_kernel attributes");
-  dyson_coef_kernel<RP><<<B.nb, 256, sm, s>>>(B, Sigma, eta);
+  dyson_coef_kernel<RP><<<B.nb, 256, sm, s>>>(B, Sigma, eta, op);
   check_launch("dyson_coef_kernel");
   dim3 grid((unsigned)((n_conv_rows + 63) / 64), (unsigned)B.nb);
   dyson_convmat_kernel<RP><<<grid, 64, 0, s>>>(B);
@@ -146,11 +146,11 @@ int launch_axpby(cudaStream_t s, double alpha, const double *x, double beta, dou
 }
 
 template int launch_dyson<32>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *, int,
-                               int, int);
+                               int, int, const double *);
 template int launch_dyson<48>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *, int,
-                               int, int);
+                               int, int, const double *);
 template int launch_dyson<64>(cudaStream_t, const DysonBasis &, long, const double *, double, int, double *, double *, int *, int,
-                               int, int);
+                               int, int, const double *);
 template int launch_convolve_ppsc<32>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);
 template int launch_convolve_ppsc<48>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);
 template int launch_convolve_ppsc<64>(cudaStream_t, const DysonBasis &, const double *, const double *, double *);

@@ -95,7 +95,8 @@ __device__ __forceinline__ void coefs_and_hilbert(const double *sLU, const doubl
 // One CTA per block: sigc, gt, Q, P', ggs, then f = K^-1 ggs and ft = W f into the block's work area
 // [sigc | gt | Q | P' | f | ft], each r d^2 doubles.
 template <int RP>
-__global__ void __launch_bounds__(256) dyson_coef_kernel(DysonBasis B, const double *__restrict__ Sigma, double eta) {
+__global__ void __launch_bounds__(256) dyson_coef_kernel(DysonBasis B, const double *__restrict__ Sigma, double eta,
+                                                         const double *__restrict__ op) {
   extern __shared__ __align__(16) double smem[];
   double *sLU = smem;
   double *sW = sLU + RP * RP + RP;
@@ -124,7 +125,12 @@ __global__ void __launch_bounds__(256) dyson_coef_kernel(DysonBasis B, const dou
     P[e] = mul(B.k0[l], sp);
   }
   __syncthreads();
-  // ggs(t_i) = -(h(t_i) + eta G0(t_i)), h = fma(t_i, h2, h1); stored in the sigc slot (no longer read)
+  // ggs(t_i) = -(h(t_i) + eta G0(t_i)), h = fma(t_i, h2, h1); stored in the sigc slot (no longer read).  With an
+  // operator (solve_with_op, dlr_dyson_ppsc.hpp:188-196): ggs(t_i) = -((h + eta G0) + G0(t_i) op), the
+  // product summed over the inner index ascending, each product and sum separately rounded.
+  const double *ob = op;
+  if (op)
+    for (int bb = 0; bb < b; ++bb) ob += (long)B.dims[bb] * B.dims[bb];
   for (long e = threadIdx.x; e < rdd; e += blockDim.x) {
     const int i = (int)(e / dd), xz = (int)(e - (long)i * dd);
     double h1 = 0.0, h2 = 0.0;
@@ -134,7 +140,15 @@ __global__ void __launch_bounds__(256) dyson_coef_kernel(DysonBasis B, const dou
       h2 = fmad(bk, P[(long)l * dd + xz], h2);
     }
     const double h = fmad(B.tabs[i], h2, h1);
-    sigc[e] = -add(h, mul(eta, g0[e]));
+    if (ob) {
+      const int x = xz / d, z = xz - x * d;
+      const double *g0r = g0 + (long)i * dd + x * d;
+      double mop = 0.0;
+      for (int y = 0; y < d; ++y) mop = add(mop, mul(g0r[y], ob[y * d + z]));
+      sigc[e] = -add(add(h, mul(eta, g0[e])), mop);
+    } else {
+      sigc[e] = -add(h, mul(eta, g0[e]));
+    }
   }
   __syncthreads();
   coefs_and_hilbert<RP, false>(sLU, sW, sPerm, r, dd, sigc, f, ft);

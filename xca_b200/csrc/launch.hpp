@@ -49,7 +49,7 @@ constexpr size_t DYSON_SMEM_MAX_BYTES = 220 * 1024;
 
 template <int RP>
 int launch_dyson(cudaStream_t s, const DysonBasis &B, long n_conv_rows, const double *Sigma, double eta, int hermitize, double *rhs,
-                 double *G, int *status, int n_max, int d_max, int blocked_min_n);
+                 double *G, int *status, int n_max, int d_max, int blocked_min_n, const double *op = nullptr);
 
 template <int RP>
 int launch_trace_beta(cudaStream_t s, const DysonBasis &B, const double *G, double *out);

@@ -298,6 +298,7 @@ struct Ctx {
   DevBuf<int> d_dims, d_set_to_orb, d_perm, d_pinv;
   DevBuf<double> d_LUp, d_Wp, d_BKp, d_tab;
   DevBuf<double> d_convw;  // RP^3: divided weights of the Dyson convolution-matrix rows
+  DevBuf<double> d_op;     // per-block operator of xca_dyson_solve_with_op
   DevBuf<long> d_tab_off;
   DevBuf<long> d_goff, d_F_off, d_Fd_off, d_Fb_off, d_Fdb_off;
   DevBuf<int> d_counter;
@@ -1094,17 +1095,17 @@ static void require_dyson(const Ctx *c) {
   if (!c->dyson_ready) throw Error(XCA_ERR_INVALID, "Dyson solver not set up (xca_dyson_setup)");
 }
 
-static void launch_dyson(Ctx *c, const double *Sig_dev, double eta, int hermitize, double *G_dev) {
+static void launch_dyson(Ctx *c, const double *Sig_dev, double eta, int hermitize, double *G_dev, const double *op_dev = nullptr) {
   CUDA_CHECK(cudaMemsetAsync(c->d_status.ptr, 0, sizeof(int), c->stream));
   const DysonBasis B = dyson_basis(c);
   const int n_max = c->r * c->nmax, d_max = c->nmax;
   switch (c->RP) {
     case 32: c->launches += launch_dyson<32>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max,
-                                                        c->dyson_blocked_min_n); break;
+                                                        c->dyson_blocked_min_n, op_dev); break;
     case 48: c->launches += launch_dyson<48>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max,
-                                                        c->dyson_blocked_min_n); break;
+                                                        c->dyson_blocked_min_n, op_dev); break;
     default: c->launches += launch_dyson<64>(c->stream, B, c->n_conv_rows, Sig_dev, eta, hermitize, c->d_rhs.ptr, G_dev, c->d_status.ptr, n_max, d_max,
-                                                        c->dyson_blocked_min_n); break;
+                                                        c->dyson_blocked_min_n, op_dev); break;
   }
 }
 
@@ -1731,6 +1732,30 @@ int xca_dyson_solve(xca_ctx *ctx, const double *Sigma, double eta, int hermitize
   c->d_G.resize(c->slab);
   CUDA_CHECK(cudaMemcpyAsync(c->d_Sig.ptr, sg.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   launch_dyson(c, c->d_Sig.ptr, eta, hermitize, c->d_G.ptr);
+  std::vector<double> g(c->slab);
+  CUDA_CHECK(cudaMemcpyAsync(g.data(), c->d_G.ptr, c->slab * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_CHECK(cudaStreamSynchronize(c->stream));
+  check_dyson_status(c);
+  for (long i = 0; i < c->slab; ++i) { G_out[2 * i] = g[i]; G_out[2 * i + 1] = 0.0; }
+  API_END
+}
+
+int xca_dyson_solve_with_op(xca_ctx *ctx, const double *Sigma, double eta, const double *op, int hermitize, double *G_out) {
+  API_BEGIN
+  auto *c = reinterpret_cast<Ctx *>(ctx);
+  require_dyson(c);
+  set_device(c);
+  long nop = 0;
+  for (int b = 0; b < c->nb; ++b) nop += (long)c->dims[b] * c->dims[b];
+  std::vector<double> sg, o;
+  real_part(Sigma, c->slab, sg, "Sigma");
+  real_part(op, nop, o, "op");
+  c->d_Sig.resize(c->slab);
+  c->d_G.resize(c->slab);
+  c->d_op.resize(std::max(nop, 1L));
+  CUDA_CHECK(cudaMemcpyAsync(c->d_Sig.ptr, sg.data(), c->slab * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CUDA_CHECK(cudaMemcpyAsync(c->d_op.ptr, o.data(), nop * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  launch_dyson(c, c->d_Sig.ptr, eta, hermitize, c->d_G.ptr, c->d_op.ptr);
   std::vector<double> g(c->slab);
   CUDA_CHECK(cudaMemcpyAsync(g.data(), c->d_G.ptr, c->slab * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CUDA_CHECK(cudaStreamSynchronize(c->stream));

@@ -53,3 +53,18 @@ class DysonItPPSC:
         _lib.check(_lib.lib().xca_dyson_solve(self._ctx, _lib.as_dp(s.view(np.float64)), float(eta), int(bool(hermitize)),
                                               _lib.as_dp(out.view(np.float64))))
         return out
+
+    def solve_with_op(self, sig, eta, op, hermitize=False):
+        """G solving (1 - G0 * (Sigma + eta + op) *) G = G0: the source term gains G0(t) op, as the reference's
+        solve_with_op (dlr_dyson_ppsc.hpp:188-216) adds it (``op`` a d x d matrix)."""
+        s = np.ascontiguousarray(sig, dtype=np.complex128)
+        if s.shape != self.g0.shape:
+            raise ValueError(f"sig has shape {s.shape}, expected {self.g0.shape}")
+        o = np.ascontiguousarray(op, dtype=np.complex128)
+        if o.shape != (self.d, self.d):
+            raise ValueError(f"op has shape {o.shape}, expected {(self.d, self.d)}")
+        out = np.empty_like(s)
+        _lib.check(_lib.lib().xca_dyson_solve_with_op(self._ctx, _lib.as_dp(s.view(np.float64)), float(eta),
+                                                      _lib.as_dp(o.view(np.float64)), int(bool(hermitize)),
+                                                      _lib.as_dp(out.view(np.float64))))
+        return out
