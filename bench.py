@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--serving", action="store_true",
                     help="instead of the Sigma metric: a Poisson stream of whole self-consistent solves through the solve server")
     ap.add_argument("--serving-requests", type=int, default=256)
+    ap.add_argument("--serving-concurrency", type=int, default=8, help="solves the server runs at once")
     ap.add_argument("--no-serving", action="store_true", help="skip the served-solves measurement of the default line")
     ap.add_argument("--dshell", action="store_true",
                     help="instead of the Sigma metric: OCA Sigma of the five-orbital d shell (wide-chain kernel)")
@@ -177,9 +178,9 @@ def run_serving(args, batched=False):
     (mean gap 5 ms, numpy default_rng(2)); each request draws a model family (single-orbital Anderson,
     two-orbital Kanamori, three-orbital t2g with its 8-pole off-diagonal bath), beta in {10, 20, 50, 100},
     Lambda = 10 beta, U ~ U(1, 6), an order in {NCA, OCA, TCA} (t2g: NCA, OCA) and tolerance 1e-8, at most
-    100 iterations, the hybridization compressed as the reference's solve does by default.  Up to 8 solves
-    run concurrently, each with its own context and stream, in lock step with one Sigma launch per iteration
-    for all of them (``batched``) or in worker threads."""
+    100 iterations, the hybridization compressed as the reference's solve does by default.  Up to
+    --serving-concurrency solves (default 8) run concurrently, each with its own context and stream, in lock
+    step with one Sigma launch per iteration for all of them (``batched``) or in worker threads."""
     from xca_b200.serving import SolveServer, STREAM_EPS, synthetic_request
     rng = np.random.default_rng(2)
     n = args.serving_requests
@@ -192,7 +193,7 @@ def run_serving(args, batched=False):
         U = float(rng.uniform(1.0, 6.0))
         order = int(rng.integers(1, 3 if kind == "t2g" else 4))
         reqs.append(synthetic_request(kind, beta, U, order, tag=(kind, beta, order)))
-    srv = SolveServer(max_concurrent=8, batched=batched)
+    srv = SolveServer(max_concurrent=args.serving_concurrency, batched=batched)
     for kind, order in (("anderson", 3), ("kanamori", 3), ("t2g", 2)):  # warm-up: module load and first-use set-up
         srv.submit(synthetic_request(kind, 10.0, 2.0, order)).result()
     t0 = time.perf_counter()
@@ -210,7 +211,7 @@ def run_serving(args, batched=False):
     lat = np.array([r.latency for r in res])
     out = {"metric": "served solves/s (FP64 plain, mixed stream)", "value": n / (t1 - t0), "unit": "solves/s", "n_gpus": 1,
            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "poisson_stream", "requests": n, "mean_gap_ms": 5.0, "max_concurrent": 8,
+           "config": {"workload": "poisson_stream", "requests": n, "mean_gap_ms": 5.0, "max_concurrent": args.serving_concurrency,
                       "mode": "lock step, one batched Sigma launch per iteration" if batched else "worker threads",
                       "models": "anderson, kanamori_2orb, t2g_3orb (U ~ U(1, 6))", "orders": "1-3; t2g 1-2",
                       "t2g_tca_excluded": "a t2g TCA solve alone takes 41-172 s (0.45 s per iteration, up to 100 iterations)",

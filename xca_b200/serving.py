@@ -8,14 +8,20 @@ solve has its own evaluator context — its own CUDA stream, its G, Σ and Dyson
 device for the whole solve — so a result does not depend on what else runs (up to the summation order
 of the Σ items).  Two ways to run them:
 
-- lock step (``batched=True``, the default): one scheduler thread runs an iteration of every live solve at a time,
+- lock step (``batched=True``): one scheduler thread runs an iteration of every live solve at a time,
   the Σ of all of them (every topology of every solve, grouped by padded DLR rank) in ONE job-batched
   launch (``DiagramEvaluator.compute_self_energy_device_batch``), then their Dyson solves, then their
   normalisations and convergence tests.  Set-up (hybridization fit, evaluator) and the final
   single-particle Green's function run in helper threads beside it; a solve joins the next iteration
   when its set-up is done and leaves when it converges;
-- threads (``batched=False``): each solve iterates in its own worker thread; the device work of
-  concurrent solves overlaps through their streams.
+- threads (``batched=False``, the default): each solve iterates in its own worker thread; the device work
+  of concurrent solves overlaps through their streams, and each solve's own topologies share one batched
+  launch per iteration.
+
+Which is faster depends on the stream, measured: one batched launch ties its solves to the slowest of
+them, so the lock step wins when the solves are alike and small (43 vs 29 solves/s on a stream of small
+Anderson and Kanamori solves) and loses when their costs spread (5.2 vs 5.5 solves/s on the stream of
+bench.py, which mixes t2g and beta = 100 third-order solves with small ones; 4.3 vs 5.8 at 16 concurrent).
 """
 
 import threading
@@ -93,7 +99,7 @@ class SolveServer:
     """Admits solve requests by device-memory budget and runs up to ``max_concurrent`` at a time, each in
     its own thread or (``batched``) all in lock step with one Σ launch per iteration."""
 
-    def __init__(self, max_concurrent=8, hbm_budget=48 << 30, device=0, batched=True):
+    def __init__(self, max_concurrent=8, hbm_budget=48 << 30, device=0, batched=False):
         self.max_concurrent = max_concurrent
         self.budget = int(hbm_budget)
         self.device = device
