@@ -258,6 +258,14 @@ class dyson_it_ppsc {
     check(xca_dyson_solve(ctx_, detail::dp(sig), eta, 0, detail::dp(out)));
     return out;
   }
+  // dlr_dyson_ppsc.hpp:188-216: the source term gains G0(t) op (op: d x d)
+  std::vector<dcomplex> solve_with_op(const std::vector<dcomplex> &sig, double eta, const std::vector<dcomplex> &op) {
+    if (sig.size() != (size_t)r_ * d_ * d_) throw std::invalid_argument("dyson_it_ppsc::solve_with_op: sig must be r x d x d");
+    if (op.size() != (size_t)d_ * d_) throw std::invalid_argument("dyson_it_ppsc::solve_with_op: op must be d x d");
+    std::vector<dcomplex> out(sig.size());
+    check(xca_dyson_solve_with_op(ctx_, detail::dp(sig), eta, detail::dp(op), 0, detail::dp(out)));
+    return out;
+  }
   int rank() const { return r_; }
 
  private:
