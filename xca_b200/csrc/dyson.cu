@@ -21,10 +21,21 @@ static int launch_blocked_lu(cudaStream_t s, const DysonBasis &B, int n_max, int
   lu_rhs_init_kernel<<<gi, 256, 0, s>>>(B, rhs);
   check_launch("lu_rhs_init_kernel");
   ++launches;
-  const int tiles = (n_max + 63) / 64;
+  // the attribute is set to the same maximum by every caller (contexts of different sizes may call this
+  // concurrently from several host threads)
+  if (cudaFuncSetAttribute(lu_panel_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, LU_PANEL_SMEM_MAX_BYTES) !=
+      cudaSuccess)
+    check_launch("lu_panel_smem_kernel attributes");
   for (int k0 = 0; k0 < n_max; k0 += LU_NB) {
-    lu_panel_kernel<<<B.nb, 1024, 0, s>>>(B, rhs, k0, status);
-    check_launch("lu_panel_kernel");
+    // the panel's rows [k0, N) in shared memory where they fit, else the panel in global memory
+    const size_t psm = (size_t)(n_max - k0) * LU_PS * sizeof(double);
+    if (psm <= (size_t)LU_PANEL_SMEM_MAX_BYTES) {
+      lu_panel_smem_kernel<<<B.nb, 1024, psm, s>>>(B, rhs, k0, status);
+      check_launch("lu_panel_smem_kernel");
+    } else {
+      lu_panel_kernel<<<B.nb, 1024, 0, s>>>(B, rhs, k0, status);
+      check_launch("lu_panel_kernel");
+    }
     const int rest = n_max - k0 - LU_NB;
     if (rest > 0) {
       lu_u12_kernel<<<dim3((unsigned)((rest + 127) / 128), 1, (unsigned)B.nb), 128, 0, s>>>(B, k0);
@@ -36,7 +47,6 @@ static int launch_blocked_lu(cudaStream_t s, const DysonBasis &B, int n_max, int
     }
     ++launches;
   }
-  (void)tiles;
   const unsigned dcol = (unsigned)((d_max + 127) / 128);
   for (int k0 = 0; k0 < n_max; k0 += LU_NB) {
     lu_fwd_panel_kernel<<<B.nb, 128, 0, s>>>(B, rhs, k0);

@@ -580,6 +580,106 @@ __global__ void __launch_bounds__(1024) lu_panel_kernel(DysonBasis B, double *__
   }
 }
 
+// The panel factorisation of lu_panel_kernel with the panel -- rows [k0, N) x columns [k0, k0 + LU_NB) --
+// held in shared memory (row stride LU_PS, so a warp reading one column hits distinct banks): the same pivot
+// choices (largest |a_ik|, lowest row on ties) and the same separately rounded divisions and updates in the
+// same order.  Interchanges only permute the entries of the other columns and of the right-hand side, so
+// those are applied after the panel, pivot by pivot in order, one thread per column.  Launched with
+// (n_max - k0) LU_PS doubles of dynamic shared memory, at most LU_PANEL_SMEM_MAX_BYTES.
+constexpr int LU_PS = LU_NB + 1;
+constexpr int LU_PANEL_SMEM_MAX_BYTES = 200 * 1024;
+
+__global__ void __launch_bounds__(1024) lu_panel_smem_kernel(DysonBasis B, double *__restrict__ rhs, int k0, int *__restrict__ status) {
+  extern __shared__ double P[];
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  __shared__ int s_piv[LU_NB];
+  const int b = blockIdx.x;
+  const int N = (int)lu_dim(B, b), d = B.dims[b];
+  if (k0 >= N) return;
+  const int M = N - k0, nb = min(LU_NB, M);
+  double *A = B.mats + B.moff[b];
+  double *x = rhs + B.goff[b];
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < M * nb; e += nt) {
+    const int i = e / nb, c = e - i * nb;
+    P[i * LU_PS + c] = A[(long)(k0 + i) * N + k0 + c];
+  }
+  __syncthreads();
+  for (int c = 0; c < nb; ++c) {
+    double bv = -1.0;
+    int bi = M;
+    for (int i = c + tid; i < M; i += nt) argmax_combine(bv, bi, fabs(P[i * LU_PS + c]), i);
+    for (int o = 16; o > 0; o >>= 1) {
+      const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+      argmax_combine(bv, bi, v2, i2);
+    }
+    if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
+    __syncthreads();
+    if (warp == 0) {
+      bv = lane < (nt >> 5) ? red_v[lane] : -1.0;
+      bi = lane < (nt >> 5) ? red_i[lane] : M;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        argmax_combine(bv, bi, v2, i2);
+      }
+      if (lane == 0) s_piv[c] = bi;
+    }
+    __syncthreads();
+    const int p = s_piv[c];
+    if (p >= M) {  // a column of NaN: flag and leave the block
+      if (tid == 0) atomicExch(status, 1);
+      return;
+    }
+    if (p != c && tid < nb) {
+      const double t = P[c * LU_PS + tid];
+      P[c * LU_PS + tid] = P[p * LU_PS + tid];
+      P[p * LU_PS + tid] = t;
+    }
+    __syncthreads();
+    const double piv = P[c * LU_PS + c];
+    if (piv == 0.0) {
+      if (tid == 0) atomicExch(status, 1);
+      return;
+    }
+    for (int i = c + 1 + tid; i < M; i += nt) P[i * LU_PS + c] = __ddiv_rn(P[i * LU_PS + c], piv);
+    __syncthreads();
+    const int w = nb - c - 1;
+    if (w > 0)
+      for (int e = tid; e < (M - c - 1) * w; e += nt) {
+        const int i = c + 1 + e / w, j = c + 1 + (e - (e / w) * w);
+        P[i * LU_PS + j] = __dsub_rn(P[i * LU_PS + j], mul(P[i * LU_PS + c], P[c * LU_PS + j]));
+      }
+    __syncthreads();
+  }
+  for (int e = tid; e < M * nb; e += nt) {
+    const int i = e / nb, c = e - i * nb;
+    A[(long)(k0 + i) * N + k0 + c] = P[i * LU_PS + c];
+  }
+  // columns [0, k0) and [k0 + nb, N) of the matrix, then the d right-hand-side columns
+  for (int j = tid; j < N - nb + d; j += nt) {
+    double *col;
+    long ld;
+    if (j < N - nb) {
+      col = A + (j < k0 ? j : j + nb);
+      ld = N;
+    } else {
+      col = x + (j - (N - nb));
+      ld = d;
+    }
+    for (int c = 0; c < nb; ++c) {
+      const int p = s_piv[c];
+      if (p != c) {
+        const double t = col[(long)(k0 + c) * ld];
+        col[(long)(k0 + c) * ld] = col[(long)(k0 + p) * ld];
+        col[(long)(k0 + p) * ld] = t;
+      }
+    }
+  }
+}
+
 // Panel rows right of the panel (U12): for every column j >= k0 + LU_NB, the panel's updates
 // a_ij -= l_ik a_kj for k0 <= k < i < k0 + LU_NB in ascending k.  One thread per column.
 __global__ void __launch_bounds__(128) lu_u12_kernel(DysonBasis B, int k0) {
@@ -660,18 +760,36 @@ __global__ void __launch_bounds__(256) lu_trail_kernel(DysonBasis B, int k0) {
 
 // Forward substitution with the unit lower factor, panel [k0, k0 + LU_NB): in-panel rows (one thread per
 // right-hand-side column), then the rows below (64-row tiles).  x_ij <- fma(-L_ik, x_kj, x_ij), k ascending.
+// The panel's diagonal block in shared memory (zero outside the nb x nb block), each column's nb entries in
+// registers.
 __global__ void __launch_bounds__(128) lu_fwd_panel_kernel(DysonBasis B, double *__restrict__ rhs, int k0) {
+  __shared__ double L[LU_NB][LU_PS];
   const int b = blockIdx.x;
   const int N = (int)lu_dim(B, b), d = B.dims[b];
   if (k0 >= N) return;
-  const int kend = min(k0 + LU_NB, N);
+  const int nb = min(LU_NB, N - k0);
   const double *A = B.mats + B.moff[b];
   double *x = rhs + B.goff[b];
-  for (int j = threadIdx.x; j < d; j += blockDim.x)
-    for (int k = k0; k < kend; ++k) {
-      const double xk = x[(long)k * d + j];
-      for (int i = k + 1; i < kend; ++i) x[(long)i * d + j] = fmad(-A[(long)i * N + k], xk, x[(long)i * d + j]);
-    }
+  for (int e = threadIdx.x; e < LU_NB * LU_NB; e += blockDim.x) {
+    const int i = e / LU_NB, k = e - i * LU_NB;
+    L[i][k] = (i < nb && k < nb) ? A[(long)(k0 + i) * N + k0 + k] : 0.0;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < d; j += blockDim.x) {
+    double xr[LU_NB];
+#pragma unroll
+    for (int i = 0; i < LU_NB; ++i) xr[i] = i < nb ? x[(long)(k0 + i) * d + j] : 0.0;
+#pragma unroll
+    for (int k = 0; k < LU_NB; ++k)
+      if (k < nb) {
+        const double xk = xr[k];
+#pragma unroll
+        for (int i = k + 1; i < LU_NB; ++i) xr[i] = fmad(-L[i][k], xk, xr[i]);
+      }
+#pragma unroll
+    for (int i = 0; i < LU_NB; ++i)
+      if (i < nb) x[(long)(k0 + i) * d + j] = xr[i];
+  }
 }
 
 __global__ void __launch_bounds__(256) lu_fwd_trail_kernel(DysonBasis B, double *__restrict__ rhs, int k0) {
@@ -697,19 +815,36 @@ __global__ void __launch_bounds__(256) lu_fwd_trail_kernel(DysonBasis B, double 
 
 // Backward substitution with the upper factor, panel [k0, k0 + LU_NB) from the bottom: in-panel rows
 // (x_kj <- x_kj / U_kk, then the rows above it in the panel), then the rows above the panel; k descending.
+// The panel's diagonal block in shared memory, each column's nb entries in registers, as the forward panel.
 __global__ void __launch_bounds__(128) lu_bwd_panel_kernel(DysonBasis B, double *__restrict__ rhs, int k0) {
+  __shared__ double U[LU_NB][LU_PS];
   const int b = blockIdx.x;
   const int N = (int)lu_dim(B, b), d = B.dims[b];
   if (k0 >= N) return;
-  const int kend = min(k0 + LU_NB, N);
+  const int nb = min(LU_NB, N - k0);
   const double *A = B.mats + B.moff[b];
   double *x = rhs + B.goff[b];
-  for (int j = threadIdx.x; j < d; j += blockDim.x)
-    for (int k = kend - 1; k >= k0; --k) {
-      const double xk = __ddiv_rn(x[(long)k * d + j], A[(long)k * N + k]);
-      x[(long)k * d + j] = xk;
-      for (int i = k0; i < k; ++i) x[(long)i * d + j] = fmad(-A[(long)i * N + k], xk, x[(long)i * d + j]);
-    }
+  for (int e = threadIdx.x; e < LU_NB * LU_NB; e += blockDim.x) {
+    const int i = e / LU_NB, k = e - i * LU_NB;
+    U[i][k] = (i < nb && k < nb) ? A[(long)(k0 + i) * N + k0 + k] : 0.0;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < d; j += blockDim.x) {
+    double xr[LU_NB];
+#pragma unroll
+    for (int i = 0; i < LU_NB; ++i) xr[i] = i < nb ? x[(long)(k0 + i) * d + j] : 0.0;
+#pragma unroll
+    for (int k = LU_NB - 1; k >= 0; --k)
+      if (k < nb) {
+        const double xk = __ddiv_rn(xr[k], U[k][k]);
+        xr[k] = xk;
+#pragma unroll
+        for (int i = 0; i < k; ++i) xr[i] = fmad(-U[i][k], xk, xr[i]);
+      }
+#pragma unroll
+    for (int i = 0; i < LU_NB; ++i)
+      if (i < nb) x[(long)(k0 + i) * d + j] = xr[i];
+  }
 }
 
 __global__ void __launch_bounds__(256) lu_bwd_trail_kernel(DysonBasis B, double *__restrict__ rhs, int k0) {
