@@ -350,7 +350,13 @@ __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis C
         }
         __syncwarp();
       }
-      // ---- trace contraction g(t)[mu][ka] += sum Tr[L F_mu R F^dag_ka]
+      // ---- trace contraction g(t)[mu][ka] += sum Tr[L F_mu R F^dag_ka]: per node t, s = sum_{i, j ascending}
+      // fma(tm_ij, Ok_ji, s) with tm_ij = sum_k L_ik tp_kj and tp_kj = sum_q Om_kq R_qj (fused multiply-adds
+      // from zero, inner index ascending).  Two forms with the same values: one lane per node forming every
+      // tp_kj again for each i (c3 c0 c2 (c1 + 1) dependent operations per node; faster when c0 c1 c2 c3 <= 64,
+      // as for the two-orbital blocks of dimension <= 4), or tp (r x c2 x c0, into X) and tm (r x c3 x c0,
+      // into Y) formed once per term by all lanes (faster from the 3 x 3 and 9 x 9 blocks of three orbitals
+      // on, measured; T, X and Y are free once the chains are stored).
       for (int k = 0; k < C.n_terms; ++k) {
         const CorrTerm &P = terms[C.term0 + k];
         const double *R = Rs + (long)P.rchain * slab;
@@ -358,19 +364,47 @@ __global__ void __launch_bounds__(128) correlator_kernel(DevBasis B, CorrBasis C
         const double *Om = CB.ops + CB.mu_off[P.mu * nb + P.e0];  // (c2 x c1)
         const double *Ok = CB.ops + CB.ka_off[P.ka * nb + P.e2];  // (c0 x c3)
         const int c0 = P.c0, c1 = P.c1, c2 = P.c2, c3 = P.c3;
+        if (c0 * c1 * c2 * c3 <= 64) {
+          for (int t = lane; t < r; t += 32) {
+            const double *Rt = R + (long)t * c1 * c0, *Lt = L + (long)t * c3 * c2;
+            double s = 0.0;
+            for (int i = 0; i < c3; ++i)
+              for (int jj = 0; jj < c0; ++jj) {
+                double tm = 0.0;
+                for (int kk = 0; kk < c2; ++kk) {
+                  double tp = 0.0;
+                  for (int q = 0; q < c1; ++q) tp = fmad(Om[kk * c1 + q], Rt[q * c0 + jj], tp);
+                  tm = fmad(Lt[i * c2 + kk], tp, tm);
+                }
+                s = fmad(tm, Ok[jj * c3 + i], s);
+              }
+            double *a = acc + ((long)t * nmu + P.mu) * nka + P.ka;
+            *a = add(*a, s);
+          }
+          __syncwarp();
+          continue;
+        }
+        for (int idx = lane; idx < r * c2 * c0; idx += 32) {
+          const int t = idx / (c2 * c0), rem = idx - t * c2 * c0, kk = rem / c0, jj = rem - kk * c0;
+          const double *Rt = R + (long)t * c1 * c0;
+          double tp = 0.0;
+          for (int q = 0; q < c1; ++q) tp = fmad(Om[kk * c1 + q], Rt[q * c0 + jj], tp);
+          X[idx] = tp;
+        }
+        __syncwarp();
+        for (int idx = lane; idx < r * c3 * c0; idx += 32) {
+          const int t = idx / (c3 * c0), rem = idx - t * c3 * c0, i = rem / c0, jj = rem - i * c0;
+          const double *Lt = L + (long)t * c3 * c2, *tpt = X + (long)t * c2 * c0;
+          double tm = 0.0;
+          for (int kk = 0; kk < c2; ++kk) tm = fmad(Lt[i * c2 + kk], tpt[kk * c0 + jj], tm);
+          Y[idx] = tm;
+        }
+        __syncwarp();
         for (int t = lane; t < r; t += 32) {
-          const double *Rt = R + (long)t * c1 * c0, *Lt = L + (long)t * c3 * c2;
+          const double *tmt = Y + (long)t * c3 * c0;
           double s = 0.0;
           for (int i = 0; i < c3; ++i)
-            for (int jj = 0; jj < c0; ++jj) {
-              double tm = 0.0;
-              for (int kk = 0; kk < c2; ++kk) {
-                double tp = 0.0;
-                for (int q = 0; q < c1; ++q) tp = fmad(Om[kk * c1 + q], Rt[q * c0 + jj], tp);
-                tm = fmad(Lt[i * c2 + kk], tp, tm);
-              }
-              s = fmad(tm, Ok[jj * c3 + i], s);
-            }
+            for (int jj = 0; jj < c0; ++jj) s = fmad(tmt[i * c0 + jj], Ok[jj * c3 + i], s);
           double *a = acc + ((long)t * nmu + P.mu) * nka + P.ka;
           *a = add(*a, s);
         }
