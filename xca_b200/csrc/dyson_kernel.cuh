@@ -600,16 +600,22 @@ __global__ void __launch_bounds__(1024) lu_panel_smem_kernel(DysonBasis B, doubl
   const int M = N - k0, nb = min(LU_NB, M);
   double *A = B.mats + B.moff[b];
   double *x = rhs + B.goff[b];
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  if (M > nt) {  // one thread per panel row; the launcher keeps M within the block
+    if (tid == 0) atomicExch(status, 1);
+    return;
+  }
   for (int e = tid; e < M * nb; e += nt) {
     const int i = e / nb, c = e - i * nb;
     P[i * LU_PS + c] = A[(long)(k0 + i) * N + k0 + c];
   }
   __syncthreads();
-  for (int c = 0; c < nb; ++c) {
-    double bv = -1.0;
-    int bi = M;
-    for (int i = c + tid; i < M; i += nt) argmax_combine(bv, bi, fabs(P[i * LU_PS + c]), i);
+  // thread tid owns panel row i = tid: its candidate for the first pivot, reduced per warp
+  const int i = tid;
+  double bv = -1.0;
+  int bi = M;
+  if (i < M) argmax_combine(bv, bi, fabs(P[i * LU_PS]), i);
+  for (int c = 0;; ++c) {
     for (int o = 16; o > 0; o >>= 1) {
       const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
       const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
@@ -617,15 +623,23 @@ __global__ void __launch_bounds__(1024) lu_panel_smem_kernel(DysonBasis B, doubl
     }
     if (lane == 0) { red_v[warp] = bv; red_i[warp] = bi; }
     __syncthreads();
+    if (c == nb) break;
+    // warp 0: the pivot of column c (largest |a_ic|, lowest row on ties), then the interchange of the
+    // panel rows c and p
     if (warp == 0) {
-      bv = lane < (nt >> 5) ? red_v[lane] : -1.0;
-      bi = lane < (nt >> 5) ? red_i[lane] : M;
+      double v = lane < nw ? red_v[lane] : -1.0;
+      int ix = lane < nw ? red_i[lane] : M;
       for (int o = 16; o > 0; o >>= 1) {
-        const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
-        const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
-        argmax_combine(bv, bi, v2, i2);
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, ix, o);
+        argmax_combine(v, ix, v2, i2);
       }
-      if (lane == 0) s_piv[c] = bi;
+      if (ix < M && ix != c && lane < nb) {
+        const double t = P[c * LU_PS + lane];
+        P[c * LU_PS + lane] = P[ix * LU_PS + lane];
+        P[ix * LU_PS + lane] = t;
+      }
+      if (lane == 0) s_piv[c] = ix;
     }
     __syncthreads();
     const int p = s_piv[c];
@@ -633,26 +647,21 @@ __global__ void __launch_bounds__(1024) lu_panel_smem_kernel(DysonBasis B, doubl
       if (tid == 0) atomicExch(status, 1);
       return;
     }
-    if (p != c && tid < nb) {
-      const double t = P[c * LU_PS + tid];
-      P[c * LU_PS + tid] = P[p * LU_PS + tid];
-      P[p * LU_PS + tid] = t;
-    }
-    __syncthreads();
     const double piv = P[c * LU_PS + c];
     if (piv == 0.0) {
       if (tid == 0) atomicExch(status, 1);
       return;
     }
-    for (int i = c + 1 + tid; i < M; i += nt) P[i * LU_PS + c] = __ddiv_rn(P[i * LU_PS + c], piv);
-    __syncthreads();
-    const int w = nb - c - 1;
-    if (w > 0)
-      for (int e = tid; e < (M - c - 1) * w; e += nt) {
-        const int i = c + 1 + e / w, j = c + 1 + (e - (e / w) * w);
-        P[i * LU_PS + j] = __dsub_rn(P[i * LU_PS + j], mul(P[i * LU_PS + c], P[c * LU_PS + j]));
-      }
-    __syncthreads();
+    // rows below the pivot: l_ic = a_ic / u_cc, then a_ij -= l_ic u_cj for the panel columns j > c, and the
+    // row's candidate for the next pivot
+    bv = -1.0;
+    bi = M;
+    if (i > c && i < M) {
+      const double l = __ddiv_rn(P[i * LU_PS + c], piv);
+      P[i * LU_PS + c] = l;
+      for (int j = c + 1; j < nb; ++j) P[i * LU_PS + j] = __dsub_rn(P[i * LU_PS + j], mul(l, P[c * LU_PS + j]));
+      if (c + 1 < nb) argmax_combine(bv, bi, fabs(P[i * LU_PS + c + 1]), i);
+    }
   }
   for (int e = tid; e < M * nb; e += nt) {
     const int i = e / nb, c = e - i * nb;
